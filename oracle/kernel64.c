@@ -1,0 +1,73 @@
+/*
+ * FP64 oracle: the reference kernel's algorithm and random draws in double precision with
+ * libm's double functions (see lw_oracle.h). It is the converged-image reference the FP32
+ * kernels are measured against. Test infrastructure only.
+ */
+#include <math.h>
+#include <omp.h>
+
+#define LWO_F64 1
+#define REAL double
+#define K(x) x
+#define R_SQRT sqrt
+#define R_FLOOR floor
+#define R_EXP exp
+#define R_FMOD fmod
+#define R_ACOS acos
+#define R_ATAN2 atan2
+#define R_GAMMA d_gamma_to_linear
+#define R_SINCOS_TURNS d_sin_cos_turns
+
+static inline double d_gamma_to_linear(double c) { return c <= 0.0 ? 0.0 : pow(c, 2.2); }
+static inline void d_sin_cos_turns(double u, double *s, double *c) {
+    double a = 6.283185307179586476925 * u;
+    *s = sin(a);
+    *c = cos(a);
+}
+
+#define lwo_bounds_error_count lwo_bounds_error_count
+#include "kernel_impl.h"
+
+static Cam cam64(const lwo_scene *s, const lwo_camera64 *c) {
+    if (!c) {
+        const lwo_params *p = s->params;
+        Cam r = {v3f4(p->cam_pos), v3f4(p->cam_fwd), v3f4(p->cam_right), v3f4(p->cam_up), p->cam_pos[3], p->cam_fwd[3]};
+        return r;
+    }
+    Cam r = {v3(c->eye[0], c->eye[1], c->eye[2]), v3(c->fwd[0], c->fwd[1], c->fwd[2]),
+             v3(c->right[0], c->right[1], c->right[2]), v3(c->up[0], c->up[1], c->up[2]), c->tan_half, c->aspect};
+    return r;
+}
+
+void lwo64_render_sample(const lwo_scene *s, const lwo_camera64 *cam, uint32_t px, uint32_t py, uint32_t sample,
+                         double out[3]) {
+    Cam c = cam64(s, cam);
+    V3 r = render_sample(s, &c, px, py, sample);
+    out[0] = r.x;
+    out[1] = r.y;
+    out[2] = r.z;
+}
+
+void lwo64_render_mean(const lwo_scene *s, const lwo_camera64 *cam, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                       uint32_t spp, double *out, int threads) {
+    Cam c = cam64(s, cam);
+    if (spp < 1) spp = 1;
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (uint32_t py = 0; py < h; py++)
+        for (uint32_t px = 0; px < w; px++) {
+            double acc[3] = {0, 0, 0};
+            for (uint32_t k = 0; k < spp; k++) {
+                V3 r = render_sample(s, &c, x0 + px, y0 + py, k);
+                if (isfinite(r.x) && isfinite(r.y) && isfinite(r.z)) {
+                    acc[0] += r.x;
+                    acc[1] += r.y;
+                    acc[2] += r.z;
+                }
+            }
+            double *o = out + (uint64_t)(py * w + px) * 3u;
+            o[0] = acc[0] / (double)spp;
+            o[1] = acc[1] / (double)spp;
+            o[2] = acc[2] / (double)spp;
+        }
+}
