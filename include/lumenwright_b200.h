@@ -1,0 +1,186 @@
+/*
+ * lumenwright_b200: the hq path tracer of Lumenwright (brick-grid traversal, block shading,
+ * Chunky/game sky with sun shadow rays, emitter sampling, per-pixel sample accumulation),
+ * written for NVIDIA B200 (sm_100a), behind a C ABI.
+ *
+ * It replaces the reference's CUDA entry `pt_render`
+ * (crates/lumenwright-ptx/src/lib.rs:37-87) and its host launcher `CudaBackend::render_hq`
+ * (crates/lumenwright/src/render/cuda.rs:77-184). A Rust `Backend` implementation calls these
+ * functions (INTEGRATION.md shows the binding).
+ *
+ * Conventions: every length is in elements of its buffer, as `pt_render` takes them; the caller
+ * owns every host buffer; the library owns device memory inside an `lw_ctx`. No function traps
+ * or aborts: each returns an `lw_status`, and `lw_last_error` gives the text of the last failure.
+ * A context is used from one thread at a time.
+ */
+#ifndef LUMENWRIGHT_B200_H
+#define LUMENWRIGHT_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- records shared with the reference (crates/lumenwright-kernel/src/scene.rs) ---------- */
+
+/* `GpuQuad` (scene.rs:46-57), 80 bytes. */
+typedef struct {
+    float p0[4];  /* xyz corner, w = flags (bit cast) */
+    float eu[4];  /* xyz edge along s, w = tint RGBA8 (bit cast) */
+    float ev[4];  /* xyz edge along t, w = emittance */
+    float uv[4];  /* uv0.xy, uvs.xy */
+    float uvt[4]; /* uvt.xy, unused, unused */
+} lw_quad;
+
+/* `GpuModel` (scene.rs:103-112), 16 bytes. */
+typedef struct {
+    uint32_t quad_offset, quad_count, flags, pad;
+} lw_model;
+
+/* `GpuEmitter` (scene.rs:119-124), 32 bytes. */
+typedef struct {
+    float pos[4];      /* xyz offset into grid space, w = first quad (bit cast) */
+    uint32_t faces[4]; /* x = face count */
+} lw_emitter;
+
+/* `Params` (scene.rs:160-228), 27 x 16 = 432 bytes, layout-identical. */
+typedef struct {
+    float cam_pos[4], cam_fwd[4], cam_right[4], cam_up[4];
+    float sun_dir[4], sun_color[4], sky_sun[4], sky_zenith[4];
+    float perez_a[4], perez_b[4], perez_c[4], perez_d[4], perez_e[4];
+    float water_color[4], misc_f[4];
+    uint32_t grid_dims[4], off[4], off2[4], frame[4], misc_u[4], see_through[4], emitter[4];
+    float sun_su[4], sun_sv[4], sun_sprite[4], sky_map[4], water_plane[4];
+} lw_params;
+
+/* `Hit` (crates/lumenwright-kernel/src/trace.rs:11-22); found = 0 for `None`. */
+typedef struct {
+    float t;
+    uint32_t quad, texel;
+    float s, tt;
+    int32_t found;
+} lw_hit;
+
+/* ---- status ------------------------------------------------------------------------------ */
+typedef enum {
+    LW_OK = 0,
+    LW_ERR_INVALID_ARGUMENT = 1, /* a null pointer, a zero size, an unknown option */
+    LW_ERR_BUFFER_LENGTH = 2,    /* a buffer shorter than the layout it must hold, or an index
+                                    in one buffer that points outside another */
+    LW_ERR_OUT_OF_MEMORY = 3,
+    LW_ERR_DEVICE_TIMEOUT = 4, /* a bounded wait on the device ran out */
+    LW_ERR_LAUNCH = 5,         /* a CUDA launch or copy failed */
+    LW_ERR_CANCELLED = 6,      /* lw_cancel was called during the render */
+    LW_ERR_NO_DEVICE = 7,      /* no CUDA device, or not an sm_100 one */
+    LW_ERR_NO_SCENE = 8        /* a render before lw_scene_upload */
+} lw_status;
+
+typedef struct lw_ctx lw_ctx;
+
+/* The scene a frame is drawn in: `HqScene` (crates/lumenwright/src/scene/voxel.rs:19-49).
+ * `dims` is the grid in bricks and `offsets` the word offsets of top, bricks, ov_top,
+ * ov_cells, ov_quads in `grid` (the reference's `HqScene.dims` / `offsets`). */
+typedef struct {
+    const uint32_t *grid;
+    uint64_t grid_len;
+    const lw_model *models;
+    uint64_t models_len;
+    const lw_quad *quads;
+    uint64_t quads_len;
+    const uint32_t *atlas;
+    uint64_t atlas_len;
+    const lw_emitter *emitters;
+    uint64_t emitters_len;
+    const uint32_t *emitter_grid;
+    uint64_t emitter_grid_len;
+    uint32_t dims[3];
+    uint32_t offsets[5];
+    uint32_t atlas_size[2];
+} lw_scene_desc;
+
+/* Progress after each batch of samples: (samples done, samples total, user). Called on the
+ * thread that called lw_render_hq, between launches; never from a CUDA callback thread. */
+typedef void (*lw_progress_fn)(uint32_t done, uint32_t total, void *user);
+
+/* Launch statistics of the last render on a context. */
+typedef struct {
+    double kernel_ms;        /* CUDA-event time of the path-tracing launches */
+    double upload_ms;        /* host-to-device copies and the grid re-layout of the last upload */
+    uint32_t launches;       /* path-tracing kernel launches */
+    uint32_t blocks, threads; /* launch shape (persistent: blocks = SMs x resident blocks) */
+    uint64_t samples;        /* path samples traced */
+} lw_stats;
+
+/* ---- context ------------------------------------------------------------------------------
+ * Replaces CudaBackend::new (crates/lumenwright/src/render/cuda.rs:55-63): opens `device`,
+ * checks it is sm_100, creates the context's streams. */
+lw_status lw_ctx_create(int device, lw_ctx **out);
+void lw_ctx_destroy(lw_ctx *ctx);
+/* Text of the last failure on `ctx` (or of the last lw_ctx_create failure when ctx is null). */
+const char *lw_last_error(const lw_ctx *ctx);
+/* The CUDA stream (cudaStream_t) the context launches its path-tracing kernels on. */
+void *lw_stream(lw_ctx *ctx);
+lw_status lw_get_stats(const lw_ctx *ctx, lw_stats *out);
+/* Asks a running render on `ctx` to stop; it returns LW_ERR_CANCELLED. Safe from any thread. */
+void lw_cancel(lw_ctx *ctx);
+/* Records timing mark `slot` (0..7), a CUDA event on the context's stream, and reads the time
+ * between two marks once both are reached (the device's clock, not the host's). */
+lw_status lw_mark(lw_ctx *ctx, uint32_t slot);
+lw_status lw_elapsed_ms(lw_ctx *ctx, uint32_t from, uint32_t to, double *ms);
+
+/* ---- scene ---------------------------------------------------------------------------------
+ * Replaces the seven `clone_htod` copies of CudaBackend::render_hq (cuda.rs:96-111): validates
+ * every buffer length and every cross-buffer index (what the reference's slice bounds checks
+ * would trap on), copies the buffers and re-lays the brick grid for the B200 kernels. The scene
+ * stays resident across renders until the next upload. */
+lw_status lw_scene_upload(lw_ctx *ctx, const lw_scene_desc *scene);
+
+/* ---- rendering -----------------------------------------------------------------------------
+ * `Backend::render_hq` (crates/lumenwright/src/render/mod.rs:98-102) on the uploaded scene:
+ * `params` is the frame's `Params`, `sky` the frame's sky buffer (`HqFrame.sky`), `spp` the
+ * samples per pixel (at least 1). Writes the mean linear radiance per pixel, row-major, top row
+ * first, to `out_rgb` (frame[0] * frame[1] * 3 floats). Non-finite samples are left out of the
+ * sum and counted, as `pt_render` does (crates/lumenwright-ptx/src/lib.rs:76-84). The sums are
+ * Kahan-compensated FP32. */
+lw_status lw_render_hq(lw_ctx *ctx, const lw_params *params, const float *sky, uint64_t sky_len, uint32_t spp,
+                       lw_progress_fn progress, void *user, float *out_rgb);
+
+/* The same render with every buffer already on the device: the scene uploaded, the sky
+ * uploaded by lw_sky_upload, the result left in the context's device accumulator (read it with
+ * lw_read_accumulator). Samples [sample_start, sample_start + spp) are added to the
+ * accumulator; clear it with lw_clear_accumulator. No host copies happen inside. */
+lw_status lw_sky_upload(lw_ctx *ctx, const float *sky, uint64_t sky_len);
+lw_status lw_clear_accumulator(lw_ctx *ctx, uint32_t width, uint32_t height);
+lw_status lw_render_device(lw_ctx *ctx, const lw_params *params, uint32_t sample_start, uint32_t spp);
+lw_status lw_read_accumulator(lw_ctx *ctx, float *out_rgb);
+
+/* ---- parity entry points (the reference's kernel functions, one call per query) ----------
+ * Per-sample radiance of `render_sample` (crates/lumenwright-kernel/src/integrator.rs:539-709)
+ * for samples [sample_start, sample_start + count) of every pixel of the rectangle
+ * [x0, x0+w) x [y0, y0+h): out[((py*w + px) * count + k) * 3 + c]. */
+lw_status lw_render_samples(lw_ctx *ctx, const lw_params *params, uint32_t x0, uint32_t y0, uint32_t w,
+                            uint32_t h, uint32_t sample_start, uint32_t count, float *out);
+/* `trace` (crates/lumenwright-kernel/src/trace.rs:137-290) for n rays: o, d are 3n floats. */
+lw_status lw_trace_rays(lw_ctx *ctx, const lw_params *params, uint32_t n, const float *o, const float *d,
+                        float tmin, float tmax, lw_hit *out);
+/* `SceneView::voxel` (crates/lumenwright-kernel/src/scene.rs:271-284) on the re-laid grid, for n
+ * voxels given as 3n int32 coordinates. */
+lw_status lw_voxel_lookup(lw_ctx *ctx, uint32_t n, const int32_t *xyz, uint32_t *out);
+
+/* ---- sky precompute on the device -----------------------------------------------------------
+ * Chunky's sky cache for the sky in `params` (sky_sun, sky_zenith, perez_a..e) at resolution n:
+ * `build_sky_cache` (crates/lumenwright-kernel/src/integrator.rs:133-148), which the reference
+ * runs on the host per frame (crates/lumenwright/src/render/sky.rs:593-611). Writes (n+1)^2 * 3
+ * floats to `out`. */
+lw_status lw_build_sky_cache(lw_ctx *ctx, const lw_params *params, uint32_t n, float *out);
+/* `blend_chunky_sky` (crates/lumenwright/src/render/sky.rs:836-850): mixes Chunky's sky, read
+ * through `cache` at params->misc_f[2] as the kernel reads it, into the lens map then the light
+ * map in `maps` (sizes lens w, h, light w, h), in place: weight * chunky + (1 - weight) * map. */
+lw_status lw_blend_chunky_sky(lw_ctx *ctx, const lw_params *params, const float *cache, uint64_t cache_len,
+                              float *maps, const float sizes[4], float weight);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,644 @@
+// The C ABI (include/lumenwright_b200.h): contexts, scene upload and validation, the render
+// loop that replaces CudaBackend::render_hq (crates/lumenwright/src/render/cuda.rs:77-184), and
+// the parity entry points.
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/lumenwright_b200.h"
+#include "internal.h"
+
+using namespace lw;
+
+static_assert(sizeof(lw_params) == sizeof(DevParams), "Params layout");
+static_assert(sizeof(lw_quad) == 80 && sizeof(lw_model) == 16 && sizeof(lw_emitter) == 32, "record layout");
+
+namespace {
+
+thread_local std::string g_create_error;
+
+template <typename T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;  // elements allocated
+    void free_() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+// The reference's `gamma_to_linear` (crates/lumenwright-kernel/src/math.rs:183-216), exp(2.2 ln c)
+// with its own f32 `ln` and the platform expf, evaluated once per byte value on the host.
+float ref_ln(float x) {
+    if (x <= 0.0f) return x == 0.0f ? -INFINITY : NAN;
+    uint32_t bits;
+    std::memcpy(&bits, &x, 4);
+    int32_t e = (int32_t)((bits >> 23) & 0xFFu) - 127;
+    uint32_t mb = (bits & 0x007FFFFFu) | 0x3F800000u;
+    float m;
+    std::memcpy(&m, &mb, 4);
+    if (m > 1.41421356237309504880f) {
+        m *= 0.5f;
+        e += 1;
+    }
+    float s = (m - 1.0f) / (m + 1.0f);
+    float s2 = s * s;
+    float series = 2.0f * s * (1.0f + s2 * (1.0f / 3.0f + s2 * (1.0f / 5.0f + s2 * (1.0f / 7.0f + s2 * (1.0f / 9.0f)))));
+    return (float)e * 0.693147180559945309417f + series;
+}
+float ref_gamma_to_linear(float c) { return c <= 0.0f ? 0.0f : expf(2.2f * ref_ln(c)); }
+
+}  // namespace
+
+struct lw_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    LaunchShape shape_accum{}, shape_samples{};
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    cudaEvent_t marks[8] = {};
+    // scene
+    bool has_scene = false;
+    uint32_t dims[3] = {}, offsets[5] = {}, atlas_size[2] = {};
+    uint32_t nb = 0, n_bricks = 0, n_ov_bricks = 0;
+    DBuf<uint32_t> grid, atlas, egrid;
+    DBuf<uint2> top, occ;
+    DBuf<uint16_t> bricks;
+    DBuf<uint4> models;
+    DBuf<DevQuad> quads;
+    DBuf<float4> emitters;
+    uint64_t grid_len = 0, models_len = 0, quads_len = 0, atlas_len = 0, emitters_len = 0, egrid_len = 0;
+    // frame
+    DBuf<float> sky, gamma, out_rgb;
+    uint64_t sky_len = 0;
+    DBuf<Accum> acc;
+    uint32_t acc_w = 0, acc_h = 0;
+    DBuf<float4> partials;
+    DBuf<uint32_t> counter, error;
+    DBuf<float> samples;
+    DBuf<float> rays;
+    DBuf<uint8_t> hits;
+    DBuf<int32_t> xyz;
+    DBuf<uint32_t> vox;
+    int *cancel_host = nullptr, *cancel_dev = nullptr;
+    lw_stats stats{};
+    size_t partials_cap_bytes = size_t(4) << 30;
+};
+
+namespace {
+
+lw_status fail(lw_ctx *c, lw_status s, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->err = buf;
+    else g_create_error = buf;
+    return s;
+}
+
+lw_status cuda_fail(lw_ctx *c, cudaError_t e, const char *what) {
+    lw_status s = e == cudaErrorMemoryAllocation ? LW_ERR_OUT_OF_MEMORY : LW_ERR_LAUNCH;
+    return fail(c, s, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+#define CK(c, call, what)                                  \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
+    } while (0)
+
+template <typename T>
+cudaError_t ensure(DBuf<T> &b, size_t n) {
+    if (n == 0) n = 1;
+    if (b.n >= n) return cudaSuccess;
+    b.free_();
+    cudaError_t e = cudaMalloc(&b.p, n * sizeof(T));
+    if (e == cudaSuccess) b.n = n;
+    else b.p = nullptr;
+    return e;
+}
+
+template <typename T>
+cudaError_t upload(lw_ctx *c, DBuf<T> &b, const void *src, size_t n_elems, size_t elem_bytes) {
+    size_t bytes = n_elems * elem_bytes;
+    cudaError_t e = ensure(b, (bytes + sizeof(T) - 1) / sizeof(T));
+    if (e != cudaSuccess || bytes == 0) return e;
+    return cudaMemcpyAsync(b.p, src, bytes, cudaMemcpyHostToDevice, c->stream);
+}
+
+DevScene dev_scene(const lw_ctx *c) {
+    DevScene S;
+    S.top = c->top.p;
+    S.bricks = c->bricks.p;
+    S.occ = c->occ.p;
+    S.grid = c->grid.p;
+    S.models = c->models.p;
+    S.quads = c->quads.p;
+    S.atlas = c->atlas.p;
+    S.emitters = c->emitters.p;
+    S.emitter_grid = c->egrid.p;
+    S.sky = c->sky.p;
+    S.gamma = c->gamma.p;
+    return S;
+}
+
+// Checks a frame's Params against the uploaded scene and sky: every index the kernels form from
+// them stays inside its buffer.
+lw_status check_params(lw_ctx *c, const lw_params *p, bool need_frame) {
+    if (!p) return fail(c, LW_ERR_INVALID_ARGUMENT, "params is null");
+    if (!c->has_scene) return fail(c, LW_ERR_NO_SCENE, "no scene uploaded");
+    for (int a = 0; a < 3; a++)
+        if (p->grid_dims[a] != c->dims[a])
+            return fail(c, LW_ERR_INVALID_ARGUMENT, "params.grid_dims[%d] = %u, the scene has %u", a, p->grid_dims[a], c->dims[a]);
+    for (int a = 0; a < 4; a++)
+        if (p->off[a] != c->offsets[a])
+            return fail(c, LW_ERR_INVALID_ARGUMENT, "params.off[%d] = %u, the scene has %u", a, p->off[a], c->offsets[a]);
+    if (p->off2[0] != c->offsets[4] || p->off2[1] != c->atlas_size[0] || p->off2[2] != c->atlas_size[1])
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "params.off2 does not match the scene (ov_quads offset, atlas size)");
+    if (need_frame && (p->frame[0] == 0 || p->frame[1] == 0))
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "frame size %ux%u", p->frame[0], p->frame[1]);
+    if ((uint64_t)p->see_through[0] + p->see_through[1] > c->quads_len)
+        return fail(c, LW_ERR_BUFFER_LENGTH, "see-through quads [%u, +%u) outside %llu quads", p->see_through[0],
+                    p->see_through[1], (unsigned long long)c->quads_len);
+    if (p->sky_map[0] >= 1.0f) {
+        double lens = (double)(uint64_t)p->sky_map[0] * (uint64_t)p->sky_map[1];
+        double light = (double)(uint64_t)p->sky_map[2] * (uint64_t)p->sky_map[3];
+        if (!(p->sky_map[1] >= 1.0f && p->sky_map[2] >= 1.0f && p->sky_map[3] >= 1.0f) ||
+            (lens + light) * 3.0 > (double)c->sky_len || p->sky_map[0] * p->sky_map[1] >= 4294967040.0f)
+            return fail(c, LW_ERR_BUFFER_LENGTH, "sky maps %gx%g + %gx%g need more than the %llu sky floats", p->sky_map[0],
+                        p->sky_map[1], p->sky_map[2], p->sky_map[3], (unsigned long long)c->sky_len);
+    } else if (p->misc_f[2] >= 1.0f) {
+        double n = std::floor((double)p->misc_f[2]);
+        if ((n + 1.0) * (n + 1.0) * 3.0 > (double)c->sky_len)
+            return fail(c, LW_ERR_BUFFER_LENGTH, "sky cache of resolution %g needs %g floats, %llu given", n,
+                        (n + 1.0) * (n + 1.0) * 3.0, (unsigned long long)c->sky_len);
+    }
+    return LW_OK;
+}
+
+DevParams dev_params(const lw_params *p) {
+    DevParams d;
+    std::memcpy(&d, p, sizeof d);
+    return d;
+}
+
+// Splits [sample_start, sample_start + spp) over a rectangle into launches whose partial sums fit
+// the context's buffer; `sub` samples per item, chosen so each lane gets many items.
+struct Plan {
+    uint32_t sub, batch;
+};
+Plan plan(const lw_ctx *c, uint64_t n_slots, uint32_t spp) {
+    uint64_t lanes = (uint64_t)c->shape_accum.blocks * c->shape_accum.threads;
+    uint64_t total = n_slots * spp;
+    uint64_t sub = total / (lanes * 16ull + 1ull);
+    sub = sub < 1 ? 1 : (sub > 16 ? 16 : sub);
+    uint64_t max_items = c->partials_cap_bytes / sizeof(float4);
+    uint64_t max_sub_per_launch = max_items / (n_slots ? n_slots : 1);
+    if (max_sub_per_launch < 1) max_sub_per_launch = 1;
+    uint64_t batch = max_sub_per_launch * sub;
+    if (batch > spp) batch = spp;
+    return Plan{(uint32_t)sub, (uint32_t)batch};
+}
+
+WorkDesc work(lw_ctx *c, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t spp, uint32_t sub) {
+    WorkDesc W{};
+    W.x0 = x0;
+    W.y0 = y0;
+    W.w = w;
+    W.h = h;
+    W.tiles_x = (w + 7) / 8;
+    uint32_t tiles_y = (h + 3) / 4;
+    W.n_slots = W.tiles_x * tiles_y * 32u;
+    W.sample_start = s0;
+    W.spp = spp;
+    W.sub = sub;
+    W.n_sub = (spp + sub - 1) / sub;
+    W.n_items = W.n_slots * W.n_sub;
+    W.counter = c->counter.p;
+    W.partials = c->partials.p;
+    W.samples_out = c->samples.p;
+    W.cancel = c->cancel_dev;
+    return W;
+}
+
+lw_status ensure_accum(lw_ctx *c, uint32_t w, uint32_t h) {
+    CK(c, ensure(c->acc, (size_t)w * h), "allocating the accumulator");
+    c->acc_w = w;
+    c->acc_h = h;
+    return LW_OK;
+}
+
+// Launches the accumulating render of samples [s0, s0 + spp) over the whole frame, in batches.
+// With `progress`, each batch is waited for and reported; without it nothing waits.
+lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32_t spp, lw_progress_fn progress,
+                         void *user, uint32_t progress_total) {
+    const uint32_t w = params->frame[0], h = params->frame[1];
+    WorkDesc probe = work(c, 0, 0, w, h, 0, 1, 1);
+    Plan pl = plan(c, probe.n_slots, spp);
+    CK(c, ensure(c->partials, (size_t)probe.n_slots * ((pl.batch + pl.sub - 1) / pl.sub)), "allocating partial sums");
+    DevScene S = dev_scene(c);
+    DevParams P = dev_params(params);
+    uint32_t done = 0;
+    while (done < spp) {
+        uint32_t n = spp - done < pl.batch ? spp - done : pl.batch;
+        WorkDesc W = work(c, 0, 0, w, h, s0 + done, n, pl.sub);
+        CK(c, cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream), "clearing the work counter");
+        CK(c, cudaEventRecord(c->ev_a, c->stream), "recording an event");
+        CK(c, launch_render(MODE_ACCUM, S, P, W, c->shape_accum, c->stream), "launching the render kernel");
+        CK(c, cudaEventRecord(c->ev_b, c->stream), "recording an event");
+        CK(c, launch_reduce(W, c->acc.p, w, c->stream), "launching the reduction");
+        c->stats.launches++;
+        c->stats.samples += (uint64_t)w * h * n;
+        done += n;
+        if (progress || done < spp) {
+            CK(c, cudaEventSynchronize(c->ev_b), "waiting for the render kernel");
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, c->ev_a, c->ev_b);
+            c->stats.kernel_ms += ms;
+            if (progress) progress(done, progress_total, user);
+            if (__atomic_load_n(c->cancel_host, __ATOMIC_RELAXED))
+                return fail(c, LW_ERR_CANCELLED, "cancelled after %u of %u samples", done, spp);
+        } else {
+            c->stats.kernel_ms = -1.0;  // read by lw_get_stats once the last launch is done
+        }
+    }
+    return LW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+lw_status lw_ctx_create(int device, lw_ctx **out) {
+    if (!out) return fail(nullptr, LW_ERR_INVALID_ARGUMENT, "out is null");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return fail(nullptr, LW_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= n) return fail(nullptr, LW_ERR_NO_DEVICE, "device %d of %d", device, n);
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    if (prop.major != 10) return fail(nullptr, LW_ERR_NO_DEVICE, "device %d (%s) is sm_%d%d; this library is built for sm_100a", device, prop.name, prop.major, prop.minor);
+    lw_ctx *c = new lw_ctx();
+    c->device = device;
+    auto bail = [&](cudaError_t e, const char *what) {
+        g_create_error = std::string(what) + ": " + cudaGetErrorString(e);
+        lw_ctx_destroy(c);
+        return e == cudaErrorMemoryAllocation ? LW_ERR_OUT_OF_MEMORY : LW_ERR_LAUNCH;
+    };
+    cudaError_t e;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return bail(e, "cudaSetDevice");
+    if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "creating a stream");
+    if ((e = cudaEventCreate(&c->ev_a)) != cudaSuccess || (e = cudaEventCreate(&c->ev_b)) != cudaSuccess)
+        return bail(e, "creating events");
+    for (auto &m : c->marks)
+        if ((e = cudaEventCreate(&m)) != cudaSuccess) return bail(e, "creating events");
+    if ((e = cudaHostAlloc(&c->cancel_host, sizeof(int), cudaHostAllocMapped)) != cudaSuccess) return bail(e, "allocating the cancel flag");
+    *c->cancel_host = 0;
+    if ((e = cudaHostGetDevicePointer(&c->cancel_dev, c->cancel_host, 0)) != cudaSuccess) return bail(e, "mapping the cancel flag");
+    float lut[256];
+    for (int k = 0; k < 256; k++) lut[k] = ref_gamma_to_linear((float)k / 255.0f);
+    if ((e = ensure(c->gamma, 256)) != cudaSuccess) return bail(e, "allocating the gamma table");
+    if ((e = cudaMemcpy(c->gamma.p, lut, sizeof lut, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "uploading the gamma table");
+    if ((e = ensure(c->counter, 1)) != cudaSuccess || (e = ensure(c->error, 1)) != cudaSuccess) return bail(e, "allocating counters");
+    c->shape_accum = render_shape(MODE_ACCUM, device);
+    c->shape_samples = render_shape(MODE_SAMPLES, device);
+    *out = c;
+    return LW_OK;
+}
+
+void lw_ctx_destroy(lw_ctx *c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto *b : {&c->grid, &c->atlas, &c->egrid, &c->counter, &c->error, &c->vox}) b->free_();
+    c->top.free_();
+    c->occ.free_();
+    c->bricks.free_();
+    c->models.free_();
+    c->quads.free_();
+    c->emitters.free_();
+    c->partials.free_();
+    for (auto *b : {&c->sky, &c->gamma, &c->out_rgb, &c->samples, &c->rays}) b->free_();
+    c->acc.free_();
+    c->hits.free_();
+    c->xyz.free_();
+    if (c->cancel_host) cudaFreeHost(c->cancel_host);
+    if (c->ev_a) cudaEventDestroy(c->ev_a);
+    if (c->ev_b) cudaEventDestroy(c->ev_b);
+    for (auto m : c->marks)
+        if (m) cudaEventDestroy(m);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char *lw_last_error(const lw_ctx *c) { return c ? c->err.c_str() : g_create_error.c_str(); }
+
+void *lw_stream(lw_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+void lw_cancel(lw_ctx *c) {
+    if (c && c->cancel_host) __atomic_store_n(c->cancel_host, 1, __ATOMIC_RELAXED);
+}
+
+lw_status lw_mark(lw_ctx *c, uint32_t slot) {
+    if (!c || slot >= 8) return fail(c, LW_ERR_INVALID_ARGUMENT, "mark slot %u", slot);
+    cudaSetDevice(c->device);
+    CK(c, cudaEventRecord(c->marks[slot], c->stream), "recording a mark");
+    return LW_OK;
+}
+
+lw_status lw_elapsed_ms(lw_ctx *c, uint32_t from, uint32_t to, double *ms) {
+    if (!c || !ms || from >= 8 || to >= 8) return fail(c, LW_ERR_INVALID_ARGUMENT, "bad mark");
+    cudaSetDevice(c->device);
+    CK(c, cudaEventSynchronize(c->marks[to]), "waiting for a mark");
+    float f = 0.f;
+    CK(c, cudaEventElapsedTime(&f, c->marks[from], c->marks[to]), "reading marks");
+    *ms = f;
+    return LW_OK;
+}
+
+lw_status lw_get_stats(const lw_ctx *cc, lw_stats *out) {
+    lw_ctx *c = const_cast<lw_ctx *>(cc);
+    if (!c || !out) return LW_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    if (c->stats.kernel_ms < 0.0) {
+        if (cudaEventSynchronize(c->ev_b) != cudaSuccess) return LW_ERR_LAUNCH;
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev_a, c->ev_b);
+        c->stats.kernel_ms = ms;
+    }
+    *out = c->stats;
+    out->blocks = (uint32_t)c->shape_accum.blocks;
+    out->threads = (uint32_t)c->shape_accum.threads;
+    return LW_OK;
+}
+
+lw_status lw_scene_upload(lw_ctx *c, const lw_scene_desc *d) {
+    if (!c || !d) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(c->device);
+    auto t0 = std::chrono::steady_clock::now();
+    c->has_scene = false;
+    if (!d->grid || !d->models || !d->quads || !d->atlas || !d->emitters || !d->emitter_grid)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "a scene buffer is null");
+    if (!d->models_len || !d->quads_len || !d->emitters_len)
+        return fail(c, LW_ERR_BUFFER_LENGTH, "models, quads and emitters hold at least one entry each");
+    const uint64_t nb = (uint64_t)d->dims[0] * d->dims[1] * d->dims[2];
+    if (nb == 0 || nb > 0x7FFFFFFFull) return fail(c, LW_ERR_INVALID_ARGUMENT, "grid of %ux%ux%u bricks", d->dims[0], d->dims[1], d->dims[2]);
+    if ((uint64_t)d->dims[0] * 16 > 0x7FFFFFF || (uint64_t)d->dims[1] * 16 > 0x7FFFFFF || (uint64_t)d->dims[2] * 16 > 0x7FFFFFF)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "grid too large");
+    const uint32_t *o = d->offsets;
+    if (o[0] + nb > d->grid_len || o[2] + nb > d->grid_len)
+        return fail(c, LW_ERR_BUFFER_LENGTH, "top or ov_top entries outside the %llu grid words", (unsigned long long)d->grid_len);
+    if (o[1] > o[2] || (o[2] - o[1]) % 2048u != 0 || o[3] > o[4] || (o[4] - o[3]) % 8192u != 0 || o[4] > d->grid_len || o[3] < o[2] + nb)
+        return fail(c, LW_ERR_BUFFER_LENGTH, "grid offsets %u %u %u %u %u are not [top | bricks | ov_top | ov_cells | ov_quads]", o[0], o[1], o[2], o[3], o[4]);
+    const uint32_t n_bricks = (o[2] - o[1]) / 2048u, n_ov = (o[4] - o[3]) / 8192u;
+    const uint64_t ovq_len = d->grid_len - o[4];
+    // Cross-buffer indices the kernels follow (the reference's slice bounds checks).
+    for (uint64_t i = 0; i < d->models_len; i++)
+        if ((uint64_t)d->models[i].quad_offset + d->models[i].quad_count > d->quads_len)
+            return fail(c, LW_ERR_BUFFER_LENGTH, "model %llu's quads [%u, +%u) outside %llu quads", (unsigned long long)i,
+                        d->models[i].quad_offset, d->models[i].quad_count, (unsigned long long)d->quads_len);
+    for (uint64_t i = 0; i < d->emitters_len; i++) {
+        uint32_t first;
+        std::memcpy(&first, &d->emitters[i].pos[3], 4);
+        if ((uint64_t)first + d->emitters[i].faces[0] > d->quads_len)
+            return fail(c, LW_ERR_BUFFER_LENGTH, "emitter %llu's faces outside the quads", (unsigned long long)i);
+    }
+    if (d->emitter_grid_len < 8) return fail(c, LW_ERR_BUFFER_LENGTH, "emitter grid shorter than its header");
+    {
+        const uint32_t *g = d->emitter_grid;
+        uint64_t cells = (uint64_t)g[1] * g[2] * g[3];
+        if (8 + 2 * cells > d->emitter_grid_len) return fail(c, LW_ERR_BUFFER_LENGTH, "emitter grid cells outside the buffer");
+        uint64_t list_len = d->emitter_grid_len - 8 - 2 * cells;
+        for (uint64_t k = 0; k < cells; k++)
+            if ((uint64_t)g[8 + 2 * k] + g[9 + 2 * k] > list_len)
+                return fail(c, LW_ERR_BUFFER_LENGTH, "emitter grid cell %llu's list outside the buffer", (unsigned long long)k);
+        for (uint64_t k = 0; k < list_len; k++)
+            if (g[8 + 2 * cells + k] >= d->emitters_len)
+                return fail(c, LW_ERR_BUFFER_LENGTH, "emitter grid names emitter %u of %llu", g[8 + 2 * cells + k], (unsigned long long)d->emitters_len);
+    }
+    for (uint64_t k = 0; k < (uint64_t)n_ov * 4096u; k++) {
+        uint64_t off = d->grid[o[3] + 2 * k], cnt = d->grid[o[3] + 2 * k + 1];
+        if (off + cnt > ovq_len) return fail(c, LW_ERR_BUFFER_LENGTH, "overlay cell %llu's quads outside ov_quads", (unsigned long long)k);
+    }
+    for (uint64_t k = 0; k < (uint64_t)n_ov * 4096u; k++) {
+        uint64_t off = d->grid[o[3] + 2 * k], cnt = d->grid[o[3] + 2 * k + 1];
+        for (uint64_t i = 0; i < cnt; i++)
+            if (d->grid[o[4] + off + i] >= d->quads_len) return fail(c, LW_ERR_BUFFER_LENGTH, "an overlay cell names a quad out of range");
+    }
+    if ((uint64_t)d->atlas_size[0] * d->atlas_size[1] > d->atlas_len || d->atlas_size[0] == 0 || d->atlas_size[1] == 0)
+        return fail(c, LW_ERR_BUFFER_LENGTH, "atlas %ux%u needs more than %llu texels", d->atlas_size[0], d->atlas_size[1], (unsigned long long)d->atlas_len);
+
+    CK(c, upload(c, c->grid, d->grid, d->grid_len, 4), "uploading the grid");
+    CK(c, upload(c, c->models, d->models, d->models_len, 16), "uploading the models");
+    CK(c, upload(c, c->atlas, d->atlas, d->atlas_len, 4), "uploading the atlas");
+    CK(c, upload(c, c->emitters, d->emitters, d->emitters_len, 32), "uploading the emitters");
+    CK(c, upload(c, c->egrid, d->emitter_grid, d->emitter_grid_len, 4), "uploading the emitter grid");
+    DBuf<uint8_t> ref_quads;
+    CK(c, upload(c, ref_quads, d->quads, d->quads_len, 80), "uploading the quads");
+    CK(c, ensure(c->quads, d->quads_len), "allocating the quads");
+    CK(c, launch_quads(ref_quads.p, c->quads.p, (uint32_t)d->quads_len, c->stream), "re-laying the quads");
+    CK(c, ensure(c->top, nb), "allocating the top level");
+    CK(c, ensure(c->bricks, (size_t)n_bricks * 4096u), "allocating the bricks");
+    CK(c, ensure(c->occ, n_bricks), "allocating the occupancy masks");
+    CK(c, cudaMemsetAsync(c->error.p, 0, 4, c->stream), "clearing the error word");
+    SceneUploadDesc u{c->grid.p, (uint32_t)nb, n_bricks, o[0], o[1], o[2], (uint32_t)d->models_len, n_ov,
+                      c->top.p, c->bricks.p, c->occ.p, c->error.p};
+    CK(c, launch_relayout(u, c->stream), "re-laying the grid");
+    uint32_t err = 0;
+    CK(c, cudaMemcpyAsync(&err, c->error.p, 4, cudaMemcpyDeviceToHost, c->stream), "reading the error word");
+    CK(c, cudaStreamSynchronize(c->stream), "uploading the scene");
+    ref_quads.free_();
+    if (err & 1u) return fail(c, LW_ERR_BUFFER_LENGTH, "a top-level entry names a brick, model or overlay brick out of range");
+    if (err & 2u) return fail(c, LW_ERR_BUFFER_LENGTH, "a voxel names a model out of range");
+    std::memcpy(c->dims, d->dims, sizeof c->dims);
+    std::memcpy(c->offsets, d->offsets, sizeof c->offsets);
+    std::memcpy(c->atlas_size, d->atlas_size, sizeof c->atlas_size);
+    c->nb = (uint32_t)nb;
+    c->n_bricks = n_bricks;
+    c->n_ov_bricks = n_ov;
+    c->grid_len = d->grid_len;
+    c->models_len = d->models_len;
+    c->quads_len = d->quads_len;
+    c->atlas_len = d->atlas_len;
+    c->emitters_len = d->emitters_len;
+    c->egrid_len = d->emitter_grid_len;
+    c->has_scene = true;
+    c->stats.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return LW_OK;
+}
+
+lw_status lw_sky_upload(lw_ctx *c, const float *sky, uint64_t sky_len) {
+    if (!c) return LW_ERR_INVALID_ARGUMENT;
+    if (sky_len && !sky) return fail(c, LW_ERR_INVALID_ARGUMENT, "sky is null");
+    cudaSetDevice(c->device);
+    CK(c, upload(c, c->sky, sky, sky_len, 4), "uploading the sky");
+    c->sky_len = sky_len;
+    return LW_OK;
+}
+
+lw_status lw_clear_accumulator(lw_ctx *c, uint32_t w, uint32_t h) {
+    if (!c || !w || !h) return fail(c, LW_ERR_INVALID_ARGUMENT, "bad frame size");
+    cudaSetDevice(c->device);
+    lw_status s = ensure_accum(c, w, h);
+    if (s != LW_OK) return s;
+    CK(c, cudaMemsetAsync(c->acc.p, 0, sizeof(Accum) * (size_t)w * h, c->stream), "clearing the accumulator");
+    return LW_OK;
+}
+
+lw_status lw_render_device(lw_ctx *c, const lw_params *params, uint32_t sample_start, uint32_t spp) {
+    if (!c) return LW_ERR_INVALID_ARGUMENT;
+    cudaSetDevice(c->device);
+    lw_status s = check_params(c, params, true);
+    if (s != LW_OK) return s;
+    if (c->acc_w != params->frame[0] || c->acc_h != params->frame[1])
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "the accumulator is %ux%u, the frame %ux%u", c->acc_w, c->acc_h, params->frame[0], params->frame[1]);
+    if (spp == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "spp is 0");
+    __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
+    c->stats.launches = 0;
+    c->stats.samples = 0;
+    c->stats.kernel_ms = 0;
+    return render_batches(c, params, sample_start, spp, nullptr, nullptr, spp);
+}
+
+lw_status lw_read_accumulator(lw_ctx *c, float *out_rgb) {
+    if (!c || !out_rgb) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(c->device);
+    size_t n = (size_t)c->acc_w * c->acc_h;
+    if (!n) return fail(c, LW_ERR_INVALID_ARGUMENT, "no accumulator");
+    CK(c, ensure(c->out_rgb, 3 * n), "allocating the output");
+    CK(c, launch_finalize(c->acc.p, (uint32_t)n, c->out_rgb.p, c->stream), "launching the finalize kernel");
+    CK(c, cudaMemcpyAsync(out_rgb, c->out_rgb.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "reading the image");
+    CK(c, cudaStreamSynchronize(c->stream), "reading the image");
+    return LW_OK;
+}
+
+lw_status lw_render_hq(lw_ctx *c, const lw_params *params, const float *sky, uint64_t sky_len, uint32_t spp,
+                       lw_progress_fn progress, void *user, float *out_rgb) {
+    if (!c || !out_rgb) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(c->device);
+    if (spp < 1) spp = 1;  // `f.spp.max(1)` (cuda.rs:85)
+    lw_status s = lw_sky_upload(c, sky, sky_len);
+    if (s != LW_OK) return s;
+    s = check_params(c, params, true);
+    if (s != LW_OK) return s;
+    s = lw_clear_accumulator(c, params->frame[0], params->frame[1]);
+    if (s != LW_OK) return s;
+    __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
+    c->stats.launches = 0;
+    c->stats.samples = 0;
+    c->stats.kernel_ms = 0;
+    s = render_batches(c, params, 0, spp, progress, user, spp);
+    if (s != LW_OK) return s;
+    return lw_read_accumulator(c, out_rgb);
+}
+
+lw_status lw_render_samples(lw_ctx *c, const lw_params *params, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                            uint32_t sample_start, uint32_t count, float *out) {
+    if (!c || !out || !w || !h || !count) return fail(c, LW_ERR_INVALID_ARGUMENT, "bad argument");
+    cudaSetDevice(c->device);
+    lw_status s = check_params(c, params, true);
+    if (s != LW_OK) return s;
+    if ((uint64_t)x0 + w > params->frame[0] || (uint64_t)y0 + h > params->frame[1])
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "rectangle outside the frame");
+    size_t n = (size_t)w * h * count * 3;
+    CK(c, ensure(c->samples, n), "allocating the samples");
+    WorkDesc W = work(c, x0, y0, w, h, sample_start, count, 1);
+    W.samples_out = c->samples.p;
+    __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
+    CK(c, cudaMemsetAsync(c->counter.p, 0, 4, c->stream), "clearing the work counter");
+    CK(c, launch_render(MODE_SAMPLES, dev_scene(c), dev_params(params), W, c->shape_samples, c->stream), "launching the render kernel");
+    CK(c, cudaMemcpyAsync(out, c->samples.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "reading the samples");
+    CK(c, cudaStreamSynchronize(c->stream), "rendering samples");
+    return LW_OK;
+}
+
+lw_status lw_trace_rays(lw_ctx *c, const lw_params *params, uint32_t n, const float *o, const float *d, float tmin,
+                        float tmax, lw_hit *out) {
+    if (!c || !o || !d || !out || !n) return fail(c, LW_ERR_INVALID_ARGUMENT, "bad argument");
+    cudaSetDevice(c->device);
+    lw_status s = check_params(c, params, false);
+    if (s != LW_OK) return s;
+    CK(c, ensure(c->rays, (size_t)6 * n), "allocating rays");
+    CK(c, ensure(c->hits, sizeof(lw_hit) * (size_t)n), "allocating hits");
+    CK(c, cudaMemcpyAsync(c->rays.p, o, 12 * (size_t)n, cudaMemcpyHostToDevice, c->stream), "uploading rays");
+    CK(c, cudaMemcpyAsync(c->rays.p + 3 * (size_t)n, d, 12 * (size_t)n, cudaMemcpyHostToDevice, c->stream), "uploading rays");
+    CK(c, launch_trace_rays(dev_scene(c), dev_params(params), n, c->rays.p, c->rays.p + 3 * (size_t)n, tmin, tmax, c->hits.p, c->stream),
+       "launching the trace kernel");
+    CK(c, cudaMemcpyAsync(out, c->hits.p, sizeof(lw_hit) * (size_t)n, cudaMemcpyDeviceToHost, c->stream), "reading hits");
+    CK(c, cudaStreamSynchronize(c->stream), "tracing rays");
+    return LW_OK;
+}
+
+lw_status lw_voxel_lookup(lw_ctx *c, uint32_t n, const int32_t *xyz, uint32_t *out) {
+    if (!c || !xyz || !out || !n) return fail(c, LW_ERR_INVALID_ARGUMENT, "bad argument");
+    if (!c->has_scene) return fail(c, LW_ERR_NO_SCENE, "no scene uploaded");
+    cudaSetDevice(c->device);
+    for (uint32_t i = 0; i < n; i++)
+        for (int a = 0; a < 3; a++)
+            if (xyz[3 * i + a] < 0 || (uint32_t)xyz[3 * i + a] >= c->dims[a] * 16u)
+                return fail(c, LW_ERR_INVALID_ARGUMENT, "voxel %u outside the grid", i);
+    lw_params p{};
+    std::memcpy(p.grid_dims, c->dims, sizeof c->dims);
+    CK(c, ensure(c->xyz, (size_t)3 * n), "allocating coordinates");
+    CK(c, ensure(c->vox, n), "allocating ids");
+    CK(c, cudaMemcpyAsync(c->xyz.p, xyz, 12 * (size_t)n, cudaMemcpyHostToDevice, c->stream), "uploading coordinates");
+    CK(c, launch_voxel_lookup(dev_scene(c), dev_params(&p), n, c->xyz.p, c->vox.p, c->stream), "launching the lookup kernel");
+    CK(c, cudaMemcpyAsync(out, c->vox.p, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream), "reading ids");
+    CK(c, cudaStreamSynchronize(c->stream), "looking up voxels");
+    return LW_OK;
+}
+
+lw_status lw_build_sky_cache(lw_ctx *c, const lw_params *params, uint32_t n, float *out) {
+    if (!c || !params || !out || n == 0 || n > 8192) return fail(c, LW_ERR_INVALID_ARGUMENT, "bad argument");
+    cudaSetDevice(c->device);
+    size_t cnt = (size_t)(n + 1) * (n + 1) * 3;
+    DBuf<float> buf;
+    CK(c, ensure(buf, cnt), "allocating the sky cache");
+    cudaError_t e = launch_sky_cache(dev_params(params), n, buf.p, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, buf.p, cnt * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    buf.free_();
+    if (e != cudaSuccess) return cuda_fail(c, e, "building the sky cache");
+    return LW_OK;
+}
+
+lw_status lw_blend_chunky_sky(lw_ctx *c, const lw_params *params, const float *cache, uint64_t cache_len, float *maps,
+                              const float sizes[4], float weight) {
+    if (!c || !params || !cache || !maps || !sizes) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(c->device);
+    double n = std::floor((double)params->misc_f[2]);
+    if (n < 1.0 || (n + 1.0) * (n + 1.0) * 3.0 > (double)cache_len)
+        return fail(c, LW_ERR_BUFFER_LENGTH, "the sky cache does not hold resolution %g", n);
+    uint32_t lw_ = (uint32_t)sizes[0], lh = (uint32_t)sizes[1], gw = (uint32_t)sizes[2], gh = (uint32_t)sizes[3];
+    if (!lw_ || !lh || !gw || !gh) return fail(c, LW_ERR_INVALID_ARGUMENT, "empty map");
+    size_t nmap = ((size_t)lw_ * lh + (size_t)gw * gh) * 3;
+    DBuf<float> cbuf, mbuf;
+    CK(c, ensure(cbuf, cache_len), "allocating the sky cache");
+    if (ensure(mbuf, nmap) != cudaSuccess) {
+        cbuf.free_();
+        return fail(c, LW_ERR_OUT_OF_MEMORY, "allocating the maps");
+    }
+    cudaError_t e = cudaMemcpyAsync(cbuf.p, cache, cache_len * 4, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(mbuf.p, maps, nmap * 4, cudaMemcpyHostToDevice, c->stream);
+    DevScene S = dev_scene(c);
+    S.sky = cbuf.p;
+    DevParams P = dev_params(params);
+    if (e == cudaSuccess) e = launch_blend_chunky(S, P, mbuf.p, lw_, lh, weight, c->stream);
+    if (e == cudaSuccess) e = launch_blend_chunky(S, P, mbuf.p + (size_t)lw_ * lh * 3, gw, gh, weight, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(maps, mbuf.p, nmap * 4, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cbuf.free_();
+    mbuf.free_();
+    if (e != cudaSuccess) return cuda_fail(c, e, "blending the sky maps");
+    return LW_OK;
+}
+
+}  // extern "C"

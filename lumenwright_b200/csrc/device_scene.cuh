@@ -1,0 +1,300 @@
+// The scene as the B200 kernels read it, and the reference's traversal on it.
+//
+// Layout in HBM (built by lw_scene_upload from the reference's `HqScene` buffers):
+//   top     uint2[nb]            (top entry, overlay entry) per brick: one 8-byte load per brick
+//                                where the reference reads two words (trace.rs:181-182)
+//   bricks  uint16[n * 4096]     the voxel ids of each non-uniform brick, 4x4x4-sub-block-major:
+//                                sub-block ((y>>2)*4 + (z>>2))*4 + (x>>2), then ((y&3)*4+(z&3))*4+(x&3)
+//                                inside it, so one sub-block is one 128-byte line
+//   occ     uint2[n]             a 64-bit mask per non-uniform brick: bit s set when sub-block s
+//                                holds a voxel whose model is not 0 (air)
+//   quads   DevQuad[q]           96-byte records with the normal eu x ev and |n|^2 precomputed
+//   grid    uint32[]             the reference's grid, read for the overlay cells and ov_quads
+//   models, atlas, emitters, emitter_grid, sky: the reference's buffers unchanged
+//   gamma   float[256]           gamma_to_linear(k / 255) for every byte k (math.rs:214-216)
+#pragma once
+
+#include "device_math.cuh"
+
+namespace lw {
+
+constexpr uint32_t EMPTY = 0xFFFFFFFFu;
+constexpr uint32_t UNIFORM = 0x80000000u;
+constexpr uint32_t OV_CELL_WORDS = 8192u;
+constexpr uint32_t ALPHA_CUTOUT = 1u;
+constexpr uint32_t ALPHA_TRANSLUCENT = 2u;
+constexpr uint32_t FLAG_ALPHA_MASK = 3u;
+constexpr uint32_t FLAG_WATER = 4u;
+constexpr uint32_t FLAG_FRONT_ONLY = 16u;
+constexpr uint32_t EMITTER_SAMPLING_NONE = 0u;
+constexpr uint32_t EMITTER_SAMPLING_ONE = 1u;
+constexpr uint32_t EMITTER_SAMPLING_ONE_BLOCK = 2u;
+constexpr uint32_t EMITTER_SAMPLING_ALL = 3u;
+constexpr uint32_t EMITTER_GRID_HEADER = 8u;
+constexpr uint32_t MAX_STEPS = 65536u;  // trace.rs:31
+constexpr uint32_t MAX_EVENTS = 48u;    // integrator.rs:24
+constexpr uint32_t NO_QUAD = 0xFFFFFFFFu;
+constexpr float COPLANAR = 1e-5f;       // trace.rs:73
+
+struct __align__(16) DevQuad {
+    float4 n_nn;      // n = eu x ev, w = n . n
+    float4 p0_flags;  // p0, w = flags (bit cast)
+    float4 eu_tint;   // eu, w = tint (bit cast)
+    float4 ev_em;     // ev, w = emittance
+    float4 uv;        // uv0.xy, uvs.xy
+    float4 uvt;       // uvt.xy, 0, 0
+};
+static_assert(sizeof(DevQuad) == 96, "DevQuad is 96 bytes");
+
+// The frame parameters as the kernels use them (a copy of `Params` plus derived values).
+struct __align__(16) DevParams {
+    float4 cam_pos, cam_fwd, cam_right, cam_up, sun_dir, sun_color, sky_sun, sky_zenith;
+    float4 perez_a, perez_b, perez_c, perez_d, perez_e, water_color, misc_f;
+    uint4 grid_dims, off, off2, frame, misc_u, see_through, emitter;
+    float4 sun_su, sun_sv, sun_sprite, sky_map, water_plane;
+};
+static_assert(sizeof(DevParams) == 432, "Params is 432 bytes");
+
+struct DevScene {
+    const uint2 *top;
+    const uint16_t *bricks;
+    const uint2 *occ;
+    const uint32_t *grid;
+    const uint4 *models;
+    const DevQuad *quads;
+    const uint32_t *atlas;
+    const float4 *emitters;  // two float4 per emitter: (offset, first quad), (faces, -, -, -)
+    const uint32_t *emitter_grid;
+    const float *sky;
+    const float *gamma;
+};
+
+template <typename T>
+LW_DI T ldg(const T *p) { return __ldg(p); }
+
+struct Hit {
+    float t;
+    uint32_t quad, texel;
+    float s, tt;
+};
+LW_DI Hit no_hit() { return Hit{kINF, NO_QUAD, 0u, 0.0f, 0.0f}; }
+
+// SceneView::texel (scene.rs:288-294).
+LW_DI uint32_t texel(const DevScene &S, const DevParams &P, float u, float v) {
+    int w = (int)P.off2.y, h = (int)P.off2.z;
+    int x = clamp_i(to_i32(floorf(u)), 0, w - 1);
+    int y = clamp_i(to_i32(floorf(v)), 0, h - 1);
+    return ldg(S.atlas + (uint32_t)(y * w + x));
+}
+
+// linear_rgb (integrator.rs:27-34) through the byte table.
+LW_DI V3 linear_rgb(const float *gamma, uint32_t c) {
+    return v3(gamma[c & 0xFFu], gamma[(c >> 8) & 0xFFu], gamma[(c >> 16) & 0xFFu]);
+}
+
+// test_quad (trace.rs:81-109) with intersect_quad (:37-58) and quad_texel (:62-69). The normal
+// eu x ev and n . n come precomputed; a front-only quad met from behind is rejected before the
+// division instead of after it: `normal() . d` is exactly `-(n . d)`, and intersect_quad has no
+// side effects, so the outcome is the reference's.
+LW_DI void test_quad(const DevScene &S, const DevParams &P, uint32_t qi, V3 o, V3 d, float tmin, Hit &best) {
+    const DevQuad *q = S.quads + qi;
+    float reach = (best.quad != NO_QUAD && qi > best.quad) ? best.t + COPLANAR : best.t;
+    float4 a = ldg(&q->n_nn);
+    V3 n = f4v(a);
+    float denom = dot(n, d);
+    if (fabs_r(denom) < 1e-12f) return;
+    float4 b = ldg(&q->p0_flags);
+    uint32_t flags = __float_as_uint(b.w);
+    if ((flags & FLAG_FRONT_ONLY) && -denom >= 0.0f) return;
+    V3 p0 = f4v(b);
+    float t = __fdiv_rn(dot(n, p0 - o), denom);
+    if (!(t > tmin && t < reach)) return;
+    V3 eu = f4v(ldg(&q->eu_tint));
+    V3 ev = f4v(ldg(&q->ev_em));
+    V3 p = (o + d * t) - p0;
+    float nn = a.w;
+    float s = __fdiv_rn(dot(cross(p, ev), n), nn);
+    float tt = __fdiv_rn(dot(cross(eu, p), n), nn);
+    if (s < 0.0f || s > 1.0f || tt < 0.0f || tt > 1.0f) return;
+    float4 uv = ldg(&q->uv);
+    float4 uvt = ldg(&q->uvt);
+    float sc = fmin_r(fmax_r(s, 0.0005f), 0.9995f);
+    float tc = fmin_r(fmax_r(tt, 0.0005f), 0.9995f);
+    float u = uv.x + sc * uv.z + tc * uvt.x;
+    float v = uv.y + sc * uv.w + tc * uvt.y;
+    uint32_t tx = texel(S, P, u, v);
+    uint32_t alpha = tx >> 24;
+    uint32_t mode = flags & FLAG_ALPHA_MASK;
+    if ((mode == ALPHA_CUTOUT && alpha < 128u) || (mode == ALPHA_TRANSLUCENT && alpha == 0u)) return;
+    best = Hit{t, qi, tx, s, tt};
+}
+
+// SceneView::voxel (scene.rs:271-284) on the re-laid grid.
+LW_DI uint32_t brick_voxel(const DevScene &S, uint32_t entry, int lx, int ly, int lz) {
+    uint32_t sb = (uint32_t)(((ly >> 2) * 4 + (lz >> 2)) * 4 + (lx >> 2));
+    uint32_t v = (uint32_t)(((ly & 3) * 4 + (lz & 3)) * 4 + (lx & 3));
+    return ldg(S.bricks + ((size_t)entry * 4096u + sb * 64u + v));
+}
+LW_DI uint32_t voxel(const DevScene &S, const DevParams &P, int x, int y, int z) {
+    uint32_t b = ((uint32_t)(y >> 4) * P.grid_dims.z + (uint32_t)(z >> 4)) * P.grid_dims.x + (uint32_t)(x >> 4);
+    uint32_t e = ldg(S.top + b).x;
+    if (e == EMPTY) return 0;
+    if (e & UNIFORM) return e & ~UNIFORM;
+    return brick_voxel(S, e, x & 15, y & 15, z & 15);
+}
+
+LW_DI float safe_inv(float x) {  // trace.rs:293-299
+    if (fabs_r(x) < 1e-12f) return x < 0.0f ? -1e12f : 1e12f;
+    return __fdiv_rn(1.0f, x);
+}
+LW_DI int sgn(float x) { return x > 0.0f ? 1 : (x < 0.0f ? -1 : 0); }
+LW_DI float next_boundary(float o, float inv, int cell, int step) {  // trace.rs:313-319
+    if (step == 0) return kINF;
+    float bound = (float)(step > 0 ? cell + 1 : cell);
+    return (bound - o) * inv;
+}
+
+// trace (trace.rs:137-290). The DDA is the reference's step for step; what differs is where
+// the words come from: the brick's top and overlay entries and its occupancy mask are loaded
+// once when the ray enters the brick and kept in registers, and a voxel in an empty 4^3
+// sub-block of a brick without overlay is stepped over without reading its id, since its model
+// is 0 and it tests no quad.
+LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, float tmax) {
+    const uint32_t dx = P.grid_dims.x, dy = P.grid_dims.y, dz = P.grid_dims.z;
+    V3 size = v3((float)(dx * 16u), (float)(dy * 16u), (float)(dz * 16u));
+    V3 inv = v3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    V3 ta = vmul(v3(0.0f, 0.0f, 0.0f) - o, inv);
+    V3 tb = vmul(size - o, inv);
+    float t_enter = fmax_r(fmax_r(fmin_r(ta.x, tb.x), fmin_r(ta.y, tb.y)), fmin_r(ta.z, tb.z));
+    float t_exit = fmin_r(fmin_r(fmax_r(ta.x, tb.x), fmax_r(ta.y, tb.y)), fmax_r(ta.z, tb.z));
+    float t = fmax_r(t_enter, 0.0f);
+    float t_end = fmin_r(t_exit, tmax);
+    if (t > t_end) return no_hit();
+
+    V3 start = o + d * (t + 1e-4f);
+    const int gs0 = (int)dx * 16, gs1 = (int)dy * 16, gs2 = (int)dz * 16;
+    int c0 = clamp_i(to_i32(floorf(start.x)), 0, gs0 - 1);
+    int c1 = clamp_i(to_i32(floorf(start.y)), 0, gs1 - 1);
+    int c2 = clamp_i(to_i32(floorf(start.z)), 0, gs2 - 1);
+    const int s0 = sgn(d.x), s1 = sgn(d.y), s2 = sgn(d.z);
+    float n0 = next_boundary(o.x, inv.x, c0, s0);
+    float n1 = next_boundary(o.y, inv.y, c1, s1);
+    float n2 = next_boundary(o.z, inv.z, c2, s2);
+    const float best_t = t_end + 1e-3f;
+
+    uint32_t cur_b = 0xFFFFFFFFu, entry = EMPTY, ov = EMPTY;
+    uint2 occ = make_uint2(0u, 0u);
+    for (uint32_t it = 0; it < MAX_STEPS; it++) {
+        uint32_t bx = (uint32_t)(c0 >> 4), by = (uint32_t)(c1 >> 4), bz = (uint32_t)(c2 >> 4);
+        uint32_t b = (by * dz + bz) * dx + bx;
+        if (b != cur_b) {
+            cur_b = b;
+            uint2 e = ldg(S.top + b);
+            entry = e.x;
+            ov = e.y;
+            if (entry != EMPTY && !(entry & UNIFORM)) occ = ldg(S.occ + entry);
+        }
+        if (entry == EMPTY && ov == EMPTY) {
+            // Skip the whole brick: jump to its exit face (trace.rs:184-226).
+            int bc0 = (int)bx, bc1 = (int)by, bc2 = (int)bz;
+            float t_out = kINF;
+            int axis = 0;
+            if (s0 != 0) {
+                float tt = ((float)(s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
+                if (tt < t_out) { t_out = tt; axis = 0; }
+            }
+            if (s1 != 0) {
+                float tt = ((float)(s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
+                if (tt < t_out) { t_out = tt; axis = 1; }
+            }
+            if (s2 != 0) {
+                float tt = ((float)(s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
+                if (tt < t_out) { t_out = tt; axis = 2; }
+            }
+            if (t_out > t_end) break;
+            V3 pos = o + d * t_out;
+            c0 = axis == 0 ? (s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
+            c1 = axis == 1 ? (s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
+            c2 = axis == 2 ? (s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
+            int ca = axis == 0 ? c0 : (axis == 1 ? c1 : c2);
+            int ga = axis == 0 ? gs0 : (axis == 1 ? gs1 : gs2);
+            if (ca < 0 || ca >= ga) break;
+            n0 = next_boundary(o.x, inv.x, c0, s0);
+            n1 = next_boundary(o.y, inv.y, c1, s1);
+            n2 = next_boundary(o.z, inv.z, c2, s2);
+            t = t_out;
+            continue;
+        }
+
+        // Block model in this voxel (trace.rs:233-241).
+        uint32_t model;
+        if (entry == EMPTY) {
+            model = 0;
+        } else if (entry & UNIFORM) {
+            model = entry & ~UNIFORM;
+        } else {
+            int lx = c0 & 15, ly = c1 & 15, lz = c2 & 15;
+            uint32_t sb = (uint32_t)(((ly >> 2) * 4 + (lz >> 2)) * 4 + (lx >> 2));
+            uint32_t word = sb < 32u ? occ.x : occ.y;
+            model = (word >> (sb & 31u)) & 1u ? brick_voxel(S, entry, lx, ly, lz) : 0u;
+        }
+        if (model != 0u || ov != EMPTY) {
+            float t_cell_exit = fmin_r(n0, fmin_r(n1, n2));
+            float t_lo = fmax_r(t - 1e-4f, tmin);
+            float t_hi = t_cell_exit + 1e-4f;
+            Hit cand = no_hit();
+            cand.t = fmin_r(t_hi, best_t);
+            if (model != 0u) {
+                uint4 m = ldg(S.models + model);
+                V3 lo = o - v3((float)c0, (float)c1, (float)c2);
+                for (uint32_t i = 0; i < m.y; i++) test_quad(S, P, m.x + i, lo, d, t_lo, cand);
+            }
+            if (ov != EMPTY) {
+                uint32_t local = (uint32_t)((((c1 & 15) * 16 + (c2 & 15)) * 16) + (c0 & 15));
+                size_t base = (size_t)P.off.w + (size_t)ov * OV_CELL_WORDS + local * 2u;
+                uint32_t off = ldg(S.grid + base);
+                uint32_t count = ldg(S.grid + base + 1);
+                for (uint32_t i = 0; i < count; i++) {
+                    uint32_t qi = ldg(S.grid + (size_t)P.off2.x + off + i);
+                    test_quad(S, P, qi, o, d, t_lo, cand);
+                }
+            }
+            if (cand.quad != NO_QUAD) return cand;
+        }
+
+        // Advance to the next voxel (trace.rs:267-287).
+        int axis = n0 < n1 ? (n0 < n2 ? 0 : 2) : (n1 < n2 ? 1 : 2);
+        if (axis == 0) {
+            t = n0;
+            if (t > t_end) break;
+            c0 += s0;
+            if (c0 < 0 || c0 >= gs0) break;
+            n0 = next_boundary(o.x, inv.x, c0, s0);
+        } else if (axis == 1) {
+            t = n1;
+            if (t > t_end) break;
+            c1 += s1;
+            if (c1 < 0 || c1 >= gs1) break;
+            n1 = next_boundary(o.y, inv.y, c1, s1);
+        } else {
+            t = n2;
+            if (t > t_end) break;
+            c2 += s2;
+            if (c2 < 0 || c2 >= gs2) break;
+            n2 = next_boundary(o.z, inv.z, c2, s2);
+        }
+    }
+    return no_hit();
+}
+
+// is_see_through / see_through_hit (trace.rs:113-131).
+LW_DI bool is_see_through(const DevParams &P, uint32_t qi) {
+    return qi >= P.see_through.x && qi - P.see_through.x < P.see_through.y;
+}
+LW_DI Hit see_through_hit(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin) {
+    Hit best = no_hit();
+    for (uint32_t i = 0; i < P.see_through.y; i++) test_quad(S, P, P.see_through.x + i, o, d, tmin, best);
+    return best;
+}
+
+}  // namespace lw

@@ -1,0 +1,68 @@
+// Declarations shared by the library's translation units (not part of the C ABI).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "device_scene.cuh"
+
+namespace lw {
+
+// One render launch: samples [sample_start, sample_start + spp) of every pixel of the rectangle
+// [x0, x0+w) x [y0, y0+h), cut into items of `sub` consecutive samples of one pixel.
+struct WorkDesc {
+    uint32_t x0, y0, w, h;       // the rectangle
+    uint32_t tiles_x;            // 8x4-pixel tiles per rectangle row
+    uint32_t n_slots;            // pixel slots: tiles * 32
+    uint32_t sample_start, spp;  // the launch's samples
+    uint32_t sub;                // samples per item
+    uint32_t n_sub;              // items per pixel: ceil(spp / sub)
+    uint32_t n_items;            // n_slots * n_sub
+    uint32_t *counter;           // work counter (zeroed before the launch)
+    float4 *partials;            // [n_sub][n_slots] compensated item sums (accumulating mode)
+    float *samples_out;          // per-sample radiance (sample mode), [(py*w+px)*spp + k][3]
+    const volatile int *cancel;  // host-mapped cancel flag: the kernel stops taking items when set
+};
+
+// Per-pixel accumulator: Kahan (sum, compensation), with the sample count in sum.w.
+struct __align__(16) Accum {
+    float4 sum;
+    float4 comp;
+};
+
+enum { MODE_ACCUM = 0, MODE_SAMPLES = 1 };
+
+struct LaunchShape {
+    int blocks, threads;
+};
+
+// render.cu
+cudaError_t launch_render(int mode, const DevScene &S, const DevParams &P, const WorkDesc &W, LaunchShape shape,
+                          cudaStream_t st);
+LaunchShape render_shape(int mode, int device);
+cudaError_t launch_reduce(const WorkDesc &W, Accum *acc, uint32_t frame_w, cudaStream_t st);
+cudaError_t launch_finalize(const Accum *acc, uint32_t n, float *out_rgb, cudaStream_t st);
+cudaError_t launch_trace_rays(const DevScene &S, const DevParams &P, uint32_t n, const float *o, const float *d,
+                              float tmin, float tmax, void *out_hits, cudaStream_t st);
+cudaError_t launch_voxel_lookup(const DevScene &S, const DevParams &P, uint32_t n, const int32_t *xyz, uint32_t *out,
+                                cudaStream_t st);
+
+// sky.cu
+cudaError_t launch_sky_cache(const DevParams &P, uint32_t n, float *out, cudaStream_t st);
+cudaError_t launch_blend_chunky(const DevScene &S, const DevParams &P, float *map, uint32_t w, uint32_t h, float weight,
+                                cudaStream_t st);
+
+// scene.cu
+struct SceneUploadDesc {
+    const uint32_t *grid;  // device copy of the reference grid
+    uint32_t nb, n_bricks, off_top, off_bricks, off_ov_top;
+    uint32_t n_models, n_ov_bricks;
+    uint2 *top;
+    uint16_t *bricks;
+    uint2 *occ;
+    uint32_t *error;  // device error word: bit 0 a top entry out of range, bit 1 a voxel id out of range
+};
+cudaError_t launch_relayout(const SceneUploadDesc &d, cudaStream_t st);
+cudaError_t launch_quads(const void *ref_quads, DevQuad *out, uint32_t n, cudaStream_t st);
+
+}  // namespace lw

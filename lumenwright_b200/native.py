@@ -1,0 +1,304 @@
+"""ctypes bindings of ``liblumenwright_b200.so`` (the C ABI declared in
+``include/lumenwright_b200.h``) and the Python mirror of the reference's backend interface.
+
+The library is the product: every render and every parity query runs in its CUDA kernels. There
+is no fallback: without the library or a B200 these calls raise.
+"""
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from .layout import EMITTER_DTYPE, MODEL_DTYPE, PARAMS_DTYPE, QUAD_DTYPE
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "liblumenwright_b200.so")
+
+# lw_status (include/lumenwright_b200.h)
+STATUS = {
+    0: "LW_OK", 1: "LW_ERR_INVALID_ARGUMENT", 2: "LW_ERR_BUFFER_LENGTH", 3: "LW_ERR_OUT_OF_MEMORY",
+    4: "LW_ERR_DEVICE_TIMEOUT", 5: "LW_ERR_LAUNCH", 6: "LW_ERR_CANCELLED", 7: "LW_ERR_NO_DEVICE",
+    8: "LW_ERR_NO_SCENE",
+}
+
+# Every symbol the header declares, for the load check.
+EXPORTS = (
+    "lw_ctx_create", "lw_ctx_destroy", "lw_last_error", "lw_stream", "lw_get_stats", "lw_cancel", "lw_mark",
+    "lw_elapsed_ms",
+    "lw_scene_upload", "lw_render_hq", "lw_sky_upload", "lw_clear_accumulator", "lw_render_device",
+    "lw_read_accumulator", "lw_render_samples", "lw_trace_rays", "lw_voxel_lookup", "lw_build_sky_cache",
+    "lw_blend_chunky_sky",
+)
+
+
+class LwError(RuntimeError):
+    """A failed library call: ``status`` is the `lw_status` code."""
+
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [
+        ("grid", C.c_void_p), ("grid_len", C.c_uint64),
+        ("models", C.c_void_p), ("models_len", C.c_uint64),
+        ("quads", C.c_void_p), ("quads_len", C.c_uint64),
+        ("atlas", C.c_void_p), ("atlas_len", C.c_uint64),
+        ("emitters", C.c_void_p), ("emitters_len", C.c_uint64),
+        ("emitter_grid", C.c_void_p), ("emitter_grid_len", C.c_uint64),
+        ("dims", C.c_uint32 * 3), ("offsets", C.c_uint32 * 5), ("atlas_size", C.c_uint32 * 2),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [("kernel_ms", C.c_double), ("upload_ms", C.c_double), ("launches", C.c_uint32),
+                ("blocks", C.c_uint32), ("threads", C.c_uint32), ("samples", C.c_uint64)]
+
+
+class HitRec(C.Structure):
+    _fields_ = [("t", C.c_float), ("quad", C.c_uint32), ("texel", C.c_uint32), ("s", C.c_float),
+                ("tt", C.c_float), ("found", C.c_int32)]
+
+
+PROGRESS_FN = C.CFUNCTYPE(None, C.c_uint32, C.c_uint32, C.c_void_p)
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Loads the library (once) and declares its functions."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: run `python -m lumenwright_b200.build` (nvcc, sm_100a)")
+    L = C.CDLL(path)
+    P = C.c_void_p
+    L.lw_ctx_create.argtypes = [C.c_int, C.POINTER(P)]
+    L.lw_ctx_destroy.argtypes = [P]
+    L.lw_ctx_destroy.restype = None
+    L.lw_last_error.argtypes = [P]
+    L.lw_last_error.restype = C.c_char_p
+    L.lw_stream.argtypes = [P]
+    L.lw_stream.restype = P
+    L.lw_get_stats.argtypes = [P, C.POINTER(Stats)]
+    L.lw_cancel.argtypes = [P]
+    L.lw_cancel.restype = None
+    L.lw_scene_upload.argtypes = [P, C.POINTER(SceneDesc)]
+    L.lw_mark.argtypes = [P, C.c_uint32]
+    L.lw_elapsed_ms.argtypes = [P, C.c_uint32, C.c_uint32, C.POINTER(C.c_double)]
+    L.lw_render_hq.argtypes = [P, P, P, C.c_uint64, C.c_uint32, PROGRESS_FN, P, P]
+    L.lw_sky_upload.argtypes = [P, P, C.c_uint64]
+    L.lw_clear_accumulator.argtypes = [P, C.c_uint32, C.c_uint32]
+    L.lw_render_device.argtypes = [P, P, C.c_uint32, C.c_uint32]
+    L.lw_read_accumulator.argtypes = [P, P]
+    L.lw_render_samples.argtypes = [P, P] + [C.c_uint32] * 6 + [P]
+    L.lw_trace_rays.argtypes = [P, P, C.c_uint32, P, P, C.c_float, C.c_float, P]
+    L.lw_voxel_lookup.argtypes = [P, C.c_uint32, P, P]
+    L.lw_build_sky_cache.argtypes = [P, P, C.c_uint32, P]
+    L.lw_blend_chunky_sky.argtypes = [P, P, P, C.c_uint64, P, P, C.c_float]
+    for name in EXPORTS:
+        if name not in ("lw_ctx_destroy", "lw_last_error", "lw_stream", "lw_cancel"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data if a is not None and a.size else None
+
+
+class Context:
+    """An `lw_ctx`: one CUDA device with its streams, its resident scene and its buffers."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        h = C.c_void_p()
+        st = self.L.lw_ctx_create(device, C.byref(h))
+        if st != 0:
+            raise LwError(st, self.L.lw_last_error(None).decode())
+        self.h = h
+        self.device = device
+        self._keep = []
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.lw_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            raise LwError(st, self.L.lw_last_error(self.h).decode())
+
+    @property
+    def stream(self) -> int:
+        return self.L.lw_stream(self.h) or 0
+
+    def stats(self) -> dict:
+        s = Stats()
+        self._check(self.L.lw_get_stats(self.h, C.byref(s)))
+        return {n: getattr(s, n) for n, _ in Stats._fields_}
+
+    def cancel(self):
+        self.L.lw_cancel(self.h)
+
+    def mark(self, slot: int):
+        """Records a CUDA event on the context's stream."""
+        self._check(self.L.lw_mark(self.h, slot))
+
+    def elapsed(self, a: int, b: int) -> float:
+        """Milliseconds between two marks, by the device's clock."""
+        ms = C.c_double()
+        self._check(self.L.lw_elapsed_ms(self.h, a, b, C.byref(ms)))
+        return ms.value
+
+    def upload_scene(self, grid, models, quads, atlas, emitters, emitter_grid, dims, offsets, atlas_size):
+        grid = np.ascontiguousarray(grid, np.uint32)
+        models = np.ascontiguousarray(models, MODEL_DTYPE)
+        quads = np.ascontiguousarray(quads, QUAD_DTYPE)
+        atlas = np.ascontiguousarray(atlas, np.uint32)
+        emitters = np.ascontiguousarray(emitters, EMITTER_DTYPE)
+        emitter_grid = np.ascontiguousarray(emitter_grid, np.uint32)
+        d = SceneDesc(_ptr(grid), grid.size, _ptr(models), models.size, _ptr(quads), quads.size, _ptr(atlas),
+                      atlas.size, _ptr(emitters), emitters.size, _ptr(emitter_grid), emitter_grid.size,
+                      (C.c_uint32 * 3)(*dims), (C.c_uint32 * 5)(*offsets), (C.c_uint32 * 2)(*atlas_size))
+        self._check(self.L.lw_scene_upload(self.h, C.byref(d)))
+
+    def upload_buffers(self, params, grid, models, quads, atlas, emitters, emitter_grid):
+        """Uploads a scene described by flat buffers and the offsets in its `Params`."""
+        p = np.asarray(params, dtype=PARAMS_DTYPE).reshape(())
+        dims = [int(v) for v in p["grid_dims"][:3]]
+        off = [int(v) for v in p["off"]] + [int(p["off2"][0])]
+        self.upload_scene(grid, models, quads, atlas, emitters, emitter_grid, dims, off,
+                          (int(p["off2"][1]), int(p["off2"][2])))
+
+    def upload_hq_scene(self, s):
+        """Uploads an ``HqScene``."""
+        self.upload_scene(s.grid, s.models, s.quads, s.atlas, s.emitters, s.emitter_grid, s.dims, s.offsets,
+                          s.atlas_size)
+
+    @staticmethod
+    def _params(params):
+        return np.array(params, dtype=PARAMS_DTYPE, order="C").reshape(())
+
+    def render_hq(self, params, sky, spp, progress=None):
+        """`Backend::render_hq` on the uploaded scene: mean linear radiance, shape (h, w, 3)."""
+        p = self._params(params)
+        sky = np.ascontiguousarray(sky if sky is not None else np.zeros(0), np.float32)
+        w, h = int(p["frame"][0]), int(p["frame"][1])
+        out = np.zeros((h, w, 3), np.float32)
+        cb = PROGRESS_FN((lambda d, t, u: progress(d, t)) if progress else (lambda d, t, u: None))
+        self._check(self.L.lw_render_hq(self.h, p.ctypes.data, _ptr(sky), sky.size, spp, cb, None, out.ctypes.data))
+        return out
+
+    def upload_sky(self, sky):
+        sky = np.ascontiguousarray(sky if sky is not None else np.zeros(0), np.float32)
+        self._check(self.L.lw_sky_upload(self.h, _ptr(sky), sky.size))
+
+    def clear_accumulator(self, w, h):
+        self._check(self.L.lw_clear_accumulator(self.h, w, h))
+
+    def render_device(self, params, sample_start, spp):
+        p = self._params(params)
+        self._keep = [p]
+        self._check(self.L.lw_render_device(self.h, p.ctypes.data, sample_start, spp))
+
+    def read_accumulator(self, w, h):
+        out = np.zeros((h, w, 3), np.float32)
+        self._check(self.L.lw_read_accumulator(self.h, out.ctypes.data))
+        return out
+
+    def render_samples(self, params, x0, y0, w, h, sample_start, count):
+        """Per-sample radiance, shape (h, w, count, 3)."""
+        p = self._params(params)
+        out = np.zeros((h, w, count, 3), np.float32)
+        self._check(self.L.lw_render_samples(self.h, p.ctypes.data, x0, y0, w, h, sample_start, count,
+                                             out.ctypes.data))
+        return out
+
+    def trace_rays(self, params, o, d, tmin=0.0, tmax=float("inf")):
+        p = self._params(params)
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        n = o.shape[0]
+        out = (HitRec * n)()
+        self._check(self.L.lw_trace_rays(self.h, p.ctypes.data, n, o.ctypes.data, d.ctypes.data, tmin, tmax,
+                                         C.cast(out, C.c_void_p)))
+        return [h if h.found else None for h in out]
+
+    def build_sky_cache(self, params, n):
+        """Chunky's sky cache at resolution n, built on the device."""
+        p = self._params(params)
+        out = np.zeros((n + 1) * (n + 1) * 3, np.float32)
+        self._check(self.L.lw_build_sky_cache(self.h, p.ctypes.data, n, out.ctypes.data))
+        return out
+
+    def blend_chunky_sky(self, params, cache, maps, sizes, weight):
+        """Chunky's sky blended into the game sky's maps, on the device; returns the new maps."""
+        p = self._params(params)
+        cache = np.ascontiguousarray(cache, np.float32)
+        out = np.ascontiguousarray(maps, np.float32).copy()
+        sz = np.ascontiguousarray(sizes, np.float32)
+        self._check(self.L.lw_blend_chunky_sky(self.h, p.ctypes.data, cache.ctypes.data, cache.size, out.ctypes.data,
+                                               sz.ctypes.data, float(weight)))
+        return out
+
+    def voxel_lookup(self, xyz):
+        xyz = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)
+        out = np.zeros(xyz.shape[0], np.uint32)
+        self._check(self.L.lw_voxel_lookup(self.h, xyz.shape[0], xyz.ctypes.data, out.ctypes.data))
+        return out
+
+
+# ---- the reference's backend interface (crates/lumenwright/src/render/mod.rs:35-159) ----------
+
+class BackendKind:
+    """`BackendKind` (render/mod.rs:35-51) with the B200 backend added. Only `B200` is built
+    here: the other kinds are the reference's own backends."""
+
+    Auto = "auto"
+    Cpu = "cpu"
+    Cuda = "cuda"
+    B200 = "b200"
+
+
+class B200Backend:
+    """A `Backend` (render/mod.rs:92-103) whose hq mode runs this library's kernels: the drop-in
+    for `CudaBackend` (crates/lumenwright/src/render/cuda.rs)."""
+
+    def __init__(self, device: int = 0):
+        self.ctx = Context(device)
+        self._scene_key = None
+
+    def name(self) -> str:
+        return f"b200 device {self.ctx.device} (cuda, sm_100a)"
+
+    def render_quick(self, frame):
+        raise NotImplementedError("quick mode is not part of this library; the reference's CPU rasterizer draws it")
+
+    def render_hq(self, frame, progress=None) -> np.ndarray:
+        """Mean linear radiance per pixel, row-major from the top row, as (w*h, 3) float32
+        (the reference's `Vec<[f32; 3]>`). The scene is uploaded once and kept while the same
+        `HqScene` object is drawn again."""
+        key = id(frame.scene)
+        if key != self._scene_key:
+            self.ctx.upload_hq_scene(frame.scene)
+            self._scene_key = key
+        img = self.ctx.render_hq(frame.params, frame.sky, max(int(frame.spp), 1), progress)
+        return img.reshape(-1, 3)
+
+
+def open_backend(kind=BackendKind.B200, device: int = 0):
+    """`open_backend` (render/mod.rs:115-159) for the kind this library adds. A named backend
+    that is unavailable is an error, as in the reference: nothing falls back to the CPU."""
+    if kind in (BackendKind.B200, BackendKind.Cuda):
+        return B200Backend(device)
+    raise ValueError(f"backend {kind!r} is not provided by lumenwright_b200")

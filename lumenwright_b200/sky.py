@@ -1,0 +1,200 @@
+"""Host-side sun and sky set-up of an hq frame, restating the reference's
+`crates/lumenwright/src/render/sky.rs` (sun position, Chunky's sun and Preetham sky parameters,
+the sun texture axes, the game sky's map geometry) and the sky parts of
+`crates/lumenwright/src/request.rs`. FP64 where the reference computes in f64.
+
+The game sky's maps are the client's sky drawn per direction (`QuickSky::background` with the
+jar's environment attributes, sky.rs:909-952). No jar is available here, so
+``synthetic_game_maps`` draws a seeded stand-in of the same sizes and layout: a smooth dusk
+gradient with a glow around the sun, and the light map normalised as `game_sky_maps` normalises
+it.
+"""
+
+import math
+
+import numpy as np
+
+F32 = np.float32
+
+SUN_RADIUS = F32(0.03)                   # sky.rs:563
+DEFAULT_SUN_INTENSITY = F32(1.25)        # sky.rs:559
+SUN_TEXTURE_BRIGHTNESS = F32(16.338118)  # sky.rs:569
+SKY_CACHE_RESOLUTION = 128               # sky.rs:588
+CIVIL_TWILIGHT_END = F32(-6.0 * math.pi / 180.0)  # sky.rs:615
+NIGHT_SKY_LIGHT = F32(0.03)              # sky.rs:618
+LENS_MAP = (2048, 1024)                  # sky.rs:776
+LIGHT_MAP = (360, 180)                   # sky.rs:781
+MAX_SKY_LIGHT = F32(50.0)                # sky.rs:786
+DEFAULT_EMITTER_INTENSITY = F32(13.0)    # request.rs:127
+GAME_EMITTER_INTENSITY = F32(137.9628)   # request.rs:138
+GAMMA = F32(2.2)
+
+
+def celestial_angle(ticks: int) -> np.float32:
+    """sky.rs:28-32."""
+    f = ((ticks % 24000) / 24000.0 - 0.25) % 1.0
+    g = 0.5 - math.cos(f * math.pi) / 2.0
+    return F32((f * 2.0 + g) / 3.0)
+
+
+def normalize32(v):
+    v = np.asarray(v, F32)
+    l = F32(np.sqrt(F32(F32(v[0] * v[0]) + F32(v[1] * v[1])) + F32(v[2] * v[2])))
+    return (v * (F32(1.0) / l)).astype(F32)
+
+
+def sun_direction_from_angle(angle) -> np.ndarray:
+    """sky.rs:35-38 (f32)."""
+    t = F32(angle) * F32(2 * math.pi)
+    return normalize32([-np.sin(t, dtype=F32), np.cos(t, dtype=F32), F32(0.0)])
+
+
+def twilight(altitude) -> np.float32:
+    """sky.rs:625-629: 1 while the sun's disc is up, falling linearly to the night's sky light
+    at the end of civil twilight."""
+    v = F32((F32(altitude) - CIVIL_TWILIGHT_END) / (-SUN_RADIUS - CIVIL_TWILIGHT_END))
+    v = min(max(v, F32(0.0)), F32(1.0))
+    return F32(max(v, NIGHT_SKY_LIGHT))
+
+
+class HqSky:
+    """`HqSky` (sky.rs:549-557)."""
+
+    def __init__(self, sun_dir, sun_color, sky_light):
+        self.sun_dir = np.asarray(sun_dir, F32)
+        self.sun_color = np.asarray(sun_color, F32)
+        self.sky_light = F32(sky_light)
+
+
+def hq_sky(sun_dir, sun_intensity=DEFAULT_SUN_INTENSITY, sky_intensity=F32(1.0)) -> HqSky:
+    """sky.rs:636-643."""
+    altitude = F32(math.asin(max(-1.0, min(1.0, float(sun_dir[1])))))
+    c = F32(float(sun_intensity) ** float(GAMMA))
+    return HqSky(sun_dir, [c, c, c], F32(sky_intensity) * twilight(altitude))
+
+
+class Preetham:
+    """`Preetham::new` (sky.rs:666-742): Chunky's Preetham sky at turbidity 2.5, in f64."""
+
+    X_ZENITH = [[0.00166, -0.00375, 0.00209, 0.0], [-0.02903, 0.06377, -0.03203, 0.00394],
+                [0.11693, -0.21196, 0.06052, 0.25886]]
+    Y_ZENITH = [[0.00275, -0.00610, 0.00317, 0.0], [-0.04214, 0.08970, -0.04153, 0.00516],
+                [0.15346, -0.26756, 0.06670, 0.26688]]
+    MDX = [[-0.0193, -0.2592], [-0.0665, 0.0008], [-0.0004, 0.2125], [-0.0641, -0.8989], [-0.0033, 0.0452]]
+    MDY = [[-0.0167, -0.2608], [-0.0950, 0.0092], [-0.0079, 0.2102], [-0.0441, -1.6537], [-0.0109, 0.0529]]
+    MD_LUM = [[0.1787, -1.4630], [-0.3554, 0.4275], [-0.0227, 5.3251], [0.1206, -2.5771], [-0.0670, 0.3703]]
+
+    def __init__(self, sun_dir, turbidity=2.5):
+        T = float(turbidity)
+        d = np.asarray(sun_dir, np.float64)
+        d = d / math.sqrt(float(d @ d))
+        azimuth = math.atan2(d[2], d[0])
+        alt = min(max(math.asin(max(-1.0, min(1.0, d[1]))), 0.0), math.pi)
+        if alt > math.pi / 2:
+            alt = math.pi - alt
+        r = abs(math.cos(alt))
+        sun = np.array([math.cos(azimuth) * r, math.sin(alt), math.sin(azimuth) * r])
+
+        def coeff(m):
+            return [m[i][0] * T + m[i][1] for i in range(5)]
+
+        cx, cy, cl = coeff(self.MDX), coeff(self.MDY), coeff(self.MD_LUM)
+
+        def perez_f(cos_theta, gamma, cos2_gamma, c):
+            return (1.0 + c[0] * math.exp(c[1] / cos_theta)) * (1.0 + c[2] * math.exp(c[3] * gamma) + c[4] * cos2_gamma)
+
+        def chroma(st, m):
+            row = lambda r: r[0] * st ** 3 + r[1] * st * st + r[2] * st + r[3]  # noqa: E731
+            return T * T * row(m[0]) + T * row(m[1]) + row(m[2])
+
+        sun_theta = math.pi / 2 - alt
+        cos2_theta = math.cos(sun_theta) ** 2
+        chi = (4.0 / 9.0 - T / 120.0) * (math.pi - 2.0 * sun_theta)
+        zenith_lum = abs((4.0453 * T - 4.9710) * math.tan(chi) - 0.2155 * T + 2.4192)
+        zx, zy = chroma(sun_theta, self.X_ZENITH), chroma(sun_theta, self.Y_ZENITH)
+        f0 = lambda c: 1.0 / perez_f(1.0, sun_theta, cos2_theta, c)  # noqa: E731
+        self.sun = sun.astype(F32)
+        self.zenith = np.array([zx * f0(cx), zy * f0(cy), zenith_lum * f0(cl)], F32)
+        self.perez = np.array([[cx[i], cy[i], cl[i]] for i in range(5)], F32)
+        self.turbidity = T
+
+
+def sun_texture_axes(sw):
+    """sky.rs:574-585 (f64)."""
+    s = np.asarray(sw, np.float64)
+    su = np.array([0.0, 1.0, 0.0]) if abs(s[0]) > 0.1 else np.array([1.0, 0.0, 0.0])
+    sv = np.cross(s, su)
+    sv = sv / math.sqrt(float(sv @ sv))
+    su = np.cross(sv, s)
+    return su.astype(F32), sv.astype(F32)
+
+
+def map_direction(i, j, w, h):
+    """sky.rs:853-858 (f32), for arrays of texel indices."""
+    az = (np.asarray(i, F32) + F32(0.5)) / F32(w) * F32(2 * math.pi)
+    el = (np.asarray(j, F32) + F32(0.5)) / F32(h) * F32(math.pi) - F32(math.pi / 2)
+    return np.stack([np.cos(el) * np.cos(az), np.sin(el), np.cos(el) * np.sin(az)], -1).astype(F32)
+
+
+def default_emitter_intensity(on_day_plateau: bool, weight) -> np.float32:
+    """request.rs:156-162."""
+    if on_day_plateau:
+        return F32(0.0)
+    w = F32(weight)
+    return F32(w * DEFAULT_EMITTER_INTENSITY + (F32(1.0) - w) * GAME_EMITTER_INTENSITY)
+
+
+def dusk_day_weight(ticks: int) -> np.float32:
+    """The day weight of the client's 1.21.11 day timeline at a tick (sky.rs:824-829 over the
+    timeline `day_weight` describes): 1 on the day plateau 730..11270, falling linearly to 0 at
+    13140, 0 on the night plateau to 22860, rising back by 730."""
+    t = ticks % 24000
+    if 730 <= t <= 11270:
+        return F32(1.0)
+    if 11270 < t < 13140:
+        return F32((13140 - t) / 1870.0)
+    if 13140 <= t <= 22860:
+        return F32(0.0)
+    return F32(((t - 22860) % 24000) / 1870.0) if t > 22860 else F32((t + 24000 - 22860) / 1870.0)
+
+
+def synthetic_game_maps(sun_dir, seed: int = 7):
+    """A stand-in for `game_sky_maps` (sky.rs:909-952) at dusk: the lens map (2048x1024) and the
+    light map (360x180), linear RGB, row 0 at the nadir, laid out as the kernel's `map_lookup`
+    reads them. The client's sky is replaced by a seeded smooth gradient: a dark blue zenith, an
+    orange horizon glow strongest towards the sun and a dim ground; the light map is scaled so its
+    cosine-weighted upper-hemisphere mean is the lightmap colour of a dusk tick, as the
+    reference's normalisation makes it."""
+    sun = np.asarray(sun_dir, np.float64)
+    rng = np.random.default_rng(seed)
+    tint = 1.0 + 0.05 * rng.standard_normal(3)
+
+    def draw(w, h, with_sun):
+        j, i = np.mgrid[0:h, 0:w]
+        d = map_direction(i, j, w, h).astype(np.float64)
+        y = d[..., 1]
+        toward = np.clip(d @ sun, -1.0, 1.0)
+        zenith = np.array([0.02, 0.04, 0.12]) * tint
+        horizon = np.array([0.45, 0.22, 0.10]) * tint
+        ground = np.array([0.03, 0.025, 0.02])
+        up = np.clip(y, 0.0, 1.0)[..., None]
+        glow = np.exp(-np.abs(y) * 6.0)[..., None] * (0.35 + 0.65 * ((toward + 1.0) / 2.0) ** 4)[..., None]
+        c = zenith * up + horizon * glow + np.where(y[..., None] < 0, ground, 0.0)
+        if with_sun:
+            disc = (toward > math.cos(0.05))[..., None]
+            c = np.where(disc, np.array([6.0, 3.5, 1.5]), c)
+        return c.astype(F32)
+
+    lens = draw(*LENS_MAP, True)
+    light = draw(*LIGHT_MAP, False)
+    gw, gh = LIGHT_MAP
+    j, i = np.mgrid[0:gh, 0:gw]
+    d = map_direction(i, j, gw, gh)
+    w = np.where(d[..., 1] > 0, d[..., 1] * np.sqrt(np.clip(1.0 - d[..., 1] ** 2, 0, None)), 0.0).astype(np.float64)
+    mean = (light.astype(np.float64) * w[..., None]).sum((0, 1)) / w.sum()
+    target = np.array([0.09, 0.075, 0.07])  # a dusk lightmap colour, linear
+    scale = min(float(MAX_SKY_LIGHT), float(np.min(target / mean)))
+    veil = np.maximum(target / scale - mean, 0.0)
+    light = ((light + veil) * scale).astype(F32)
+    buf = np.concatenate([lens.ravel(), light.ravel()]).astype(F32)
+    return buf, np.array([LENS_MAP[0], LENS_MAP[1], LIGHT_MAP[0], LIGHT_MAP[1]], F32)

@@ -142,6 +142,11 @@ void lwo32_sky_lens(const lwo_scene *s, const float d[3], float out[3]) { v3o(sk
 void lwo32_sky_light(const lwo_scene *s, const float d[3], float out[3]) { v3o(sky_light(s, v3a(d)), out); }
 void lwo32_sun_texture(const lwo_scene *s, const float d[3], float out[3]) { v3o(sun_texture(s, v3a(d)), out); }
 
+void lwo32_sky_radiance_many(const lwo_scene *s, uint64_t n, const float *d, float *out) {
+#pragma omp parallel for schedule(static)
+    for (uint64_t i = 0; i < n; i++) v3o(sky_radiance(s, v3a(d + 3 * i)), out + 3 * i);
+}
+
 void lwo32_render_samples(const lwo_scene *s, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
                           uint32_t sample_start, uint32_t count, float *out, int threads) {
     Cam c = params_cam(s->params);

@@ -121,6 +121,8 @@ void lwo32_sky_radiance(const lwo_scene *s, const float d[3], float out[3]);
 void lwo32_sky_lens(const lwo_scene *s, const float d[3], float out[3]);
 void lwo32_sky_light(const lwo_scene *s, const float d[3], float out[3]);
 void lwo32_sun_texture(const lwo_scene *s, const float d[3], float out[3]);
+/* sky_radiance for n directions (d: 3n floats, out: 3n floats), over all host threads. */
+void lwo32_sky_radiance_many(const lwo_scene *s, uint64_t n, const float *d, float *out);
 
 /* Per-sample radiance of `count` samples starting at `sample_start` for every pixel of the
  * rectangle [x0, x0+w) x [y0, y0+h): out[((py*w + px) * count + k) * 3 + c]. */

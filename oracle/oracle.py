@@ -107,6 +107,7 @@ def _declare(L):
               "lwo32_sun_texture"):
         getattr(L, n).argtypes = [sp, F3, F3]
     L.lwo32_build_sky_cache.argtypes = [sp, C.c_uint32, C.c_void_p]
+    L.lwo32_sky_radiance_many.argtypes = [sp, C.c_uint64, C.c_void_p, C.c_void_p]
     L.lwo32_render_samples.argtypes = [sp] + [C.c_uint32] * 6 + [C.c_void_p, C.c_int]
     L.lwo32_render_mean.argtypes = [sp] + [C.c_uint32] * 5 + [C.c_void_p, C.c_int]
     L.lwo32_count_work.argtypes = [sp] + [C.c_uint32] * 5 + [P(Counters)]
@@ -127,7 +128,7 @@ class OracleScene:
     """
 
     def __init__(self, params, grid, models, quads, atlas, emitters, emitter_grid, sky=None):
-        self.params = np.ascontiguousarray(np.asarray(params, dtype=PARAMS_DTYPE).reshape(()))
+        self.params = np.array(params, dtype=PARAMS_DTYPE, order="C").reshape(())
         self.grid = _arr(grid, np.uint32)
         self.models = _arr(models, MODEL_DTYPE)
         self.quads = _arr(quads, QUAD_DTYPE)
@@ -202,6 +203,12 @@ class OracleScene:
 
     def sky_radiance(self, d):
         return self._v3("lwo32_sky_radiance", d)
+
+    def sky_radiance_many(self, dirs):
+        d = np.ascontiguousarray(dirs, np.float32).reshape(-1, 3)
+        out = np.zeros_like(d)
+        lib().lwo32_sky_radiance_many(self.ref, d.shape[0], d.ctypes.data, out.ctypes.data)
+        return out
 
     def sky_lens(self, d):
         return self._v3("lwo32_sky_lens", d)

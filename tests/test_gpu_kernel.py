@@ -1,0 +1,230 @@
+"""CUDA parity on the reference kernel tests' fixtures (`crates/lumenwright-kernel/src/tests.rs`):
+each query runs through the C ABI on the B200 and is checked against the FP32 oracle and against
+the reference test's own known answer. Integer results (hit quad, texel, voxel id) must be equal;
+floats must be bit-equal except where noted (the water transmittance calls each platform's expf).
+"""
+
+import math
+
+import numpy as np
+import pytest
+
+from kernel_fixtures import (INF, LAMP_EMITTANCE, LAMP_INTENSITY, basic_scene, lamp_scene, map_scene, norm,
+                             set_preetham_45, wall_rays, wall_scene)
+from lumenwright_b200 import layout as L
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from lumenwright_b200.native import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+def upload(ctx, ks):
+    ctx.upload_buffers(ks.params, ks.grid, ks.models, ks.quads, ks.atlas, ks.emitters, ks.emitter_grid)
+    ctx.upload_sky(ks.sky)
+
+
+def same_hit(a, b):
+    if a is None or b is None:
+        return a is None and b is None
+    return (a.quad == b.quad and a.texel == b.texel and np.float32(a.t).tobytes() == np.float32(b.t).tobytes()
+            and np.float32(a.s).tobytes() == np.float32(b.s).tobytes())
+
+
+def check_rays(ctx, ks, rays, tmin=0.0, tmax=INF):
+    upload(ctx, ks)
+    o = np.array([r[0] for r in rays], np.float32)
+    d = np.array([r[1] for r in rays], np.float32)
+    got = ctx.trace_rays(ks.params, o, d, tmin, tmax)
+    v = O.OracleScene(*ks.buffers())
+    want = [v.trace(oo, dd, tmin, tmax) for oo, dd in zip(o, d)]
+    bad = [i for i, (g, w) in enumerate(zip(got, want)) if not same_hit(g, w)]
+    assert not bad, f"{len(bad)} of {len(rays)} rays differ from the oracle, first {bad[:5]}"
+    return got
+
+
+def test_trace_known_answers(ctx):  # tests.rs:129-195
+    ks = basic_scene(False)
+    rays = [((0.5, 5.5, 5.5), (1, 0, 0)), ((-10.0, 5.5, 5.5), (1, 0, 0)), ((0.5, 9.5, 5.5), (1, 0, 0)),
+            ((0.5, 5.5, 5.5), (0, 1, 0)), ((0.5, 5.5, 5.5), (-1, 0, 0))]
+    o = np.array([18.0, 9.0, 3.0], np.float32)
+    rays.append((o, norm(np.array([20.5, 6.0, 5.5], np.float32) - o)))
+    got = check_rays(ctx, ks, rays)
+    assert abs(got[0].t - 19.5) < 1e-3 and got[0].quad == 3
+    assert abs(got[1].t - 30.0) < 1e-3
+    assert abs(got[2].t - 31.5) < 1e-3
+    assert got[3] is None and got[4] is None
+    assert got[5].quad == 4
+    assert check_rays(ctx, ks, [((0.5, 5.5, 5.5), (1, 0, 0))], 0.0, 10.0)[0] is None
+
+
+def test_overlay_and_front_only(ctx):  # tests.rs:198-240
+    ks = basic_scene(True)
+    got = check_rays(ctx, ks, [((0.5, 5.5, 5.25), (1, 0, 0)), ((0.5, 5.5, 5.75), (1, 0, 0))])
+    assert got[0].quad == 6 and abs(got[0].t - 8.0) < 1e-3 and abs(got[1].t - 19.5) < 1e-3
+    L.quad_words(ks.quads)[6, 3] = L.ALPHA_CUTOUT | L.FLAG_FRONT_ONLY
+    got = check_rays(ctx, ks, [((0.5, 5.5, 5.25), (1, 0, 0))], 0.0, 16.0)
+    assert got[0].quad == 6
+    assert check_rays(ctx, ks, [((12.0, 5.5, 5.25), (-1, 0, 0))])[0] is None
+
+
+def test_front_face_far_along_the_ray(ctx):  # tests.rs:607-683
+    ks = wall_scene()
+    rays = wall_rays()
+    got = check_rays(ctx, ks, rays)
+    missed = sum(1 for (o, d), h in zip(rays, got)
+                 if h is None or not (249.99 < float(o[0] + d[0] * np.float32(h.t)) < 250.01))
+    assert missed == 0
+
+
+def test_later_coplanar_quad(ctx):  # tests.rs:688-721
+    ks = basic_scene(False)
+    w = L.quad_words(ks.quads)
+    ks.quads = L.quads_array([w[0], w[1], w[2], w[3], w[4], w[5], w[4], w[0]])
+    ks.models[1]["quad_count"] = 8
+    ks.params["off2"][3] = 8
+    rays = []
+    for i in range(16):
+        f = np.float32(0.1) + np.float32(0.7) * (np.float32(i) + np.float32(0.5)) / np.float32(16.0)
+        rays.append(((20.0 + f, 9.0, 5.0 + f), norm([0.01, -1.0, 0.02])))
+        rays.append(((20.0 + f, 5.0 + f, 1.0), norm([0.02, 0.01, 1.0])))
+    got = check_rays(ctx, ks, rays, 0.0, 100.0)
+    assert [h.quad for h in got] == [6, 7] * 16
+
+
+def test_voxel_lookup_is_bit_exact(ctx):  # scene.rs:271-284 on the re-laid bricks
+    for ks in (basic_scene(True), lamp_scene(L.EMITTER_SAMPLING_ONE, True), wall_scene()):
+        upload(ctx, ks)
+        dims = [int(v) for v in ks.params["grid_dims"][:3]]
+        xs, ys, zs = np.meshgrid(np.arange(dims[0] * 16), np.arange(dims[1] * 16), np.arange(dims[2] * 16), indexing="ij")
+        xyz = np.stack([xs.ravel(), ys.ravel(), zs.ravel()], 1).astype(np.int32)
+        got = ctx.voxel_lookup(xyz)
+        v = O.OracleScene(*ks.buffers())
+        want = np.array([v.voxel(*map(int, p)) for p in xyz[:: max(1, len(xyz) // 20000)]], np.uint32)
+        assert np.array_equal(got[:: max(1, len(xyz) // 20000)], want)
+
+
+def samples_match(ctx, ks, w, h, count, rel=0.0):
+    upload(ctx, ks)
+    got = ctx.render_samples(ks.params, 0, 0, w, h, 0, count)
+    v = O.OracleScene(*ks.buffers())
+    want = v.render_samples(0, 0, w, h, 0, count)
+    if rel == 0.0:
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), np.argwhere(got != want)[:5]
+    else:
+        np.testing.assert_allclose(got, want, rtol=rel, atol=1e-7)
+    return got
+
+
+def test_empty_scene_shows_sky(ctx):  # tests.rs:262-291
+    ks = basic_scene(False)
+    p = ks.params
+    p["frame"] = [4, 4, 0, 4]
+    p["cam_pos"] = [0.5, 12.0, 0.5, 0.5]
+    p["cam_fwd"] = [0.0, 1.0, 0.0, 1.0]
+    p["cam_right"] = [1.0, 0.0, 0.0, 0.0]
+    p["cam_up"] = [0.0, 0.0, -1.0, 0.0]
+    set_preetham_45(p)
+    p["sun_dir"] = [0.0, -1.0, 0.0, 1.0]
+    p["misc_f"][2] = 128
+    ks.sky = O.OracleScene(*ks.buffers()).build_sky_cache(128)
+    got = samples_match(ctx, ks, 4, 4, 8)
+    assert np.all(got[..., 2] > got[..., 0]) and np.all(got[..., 2] > 0.3)
+
+
+def test_emitter_seen_from_the_camera(ctx):  # tests.rs:476-492
+    ks = lamp_scene(L.EMITTER_SAMPLING_ONE, False)
+    p = ks.params
+    p["frame"] = [1, 1, 0, 1]
+    p["cam_pos"] = [7.5, 2.0, 7.5, 0.01]
+    p["cam_fwd"] = [0.0, 1.0, 0.0, 1.0]
+    p["cam_right"] = [1.0, 0.0, 0.0, 0.0]
+    p["cam_up"] = [0.0, 0.0, -1.0, 0.0]
+    got = samples_match(ctx, ks, 1, 1, 16)
+    want = LAMP_EMITTANCE * LAMP_INTENSITY
+    assert np.all(np.abs(got[..., :2] - want) < 1e-4)
+
+
+@pytest.mark.parametrize("strategy", [L.EMITTER_SAMPLING_NONE, L.EMITTER_SAMPLING_ONE,
+                                      L.EMITTER_SAMPLING_ONE_BLOCK, L.EMITTER_SAMPLING_ALL])
+@pytest.mark.parametrize("decoy", [False, True])
+def test_lamp_room_per_sample(ctx, strategy, decoy):  # tests.rs:310-469 through render_sample
+    ks = lamp_scene(strategy, decoy)
+    p = ks.params
+    p["frame"] = [8, 8, 0, 3]
+    p["cam_pos"] = [8.0, 10.0, 8.0, 0.9]
+    p["cam_fwd"] = [0.0, -1.0, 0.0, 1.0]
+    p["cam_right"] = [1.0, 0.0, 0.0, 0.0]
+    p["cam_up"] = [0.0, 0.0, -1.0, 0.0]
+    p["sun_dir"] = [0.3, 0.9, 0.316, 0.9995]
+    p["sun_color"] = [1.0, 0.9, 0.8, 0.03]
+    got = samples_match(ctx, ks, 8, 8, 16)
+    assert np.isfinite(got).all()
+
+
+def test_sky_maps_lens_and_light(ctx):  # tests.rs:805-831
+    ks = basic_scene(False)
+    p = ks.params
+    p["sky_map"] = [4.0, 2.0, 2.0, 2.0]
+    ks.sky = np.concatenate([np.full(4 * 2 * 3, 5.0, np.float32), np.full(2 * 2 * 3, 0.3, np.float32)])
+    p["frame"] = [1, 1, 0, 1]
+    p["cam_pos"] = [40.25, 20.0, 8.25, 1e-3]
+    p["cam_right"] = [1.0, 0.0, 0.0, 0.0]
+    p["sun_dir"] = [0.0, 1.0, 0.0, 0.9995]
+    p["cam_fwd"] = [0.0, -1.0, 0.0, 1.0]
+    p["cam_up"] = [0.0, 0.0, -1.0, 0.0]
+    got = samples_match(ctx, ks, 1, 1, 16)
+    assert np.all(np.abs(got - 0.3) < 1e-4)
+    p["sun_color"] = [1.0, 1.0, 1.0, 0.03]
+    got = samples_match(ctx, ks, 1, 1, 4)
+    assert got[0, 0, 0, 0] > 1.0
+    ms = map_scene()
+    ms.params["frame"] = [16, 8, 0, 2]
+    ms.params["cam_pos"] = [24.0, 8.0, 8.0, 1.2]
+    ms.params["cam_fwd"] = [0.0, 0.6, 0.8, 2.0]
+    ms.params["cam_right"] = [1.0, 0.0, 0.0, 0.0]
+    ms.params["cam_up"] = [0.0, 0.8, -0.6, 0.0]
+    samples_match(ctx, ms, 16, 8, 4)
+
+
+def test_render_hq_mean_matches_cpu_backend(ctx):  # cpu/mod.rs:39-87 against cuda.rs:77-184
+    ks = lamp_scene(L.EMITTER_SAMPLING_ONE, True)
+    p = ks.params
+    p["frame"] = [32, 24, 0, 4]
+    p["cam_pos"] = [8.0, 12.0, 8.0, 0.9]
+    p["cam_fwd"] = [0.0, -1.0, 0.0, 1.3333]
+    p["cam_right"] = [1.0, 0.0, 0.0, 0.0]
+    p["cam_up"] = [0.0, 0.0, -1.0, 0.0]
+    upload(ctx, ks)
+    calls = []
+    img = ctx.render_hq(p, ks.sky, 64, progress=lambda d, t: calls.append((d, t)))
+    want = O.OracleScene(*ks.buffers()).render_mean(0, 0, 32, 24, 64)
+    np.testing.assert_allclose(img, want, rtol=2e-6, atol=1e-6)
+    assert calls and calls[-1] == (64, 64)
+
+
+def test_bad_buffers_are_refused(ctx):  # the C ABI never traps on a malformed scene
+    from lumenwright_b200.native import LwError
+    ks = basic_scene(False)
+    bad = ks.grid.copy()
+    bad[1] = 7  # a top entry naming a brick that does not exist
+    with pytest.raises(LwError) as e:
+        ctx.upload_buffers(ks.params, bad, ks.models, ks.quads, ks.atlas, ks.emitters, ks.emitter_grid)
+    assert e.value.status == 2
+    m = ks.models.copy()
+    m[1]["quad_count"] = 99
+    with pytest.raises(LwError):
+        ctx.upload_buffers(ks.params, ks.grid, m, ks.quads, ks.atlas, ks.emitters, ks.emitter_grid)
+    upload(ctx, ks)
+    p = ks.params.copy()
+    p["misc_f"][2] = 128  # a sky cache that was not given
+    p["frame"] = [4, 4, 0, 1]
+    with pytest.raises(LwError) as e:
+        ctx.render_samples(p, 0, 0, 4, 4, 0, 1)
+    assert e.value.status == 2

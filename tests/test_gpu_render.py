@@ -1,0 +1,81 @@
+"""CUDA parity at the benchmark configurations (synthetic worlds): the device sky cache, per-sample
+radiance on crops of the C1 and C2 frames, and the C1 frame's mean through `render_hq`, each
+against the FP32 oracle on the same inputs and seeded RNG stream.
+
+Tolerances: per sample 1e-4 relative (the water transmittance calls each platform's `expf`, and a
+last-place difference there can flip a later Russian-roulette draw, so at most 0.5% of samples
+may differ by more); pixel means 1e-4 relative.
+"""
+
+import numpy as np
+import pytest
+
+from lumenwright_b200 import request as R
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    from lumenwright_b200.native import Context
+    c = Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def c1(ctx):
+    return R.make_frame(R.CONFIGS["c1"], sky_backend=ctx)
+
+
+@pytest.fixture(scope="module")
+def c2(ctx):
+    return R.make_frame(R.CONFIGS["c2"], sky_backend=ctx, spp=4)
+
+
+def close(a, b, rel=1e-4, atol=1e-6):
+    return np.abs(a - b) <= rel * np.maximum(np.abs(a), np.abs(b)) + atol
+
+
+def test_device_sky_cache_matches_the_oracle(ctx, c1):
+    p = c1.params
+    got = ctx.build_sky_cache(p, 128)
+    want = O.OracleScene(p, None, None, None, None, None, None).build_sky_cache(128)
+    assert got.shape == want.shape
+    np.testing.assert_allclose(got, want, rtol=2e-5, atol=2e-6)
+
+
+def per_sample(ctx, frame, x0, y0, w, h, count):
+    ctx.upload_hq_scene(frame.scene)
+    ctx.upload_sky(frame.sky)
+    got = ctx.render_samples(frame.params, x0, y0, w, h, 0, count)
+    want = O.OracleScene.from_frame(frame).render_samples(x0, y0, w, h, 0, count)
+    ok = np.all(close(got, want), axis=-1)
+    exact = np.all(got.view(np.uint32) == want.view(np.uint32), axis=-1)
+    return ok.mean(), exact.mean(), got, want
+
+
+@pytest.mark.parametrize("rect", [(0, 0, 64, 36), (96, 54, 64, 36), (192, 100, 64, 44)])
+def test_c1_per_sample_radiance(ctx, c1, rect):
+    ok, exact, got, want = per_sample(ctx, c1, *rect, 4)
+    print(f"C1 {rect}: {ok:.5f} of samples within 1e-4, {exact:.5f} bit-equal")
+    assert ok >= 0.995, ok
+
+
+@pytest.mark.parametrize("rect", [(0, 0, 64, 32), (600, 300, 64, 32), (1200, 680, 64, 32), (320, 500, 64, 32)])
+def test_c2_per_sample_radiance(ctx, c2, rect):
+    ok, exact, got, want = per_sample(ctx, c2, *rect, 2)
+    print(f"C2 {rect}: {ok:.5f} of samples within 1e-4, {exact:.5f} bit-equal")
+    assert ok >= 0.995, ok
+
+
+def test_c1_render_hq_matches_the_cpu_backend(ctx, c1):
+    from lumenwright_b200.native import B200Backend
+    be = B200Backend(0)
+    img = be.render_hq(c1).reshape(144, 256, 3)
+    want = O.OracleScene.from_frame(c1).render_mean(0, 0, 256, 144, c1.spp)
+    ok = np.all(close(img, want, 1e-4, 1e-6), axis=-1).mean()
+    print(f"C1 mean: {ok:.5f} of pixels within 1e-4; mean {img.mean():.6f} vs {want.mean():.6f}")
+    assert ok >= 0.99
+    assert abs(img.mean() - want.mean()) <= 1e-4 * abs(want.mean())
