@@ -247,10 +247,13 @@ def main():
     ctx.upload_hq_scene(frame.scene)
     ctx.upload_sky(frame.sky)
 
+    from lumenwright_b200 import shard
+
     def device_step(i):
         # Each rank renders its own sample range of the frame (weak scaling).
+        start, count = shard.sample_range(rank, world, spp, step=i)
         ctx.clear_accumulator(w, h)
-        ctx.render_device(p, (rank + i * world) * spp, spp)
+        ctx.render_device(p, start, count)
 
     for i in range(args.warmup):
         device_step(i)
@@ -273,8 +276,8 @@ def main():
         t = torch.tensor([total_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-        acc = torch.from_numpy(ctx.read_accumulator(w, h)).to(f"cuda:{local}")
-        dist.reduce(acc, 0)  # the frame's accumulators summed to rank 0 (one NCCL reduce)
+        # The frame: every rank's mean over its samples, reduced to rank 0 (one NCCL reduce).
+        shard.reduce_means(ctx.read_accumulator(w, h), dist, device=f"cuda:{local}")
     value = samples_per_step * args.steps * world / (total_ms / 1e3) / 1e6
     avg_launch_ms = kernel_ms / max(1, launches // 2)
 

@@ -73,6 +73,7 @@ struct lw_ctx {
     DBuf<uint4> models;
     DBuf<DevQuad> quads;
     DBuf<float4> emitters;
+    DBuf<uint8_t> ref_quads;  // the reference's 80-byte quads (read by the reference-port kernel)
     uint64_t grid_len = 0, models_len = 0, quads_len = 0, atlas_len = 0, emitters_len = 0, egrid_len = 0;
     // frame
     DBuf<float> sky, gamma, out_rgb;
@@ -86,7 +87,9 @@ struct lw_ctx {
     DBuf<uint8_t> hits;
     DBuf<int32_t> xyz;
     DBuf<uint32_t> vox;
-    int *cancel_host = nullptr, *cancel_dev = nullptr;
+    int *cancel_host = nullptr;      // host flag, read between launches
+    DBuf<uint32_t> cancel_word;      // device word the render kernel polls; set by lw_cancel
+    cudaStream_t aux = nullptr;      // lw_cancel's stream, so the write lands while a render runs
     lw_stats stats{};
     size_t partials_cap_bytes = size_t(4) << 30;
 };
@@ -225,7 +228,7 @@ WorkDesc work(lw_ctx *c, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint3
     W.counter = c->counter.p;
     W.partials = c->partials.p;
     W.samples_out = c->samples.p;
-    W.cancel = c->cancel_dev;
+    W.cancel = c->cancel_word.p;
     return W;
 }
 
@@ -300,9 +303,10 @@ lw_status lw_ctx_create(int device, lw_ctx **out) {
         return bail(e, "creating events");
     for (auto &m : c->marks)
         if ((e = cudaEventCreate(&m)) != cudaSuccess) return bail(e, "creating events");
-    if ((e = cudaHostAlloc(&c->cancel_host, sizeof(int), cudaHostAllocMapped)) != cudaSuccess) return bail(e, "allocating the cancel flag");
-    *c->cancel_host = 0;
-    if ((e = cudaHostGetDevicePointer(&c->cancel_dev, c->cancel_host, 0)) != cudaSuccess) return bail(e, "mapping the cancel flag");
+    c->cancel_host = new int(0);
+    if ((e = cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "creating a stream");
+    if ((e = ensure(c->cancel_word, 1)) != cudaSuccess) return bail(e, "allocating the cancel word");
+    if ((e = cudaMemset(c->cancel_word.p, 0, 4)) != cudaSuccess) return bail(e, "clearing the cancel word");
     float lut[256];
     for (int k = 0; k < 256; k++) lut[k] = ref_gamma_to_linear((float)k / 255.0f);
     if ((e = ensure(c->gamma, 256)) != cudaSuccess) return bail(e, "allocating the gamma table");
@@ -326,11 +330,14 @@ void lw_ctx_destroy(lw_ctx *c) {
     c->quads.free_();
     c->emitters.free_();
     c->partials.free_();
+    c->ref_quads.free_();
     for (auto *b : {&c->sky, &c->gamma, &c->out_rgb, &c->samples, &c->rays}) b->free_();
     c->acc.free_();
     c->hits.free_();
     c->xyz.free_();
-    if (c->cancel_host) cudaFreeHost(c->cancel_host);
+    delete c->cancel_host;
+    c->cancel_word.free_();
+    if (c->aux) cudaStreamDestroy(c->aux);
     if (c->ev_a) cudaEventDestroy(c->ev_a);
     if (c->ev_b) cudaEventDestroy(c->ev_b);
     for (auto m : c->marks)
@@ -344,7 +351,10 @@ const char *lw_last_error(const lw_ctx *c) { return c ? c->err.c_str() : g_creat
 void *lw_stream(lw_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 void lw_cancel(lw_ctx *c) {
-    if (c && c->cancel_host) __atomic_store_n(c->cancel_host, 1, __ATOMIC_RELAXED);
+    if (!c || !c->cancel_host) return;
+    __atomic_store_n(c->cancel_host, 1, __ATOMIC_RELAXED);
+    cudaSetDevice(c->device);
+    cudaMemsetAsync(c->cancel_word.p, 0xFF, 4, c->aux);  // lands while a render kernel runs
 }
 
 lw_status lw_mark(lw_ctx *c, uint32_t slot) {
@@ -441,10 +451,9 @@ lw_status lw_scene_upload(lw_ctx *c, const lw_scene_desc *d) {
     CK(c, upload(c, c->atlas, d->atlas, d->atlas_len, 4), "uploading the atlas");
     CK(c, upload(c, c->emitters, d->emitters, d->emitters_len, 32), "uploading the emitters");
     CK(c, upload(c, c->egrid, d->emitter_grid, d->emitter_grid_len, 4), "uploading the emitter grid");
-    DBuf<uint8_t> ref_quads;
-    CK(c, upload(c, ref_quads, d->quads, d->quads_len, 80), "uploading the quads");
+    CK(c, upload(c, c->ref_quads, d->quads, d->quads_len, 80), "uploading the quads");
     CK(c, ensure(c->quads, d->quads_len), "allocating the quads");
-    CK(c, launch_quads(ref_quads.p, c->quads.p, (uint32_t)d->quads_len, c->stream), "re-laying the quads");
+    CK(c, launch_quads(c->ref_quads.p, c->quads.p, (uint32_t)d->quads_len, c->stream), "re-laying the quads");
     CK(c, ensure(c->top, nb), "allocating the top level");
     CK(c, ensure(c->bricks, (size_t)n_bricks * 4096u), "allocating the bricks");
     CK(c, ensure(c->occ, n_bricks), "allocating the occupancy masks");
@@ -455,7 +464,6 @@ lw_status lw_scene_upload(lw_ctx *c, const lw_scene_desc *d) {
     uint32_t err = 0;
     CK(c, cudaMemcpyAsync(&err, c->error.p, 4, cudaMemcpyDeviceToHost, c->stream), "reading the error word");
     CK(c, cudaStreamSynchronize(c->stream), "uploading the scene");
-    ref_quads.free_();
     if (err & 1u) return fail(c, LW_ERR_BUFFER_LENGTH, "a top-level entry names a brick, model or overlay brick out of range");
     if (err & 2u) return fail(c, LW_ERR_BUFFER_LENGTH, "a voxel names a model out of range");
     std::memcpy(c->dims, d->dims, sizeof c->dims);
@@ -502,6 +510,7 @@ lw_status lw_render_device(lw_ctx *c, const lw_params *params, uint32_t sample_s
         return fail(c, LW_ERR_INVALID_ARGUMENT, "the accumulator is %ux%u, the frame %ux%u", c->acc_w, c->acc_h, params->frame[0], params->frame[1]);
     if (spp == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "spp is 0");
     __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
+    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
     c->stats.launches = 0;
     c->stats.samples = 0;
     c->stats.kernel_ms = 0;
@@ -532,6 +541,7 @@ lw_status lw_render_hq(lw_ctx *c, const lw_params *params, const float *sky, uin
     s = lw_clear_accumulator(c, params->frame[0], params->frame[1]);
     if (s != LW_OK) return s;
     __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
+    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
     c->stats.launches = 0;
     c->stats.samples = 0;
     c->stats.kernel_ms = 0;
@@ -553,6 +563,7 @@ lw_status lw_render_samples(lw_ctx *c, const lw_params *params, uint32_t x0, uin
     WorkDesc W = work(c, x0, y0, w, h, sample_start, count, 1);
     W.samples_out = c->samples.p;
     __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
+    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
     CK(c, cudaMemsetAsync(c->counter.p, 0, 4, c->stream), "clearing the work counter");
     CK(c, launch_render(MODE_SAMPLES, dev_scene(c), dev_params(params), W, c->shape_samples, c->stream), "launching the render kernel");
     CK(c, cudaMemcpyAsync(out, c->samples.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "reading the samples");
@@ -594,6 +605,58 @@ lw_status lw_voxel_lookup(lw_ctx *c, uint32_t n, const int32_t *xyz, uint32_t *o
     CK(c, cudaMemcpyAsync(out, c->vox.p, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream), "reading ids");
     CK(c, cudaStreamSynchronize(c->stream), "looking up voxels");
     return LW_OK;
+}
+
+lw_status lw_render_hq_reference_port(lw_ctx *c, const lw_params *params, const float *sky, uint64_t sky_len,
+                                      uint32_t spp, float *out_rgb) {
+    if (!c || !out_rgb) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(c->device);
+    if (spp < 1) spp = 1;
+    lw_status s = lw_sky_upload(c, sky, sky_len);
+    if (s != LW_OK) return s;
+    if ((s = check_params(c, params, true)) != LW_OK) return s;
+    const uint32_t w = params->frame[0], h = params->frame[1];
+    DBuf<float4> acc;
+    CK(c, ensure(acc, (size_t)w * h), "allocating the accumulator");
+    CK(c, cudaMemsetAsync(acc.p, 0, sizeof(float4) * (size_t)w * h, c->stream), "clearing the accumulator");
+    DevScene Sv = dev_scene(c);
+    DevParams P = dev_params(params);
+    c->stats.launches = 0;
+    c->stats.samples = 0;
+    c->stats.kernel_ms = 0;
+    uint32_t done = 0, batch = 1;
+    lw_status result = LW_OK;
+    while (done < spp) {
+        uint32_t n = batch < spp - done ? batch : spp - done;
+        auto t0 = std::chrono::steady_clock::now();
+        cudaError_t e = cudaEventRecord(c->ev_a, c->stream);
+        if (e == cudaSuccess) e = launch_refport(c->grid.p, c->models.p, c->ref_quads.p, c->atlas.p, c->emitters.p, c->egrid.p,
+                                                 c->sky.p, c->gamma.p, Sv, P, acc.p, done, n, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_b, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            result = cuda_fail(c, e, "running the reference-port kernel");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev_a, c->ev_b);
+        c->stats.kernel_ms += ms;
+        c->stats.launches++;
+        c->stats.samples += (uint64_t)w * h * n;
+        double took = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        done += n;
+        if (took < 75.0) batch = batch * 2 < 64 ? batch * 2 : 64;
+        else if (took > 300.0 && batch > 1) batch /= 2;
+    }
+    if (result == LW_OK) {
+        CK(c, ensure(c->out_rgb, (size_t)3 * w * h), "allocating the output");
+        cudaError_t e = launch_refport_finalize(acc.p, w * h, c->out_rgb.p, c->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(out_rgb, c->out_rgb.p, (size_t)12 * w * h, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) result = cuda_fail(c, e, "reading the image");
+    }
+    acc.free_();
+    return result;
 }
 
 lw_status lw_build_sky_cache(lw_ctx *c, const lw_params *params, uint32_t n, float *out) {

@@ -28,7 +28,7 @@ LW_DI V3 rgb_from_hsl(float hue, float saturation, float lightness) {  // :108-1
     return rgb + v3(m, m, m);
 }
 
-LW_DI V3 sky_radiance(const DevScene &S, const DevParams &P, V3 d) {  // :158-188
+LW_COLD V3 sky_radiance(const DevScene &S, const DevParams &P, V3 d) {  // :158-188
     float n = P.misc_f.z;
     if (n < 1.0f) return v3(0.0f, 0.0f, 0.0f);
     float theta = __fdiv_rn(atan2_r(d.z, d.x), 2.0f * kPI);
@@ -59,7 +59,7 @@ LW_DI V3 sky_texel(const DevScene &S, uint32_t base, uint32_t w, float i, float 
     return v3(ldg(S.sky + k), ldg(S.sky + k + 1), ldg(S.sky + k + 2));
 }
 
-LW_DI V3 map_lookup(const DevScene &S, uint32_t base, float w, float h, V3 d) {  // :196-217
+LW_COLD V3 map_lookup(const DevScene &S, uint32_t base, float w, float h, V3 d) {  // :196-217
     float u = __fdiv_rn(atan2_r(d.z, d.x), 2.0f * kPI);
     u = fmodf(fmodf(u, 1.0f) + 1.0f, 1.0f);
     float v = 1.0f - __fdiv_rn(acos_r(clamp_r(d.y, -1.0f, 1.0f)), kPI);
@@ -85,7 +85,7 @@ LW_DI V3 sky_light(const DevScene &S, const DevParams &P, V3 d) {  // :237-243
     return map_lookup(S, to_u32(P.sky_map.x * P.sky_map.y) * 3u, P.sky_map.z, P.sky_map.w, d);
 }
 
-LW_DI V3 sun_texture(const DevScene &S, const DevParams &P, V3 d) {  // :252-277
+LW_COLD V3 sun_texture(const DevScene &S, const DevParams &P, V3 d) {  // :252-277
     float4 sprite = P.sun_sprite;
     if (sprite.z <= 0.0f || dot(d, f4v(P.sun_dir)) < 0.5f) return v3(0.0f, 0.0f, 0.0f);
     float width = P.sun_sv.w;
@@ -147,7 +147,7 @@ LW_DI void emitter_cell(const DevScene &S, V3 p, uint32_t &start, uint32_t &coun
 }
 
 // ---- water (integrator.rs:477-534) ------------------------------------------------------------
-LW_DI bool water_interface(const DevParams &P, V3 pos, V3 d, V3 n, bool front, bool in_water, float eps,
+LW_COLD bool water_interface(const DevParams &P, V3 pos, V3 d, V3 n, bool front, bool in_water, float eps,
                            uint32_t &rng, V3 &nd, V3 &no) {
     float ior = P.water_color.w;
     float eta = front ? __fdiv_rn(1.0f, ior) : ior;

@@ -11,6 +11,16 @@ namespace lw {
 
 #define LW_DI __device__ __forceinline__
 #define LW_HDI __host__ __device__ __forceinline__
+// Rarely taken paths (sky lookups, the sun texture, water interfaces, see-through quads) are kept
+// out of line so the hot loop stays small in the instruction cache.
+#ifndef LW_NOINLINE_COLD
+#define LW_NOINLINE_COLD 0
+#endif
+#if LW_NOINLINE_COLD
+#define LW_COLD static __device__ __noinline__
+#else
+#define LW_COLD __device__ __forceinline__
+#endif
 
 constexpr float kPI = 3.14159265358979323846f;
 constexpr float kFRAC_PI_2 = 1.57079632679489661923f;

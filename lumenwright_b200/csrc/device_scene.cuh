@@ -154,12 +154,46 @@ LW_DI float next_boundary(float o, float inv, int cell, int step) {  // trace.rs
     return (bound - o) * inv;
 }
 
-// trace (trace.rs:137-290). The DDA is the reference's step for step; what differs is where
-// the words come from: the brick's top and overlay entries and its occupancy mask are loaded
-// once when the ray enters the brick and kept in registers, and a voxel in an empty 4^3
-// sub-block of a brick without overlay is stepped over without reading its id, since its model
-// is 0 and it tests no quad.
-LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, float tmax) {
+// One DDA step (trace.rs:267-287): to the next voxel along the axis whose boundary is nearest.
+// Written with selects so the lanes of a warp take no branch on the axis. False when the ray
+// leaves the range or the grid.
+struct Dda {
+    int c0, c1, c2;    // the current cell
+    float n0, n1, n2;  // distances to its next boundary along each axis
+    float t;           // distance at which the ray entered the cell
+};
+LW_DI bool dda_advance(Dda &s, V3 o, V3 inv, int s0, int s1, int s2, int gs0, int gs1, int gs2, float t_end) {
+    int axis = s.n0 < s.n1 ? (s.n0 < s.n2 ? 0 : 2) : (s.n1 < s.n2 ? 1 : 2);
+    bool ax0 = axis == 0, ax1 = axis == 1;
+    s.t = ax0 ? s.n0 : (ax1 ? s.n1 : s.n2);
+    if (s.t > t_end) return false;
+    int st = ax0 ? s0 : (ax1 ? s1 : s2);
+    int c = (ax0 ? s.c0 : (ax1 ? s.c1 : s.c2)) + st;
+    int g = ax0 ? gs0 : (ax1 ? gs1 : gs2);
+    if (c < 0 || c >= g) return false;
+    float nb = next_boundary(ax0 ? o.x : (ax1 ? o.y : o.z), ax0 ? inv.x : (ax1 ? inv.y : inv.z), c, st);
+    s.c0 = ax0 ? c : s.c0;
+    s.c1 = ax1 ? c : s.c1;
+    s.c2 = (!ax0 && !ax1) ? c : s.c2;
+    s.n0 = ax0 ? nb : s.n0;
+    s.n1 = ax1 ? nb : s.n1;
+    s.n2 = (!ax0 && !ax1) ? nb : s.n2;
+    return true;
+}
+
+// trace (trace.rs:137-290). The DDA is the reference's step for step; what differs is where the
+// words come from and how the lanes of a warp are kept together:
+//  * the brick's top and overlay entries and its occupancy mask are loaded once when the ray
+//    enters the brick and kept in registers; a voxel in an empty 4^3 sub-block of a brick without
+//    overlay is stepped over without reading its id (its model is 0 and it tests no quad);
+//  * the loop is split in two (a "while-while" traversal): an inner loop steps through empty
+//    bricks and empty voxels until the ray reaches a voxel with a model or overlay quads, then
+//    the quads of that voxel are tested. The lanes of a warp reach the quad tests together
+//    instead of testing quads one lane at a time while the others step.
+// Every visit (brick skip, empty voxel, voxel with quads) counts towards MAX_STEPS as one
+// iteration of the reference's loop does.
+LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, float tmax, uint32_t &steps) {
+    steps = 0;
     const uint32_t dx = P.grid_dims.x, dy = P.grid_dims.y, dz = P.grid_dims.z;
     V3 size = v3((float)(dx * 16u), (float)(dy * 16u), (float)(dz * 16u));
     V3 inv = v3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
@@ -167,131 +201,124 @@ LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, f
     V3 tb = vmul(size - o, inv);
     float t_enter = fmax_r(fmax_r(fmin_r(ta.x, tb.x), fmin_r(ta.y, tb.y)), fmin_r(ta.z, tb.z));
     float t_exit = fmin_r(fmin_r(fmax_r(ta.x, tb.x), fmax_r(ta.y, tb.y)), fmax_r(ta.z, tb.z));
-    float t = fmax_r(t_enter, 0.0f);
-    float t_end = fmin_r(t_exit, tmax);
-    if (t > t_end) return no_hit();
+    float t0 = fmax_r(t_enter, 0.0f);
+    const float t_end = fmin_r(t_exit, tmax);
+    if (t0 > t_end) return no_hit();
 
-    V3 start = o + d * (t + 1e-4f);
+    V3 start = o + d * (t0 + 1e-4f);
     const int gs0 = (int)dx * 16, gs1 = (int)dy * 16, gs2 = (int)dz * 16;
-    int c0 = clamp_i(to_i32(floorf(start.x)), 0, gs0 - 1);
-    int c1 = clamp_i(to_i32(floorf(start.y)), 0, gs1 - 1);
-    int c2 = clamp_i(to_i32(floorf(start.z)), 0, gs2 - 1);
     const int s0 = sgn(d.x), s1 = sgn(d.y), s2 = sgn(d.z);
-    float n0 = next_boundary(o.x, inv.x, c0, s0);
-    float n1 = next_boundary(o.y, inv.y, c1, s1);
-    float n2 = next_boundary(o.z, inv.z, c2, s2);
+    Dda s;
+    s.c0 = clamp_i(to_i32(floorf(start.x)), 0, gs0 - 1);
+    s.c1 = clamp_i(to_i32(floorf(start.y)), 0, gs1 - 1);
+    s.c2 = clamp_i(to_i32(floorf(start.z)), 0, gs2 - 1);
+    s.n0 = next_boundary(o.x, inv.x, s.c0, s0);
+    s.n1 = next_boundary(o.y, inv.y, s.c1, s1);
+    s.n2 = next_boundary(o.z, inv.z, s.c2, s2);
+    s.t = t0;
     const float best_t = t_end + 1e-3f;
 
     uint32_t cur_b = 0xFFFFFFFFu, entry = EMPTY, ov = EMPTY;
     uint2 occ = make_uint2(0u, 0u);
-    for (uint32_t it = 0; it < MAX_STEPS; it++) {
-        uint32_t bx = (uint32_t)(c0 >> 4), by = (uint32_t)(c1 >> 4), bz = (uint32_t)(c2 >> 4);
-        uint32_t b = (by * dz + bz) * dx + bx;
-        if (b != cur_b) {
-            cur_b = b;
-            uint2 e = ldg(S.top + b);
-            entry = e.x;
-            ov = e.y;
-            if (entry != EMPTY && !(entry & UNIFORM)) occ = ldg(S.occ + entry);
-        }
-        if (entry == EMPTY && ov == EMPTY) {
-            // Skip the whole brick: jump to its exit face (trace.rs:184-226).
-            int bc0 = (int)bx, bc1 = (int)by, bc2 = (int)bz;
-            float t_out = kINF;
-            int axis = 0;
-            if (s0 != 0) {
-                float tt = ((float)(s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
-                if (tt < t_out) { t_out = tt; axis = 0; }
+    uint32_t it = 0;
+    for (;;) {
+        // Inner loop: empty space, up to the next voxel with a model or overlay quads.
+        uint32_t model = 0;
+        for (;;) {
+            if (it >= MAX_STEPS) return no_hit();
+            it++;
+            steps = it;
+            uint32_t bx = (uint32_t)(s.c0 >> 4), by = (uint32_t)(s.c1 >> 4), bz = (uint32_t)(s.c2 >> 4);
+            uint32_t b = (by * dz + bz) * dx + bx;
+            if (b != cur_b) {
+                cur_b = b;
+                uint2 e = ldg(S.top + b);
+                entry = e.x;
+                ov = e.y;
+                if (entry != EMPTY && !(entry & UNIFORM)) occ = ldg(S.occ + entry);
             }
-            if (s1 != 0) {
-                float tt = ((float)(s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
-                if (tt < t_out) { t_out = tt; axis = 1; }
-            }
-            if (s2 != 0) {
-                float tt = ((float)(s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
-                if (tt < t_out) { t_out = tt; axis = 2; }
-            }
-            if (t_out > t_end) break;
-            V3 pos = o + d * t_out;
-            c0 = axis == 0 ? (s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
-            c1 = axis == 1 ? (s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
-            c2 = axis == 2 ? (s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
-            int ca = axis == 0 ? c0 : (axis == 1 ? c1 : c2);
-            int ga = axis == 0 ? gs0 : (axis == 1 ? gs1 : gs2);
-            if (ca < 0 || ca >= ga) break;
-            n0 = next_boundary(o.x, inv.x, c0, s0);
-            n1 = next_boundary(o.y, inv.y, c1, s1);
-            n2 = next_boundary(o.z, inv.z, c2, s2);
-            t = t_out;
-            continue;
-        }
-
-        // Block model in this voxel (trace.rs:233-241).
-        uint32_t model;
-        if (entry == EMPTY) {
-            model = 0;
-        } else if (entry & UNIFORM) {
-            model = entry & ~UNIFORM;
-        } else {
-            int lx = c0 & 15, ly = c1 & 15, lz = c2 & 15;
-            uint32_t sb = (uint32_t)(((ly >> 2) * 4 + (lz >> 2)) * 4 + (lx >> 2));
-            uint32_t word = sb < 32u ? occ.x : occ.y;
-            model = (word >> (sb & 31u)) & 1u ? brick_voxel(S, entry, lx, ly, lz) : 0u;
-        }
-        if (model != 0u || ov != EMPTY) {
-            float t_cell_exit = fmin_r(n0, fmin_r(n1, n2));
-            float t_lo = fmax_r(t - 1e-4f, tmin);
-            float t_hi = t_cell_exit + 1e-4f;
-            Hit cand = no_hit();
-            cand.t = fmin_r(t_hi, best_t);
-            if (model != 0u) {
-                uint4 m = ldg(S.models + model);
-                V3 lo = o - v3((float)c0, (float)c1, (float)c2);
-                for (uint32_t i = 0; i < m.y; i++) test_quad(S, P, m.x + i, lo, d, t_lo, cand);
-            }
-            if (ov != EMPTY) {
-                uint32_t local = (uint32_t)((((c1 & 15) * 16 + (c2 & 15)) * 16) + (c0 & 15));
-                size_t base = (size_t)P.off.w + (size_t)ov * OV_CELL_WORDS + local * 2u;
-                uint32_t off = ldg(S.grid + base);
-                uint32_t count = ldg(S.grid + base + 1);
-                for (uint32_t i = 0; i < count; i++) {
-                    uint32_t qi = ldg(S.grid + (size_t)P.off2.x + off + i);
-                    test_quad(S, P, qi, o, d, t_lo, cand);
+            if (entry == EMPTY && ov == EMPTY) {
+                // Skip the whole brick: jump to its exit face (trace.rs:184-226).
+                int bc0 = (int)bx, bc1 = (int)by, bc2 = (int)bz;
+                float t_out = kINF;
+                int axis = 0;
+                if (s0 != 0) {
+                    float tt = ((float)(s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
+                    if (tt < t_out) { t_out = tt; axis = 0; }
                 }
+                if (s1 != 0) {
+                    float tt = ((float)(s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
+                    if (tt < t_out) { t_out = tt; axis = 1; }
+                }
+                if (s2 != 0) {
+                    float tt = ((float)(s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
+                    if (tt < t_out) { t_out = tt; axis = 2; }
+                }
+                if (t_out > t_end) return no_hit();
+                V3 pos = o + d * t_out;
+                s.c0 = axis == 0 ? (s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
+                s.c1 = axis == 1 ? (s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
+                s.c2 = axis == 2 ? (s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
+                int ca = axis == 0 ? s.c0 : (axis == 1 ? s.c1 : s.c2);
+                int ga = axis == 0 ? gs0 : (axis == 1 ? gs1 : gs2);
+                if (ca < 0 || ca >= ga) return no_hit();
+                s.n0 = next_boundary(o.x, inv.x, s.c0, s0);
+                s.n1 = next_boundary(o.y, inv.y, s.c1, s1);
+                s.n2 = next_boundary(o.z, inv.z, s.c2, s2);
+                s.t = t_out;
+                continue;
             }
-            if (cand.quad != NO_QUAD) return cand;
+            // Block model in this voxel (trace.rs:233-241).
+            if (entry == EMPTY) {
+                model = 0;
+            } else if (entry & UNIFORM) {
+                model = entry & ~UNIFORM;
+            } else {
+                int lx = s.c0 & 15, ly = s.c1 & 15, lz = s.c2 & 15;
+                uint32_t sb = (uint32_t)(((ly >> 2) * 4 + (lz >> 2)) * 4 + (lx >> 2));
+                uint32_t word = sb < 32u ? occ.x : occ.y;
+                model = (word >> (sb & 31u)) & 1u ? brick_voxel(S, entry, lx, ly, lz) : 0u;
+            }
+            if (model != 0u || ov != EMPTY) break;
+            if (!dda_advance(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end)) return no_hit();
         }
 
-        // Advance to the next voxel (trace.rs:267-287).
-        int axis = n0 < n1 ? (n0 < n2 ? 0 : 2) : (n1 < n2 ? 1 : 2);
-        if (axis == 0) {
-            t = n0;
-            if (t > t_end) break;
-            c0 += s0;
-            if (c0 < 0 || c0 >= gs0) break;
-            n0 = next_boundary(o.x, inv.x, c0, s0);
-        } else if (axis == 1) {
-            t = n1;
-            if (t > t_end) break;
-            c1 += s1;
-            if (c1 < 0 || c1 >= gs1) break;
-            n1 = next_boundary(o.y, inv.y, c1, s1);
-        } else {
-            t = n2;
-            if (t > t_end) break;
-            c2 += s2;
-            if (c2 < 0 || c2 >= gs2) break;
-            n2 = next_boundary(o.z, inv.z, c2, s2);
+        // The voxel's quads (trace.rs:228-264).
+        float t_cell_exit = fmin_r(s.n0, fmin_r(s.n1, s.n2));
+        float t_lo = fmax_r(s.t - 1e-4f, tmin);
+        float t_hi = t_cell_exit + 1e-4f;
+        Hit cand = no_hit();
+        cand.t = fmin_r(t_hi, best_t);
+        if (model != 0u) {
+            uint4 m = ldg(S.models + model);
+            V3 lo = o - v3((float)s.c0, (float)s.c1, (float)s.c2);
+            for (uint32_t i = 0; i < m.y; i++) test_quad(S, P, m.x + i, lo, d, t_lo, cand);
         }
+        if (ov != EMPTY) {
+            uint32_t local = (uint32_t)((((s.c1 & 15) * 16 + (s.c2 & 15)) * 16) + (s.c0 & 15));
+            size_t base = (size_t)P.off.w + (size_t)ov * OV_CELL_WORDS + local * 2u;
+            uint32_t off = ldg(S.grid + base);
+            uint32_t count = ldg(S.grid + base + 1);
+            for (uint32_t i = 0; i < count; i++) {
+                uint32_t qi = ldg(S.grid + (size_t)P.off2.x + off + i);
+                test_quad(S, P, qi, o, d, t_lo, cand);
+            }
+        }
+        if (cand.quad != NO_QUAD) return cand;
+        if (!dda_advance(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end)) return no_hit();
     }
-    return no_hit();
+}
+
+LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, float tmax) {
+    uint32_t steps;
+    return trace(S, P, o, d, tmin, tmax, steps);
 }
 
 // is_see_through / see_through_hit (trace.rs:113-131).
 LW_DI bool is_see_through(const DevParams &P, uint32_t qi) {
     return qi >= P.see_through.x && qi - P.see_through.x < P.see_through.y;
 }
-LW_DI Hit see_through_hit(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin) {
+LW_COLD Hit see_through_hit(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin) {
     Hit best = no_hit();
     for (uint32_t i = 0; i < P.see_through.y; i++) test_quad(S, P, P.see_through.x + i, o, d, tmin, best);
     return best;

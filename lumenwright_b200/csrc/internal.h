@@ -21,7 +21,7 @@ struct WorkDesc {
     uint32_t *counter;           // work counter (zeroed before the launch)
     float4 *partials;            // [n_sub][n_slots] compensated item sums (accumulating mode)
     float *samples_out;          // per-sample radiance (sample mode), [(py*w+px)*spp + k][3]
-    const volatile int *cancel;  // host-mapped cancel flag: the kernel stops taking items when set
+    const volatile uint32_t *cancel;  // device cancel word: the kernel stops taking items when set
 };
 
 // Per-pixel accumulator: Kahan (sum, compensation), with the sample count in sum.w.
@@ -51,6 +51,13 @@ cudaError_t launch_voxel_lookup(const DevScene &S, const DevParams &P, uint32_t 
 cudaError_t launch_sky_cache(const DevParams &P, uint32_t n, float *out, cudaStream_t st);
 cudaError_t launch_blend_chunky(const DevScene &S, const DevParams &P, float *map, uint32_t w, uint32_t h, float weight,
                                 cudaStream_t st);
+
+// refport.cu
+cudaError_t launch_refport(const void *grid, const void *models, const void *ref_quads, const void *atlas,
+                           const void *emitters, const void *egrid, const float *sky, const float *gamma,
+                           const DevScene &Sv, const DevParams &P, float4 *accum, uint32_t sample_start, uint32_t n,
+                           cudaStream_t st);
+cudaError_t launch_refport_finalize(const float4 *acc, uint32_t n, float *out, cudaStream_t st);
 
 // scene.cu
 struct SceneUploadDesc {

@@ -360,13 +360,26 @@ LW_DI void kahan_add(float &s, float &c, float x) {
 
 LW_DI bool finite3(V3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
 
+#ifndef LW_STATS
+#define LW_STATS 0
+#endif
+#if LW_STATS
+// Divergence counters of the instrumented build (not part of the product build):
+// [0] loop iterations per warp, [1] lanes active in them, [2] lanes tracing, [3] lane DDA
+// steps, [4] warp DDA steps (the slowest lane's), [5..7] lanes shading a path/shadow/emitter
+// ray, [8] lanes ending a path, [9] iterations with a lane taking work
+__device__ unsigned long long g_stats[16];
+#endif
 constexpr int kThreads = 128;
+#ifndef LW_MIN_BLOCKS
+#define LW_MIN_BLOCKS 4
+#endif
 
 // The persistent render kernel. Each lane takes an item (sub consecutive samples of one pixel),
 // traces its samples one after another, and takes the next item as soon as it is done; each
 // loop iteration traces one ray per active lane.
 template <int MODE>
-__global__ void __launch_bounds__(kThreads) k_render(const DevScene S, const DevParams P, const WorkDesc W) {
+__global__ void __launch_bounds__(kThreads, LW_MIN_BLOCKS) k_render(const DevScene S, const DevParams P, const WorkDesc W) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned FULL = 0xFFFFFFFFu;
     Path p;
@@ -381,7 +394,10 @@ __global__ void __launch_bounds__(kThreads) k_render(const DevScene S, const Dev
             uint32_t base = 0;
             int leader = __ffs(mask) - 1;
             if ((int)lane == leader) {
-                base = *W.cancel ? W.n_items : atomicAdd(W.counter, (uint32_t)__popc(mask));
+                uint32_t n = (uint32_t)__popc(mask);
+                base = atomicAdd(W.counter, n);
+                // The cancel word is polled once per 4096 items taken, not on every take.
+                if ((base & 4095u) < n && *W.cancel) base = W.n_items;
             }
             base = __shfl_sync(FULL, base, leader);
             if (need) {
@@ -407,10 +423,47 @@ __global__ void __launch_bounds__(kThreads) k_render(const DevScene S, const Dev
             }
         }
         if (__all_sync(FULL, exhausted)) break;
+#if LW_STATS
+        {
+            unsigned act = __ballot_sync(FULL, active);
+            if (lane == 0) {
+                atomicAdd(&g_stats[0], 1ull);
+                atomicAdd(&g_stats[1], (unsigned long long)__popc(act));
+                if (mask) atomicAdd(&g_stats[9], 1ull);
+            }
+        }
+#endif
         if (!active) continue;
 
+#if LW_STATS
+        uint32_t steps = 0;
+        Hit h = trace(S, P, p.o, p.d, p.tmin, p.tmax, steps);
+        {
+            unsigned am = __activemask();
+            uint32_t lsum = __reduce_add_sync(am, steps), lmax = __reduce_max_sync(am, steps);
+            uint32_t kind = p.kind;
+            unsigned k0 = __ballot_sync(am, kind == K_EXTEND), k1 = __ballot_sync(am, kind == K_SHADOW);
+            unsigned k2 = __ballot_sync(am, kind == K_EMIT);
+            if ((int)lane == __ffs(am) - 1) {
+                atomicAdd(&g_stats[2], (unsigned long long)__popc(am));
+                atomicAdd(&g_stats[3], (unsigned long long)lsum);
+                atomicAdd(&g_stats[4], (unsigned long long)lmax);
+                atomicAdd(&g_stats[5], (unsigned long long)__popc(k0));
+                atomicAdd(&g_stats[6], (unsigned long long)__popc(k1));
+                atomicAdd(&g_stats[7], (unsigned long long)__popc(k2));
+            }
+        }
+#else
         Hit h = trace(S, P, p.o, p.d, p.tmin, p.tmax);
+#endif
         Act a = shade(p, S, P, h);
+#if LW_STATS
+        {
+            unsigned am = __activemask();
+            unsigned e = __ballot_sync(am, a == A_END);
+            if ((int)lane == __ffs(am) - 1) atomicAdd(&g_stats[8], (unsigned long long)__popc(e));
+        }
+#endif
         if (a == A_END) {
             if (MODE == MODE_SAMPLES) {
                 size_t at = ((size_t)((py - W.y0) * W.w + (px - W.x0)) * W.spp + (sample - W.sample_start)) * 3u;
@@ -485,6 +538,18 @@ __global__ void k_voxel_lookup(const DevScene S, const DevParams P, uint32_t n, 
     if (i >= n) return;
     out[i] = voxel(S, P, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
 }
+
+#if LW_STATS
+extern "C" int lw_debug_counters(unsigned long long *out, int reset) {
+    cudaDeviceSynchronize();
+    if (cudaMemcpyFromSymbol(out, g_stats, sizeof(g_stats)) != cudaSuccess) return 1;
+    if (reset) {
+        unsigned long long z[16] = {};
+        cudaMemcpyToSymbol(g_stats, z, sizeof(z));
+    }
+    return 0;
+}
+#endif
 
 LaunchShape render_shape(int mode, int device) {
     int sms = 0, per_sm = 0;

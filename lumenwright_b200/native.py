@@ -28,7 +28,7 @@ EXPORTS = (
     "lw_elapsed_ms",
     "lw_scene_upload", "lw_render_hq", "lw_sky_upload", "lw_clear_accumulator", "lw_render_device",
     "lw_read_accumulator", "lw_render_samples", "lw_trace_rays", "lw_voxel_lookup", "lw_build_sky_cache",
-    "lw_blend_chunky_sky",
+    "lw_blend_chunky_sky", "lw_render_hq_reference_port",
 )
 
 
@@ -98,6 +98,7 @@ def load(path: str = LIB_PATH):
     L.lw_trace_rays.argtypes = [P, P, C.c_uint32, P, P, C.c_float, C.c_float, P]
     L.lw_voxel_lookup.argtypes = [P, C.c_uint32, P, P]
     L.lw_build_sky_cache.argtypes = [P, P, C.c_uint32, P]
+    L.lw_render_hq_reference_port.argtypes = [P, P, P, C.c_uint64, C.c_uint32, P]
     L.lw_blend_chunky_sky.argtypes = [P, P, P, C.c_uint64, P, P, C.c_float]
     for name in EXPORTS:
         if name not in ("lw_ctx_destroy", "lw_last_error", "lw_stream", "lw_cancel"):
@@ -197,6 +198,17 @@ class Context:
         out = np.zeros((h, w, 3), np.float32)
         cb = PROGRESS_FN((lambda d, t, u: progress(d, t)) if progress else (lambda d, t, u: None))
         self._check(self.L.lw_render_hq(self.h, p.ctypes.data, _ptr(sky), sky.size, spp, cb, None, out.ctypes.data))
+        return out
+
+    def render_hq_reference_port(self, params, sky, spp):
+        """The reference's CUDA backend ported as written (the comparison baseline): mean radiance,
+        shape (h, w, 3)."""
+        p = self._params(params)
+        sky = np.ascontiguousarray(sky if sky is not None else np.zeros(0), np.float32)
+        w, h = int(p["frame"][0]), int(p["frame"][1])
+        out = np.zeros((h, w, 3), np.float32)
+        self._check(self.L.lw_render_hq_reference_port(self.h, p.ctypes.data, _ptr(sky), sky.size, spp,
+                                                        out.ctypes.data))
         return out
 
     def upload_sky(self, sky):

@@ -1,0 +1,64 @@
+"""The multi-GPU sample sharding on the host: two gloo ranks render their sample ranges of a small
+frame with the CPU oracle, reduce their means to rank 0, and the result equals one process
+rendering every sample. CPU only (world size 2)."""
+
+import os
+import socket
+
+import numpy as np
+import torch.multiprocessing as mp
+
+from kernel_fixtures import lamp_scene
+from lumenwright_b200 import layout as L
+from lumenwright_b200 import shard
+
+
+def frame_scene():
+    ks = lamp_scene(L.EMITTER_SAMPLING_ONE, True)
+    p = ks.params
+    p["frame"] = [12, 8, 0, 3]
+    p["cam_pos"] = [8.0, 12.0, 8.0, 0.9]
+    p["cam_fwd"] = [0.0, -1.0, 0.0, 1.5]
+    p["cam_right"] = [1.0, 0.0, 0.0, 0.0]
+    p["cam_up"] = [0.0, 0.0, -1.0, 0.0]
+    p["sun_dir"] = [0.3, 0.9, 0.316, 0.9995]
+    p["sun_color"] = [1.0, 0.9, 0.8, 0.03]
+    return ks
+
+
+def mean_of_range(start, count):
+    from oracle import oracle as O
+    ks = frame_scene()
+    s = O.OracleScene(*ks.buffers()).render_samples(0, 0, 12, 8, start, count)
+    s = np.where(np.isfinite(s).all(-1, keepdims=True), s, 0.0)
+    return s.astype(np.float64).sum(2).astype(np.float32) / np.float32(count)
+
+
+def worker(rank, world, port, out):
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    start, count = shard.sample_range(rank, world, 8, step=1)
+    m = shard.reduce_means(mean_of_range(start, count), dist)
+    if rank == 0:
+        np.save(out, m)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def test_two_ranks_give_the_single_process_frame(tmp_path):
+    out = str(tmp_path / "m.npy")
+    mp.start_processes(worker, args=(2, free_port(), out), nprocs=2, join=True, start_method="spawn")
+    got = np.load(out)
+    assert shard.sample_range(0, 2, 8, 1) == (16, 8) and shard.sample_range(1, 2, 8, 1) == (24, 8)
+    want = mean_of_range(16, 16)
+    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6)
