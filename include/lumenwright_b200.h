@@ -155,6 +155,24 @@ lw_status lw_clear_accumulator(lw_ctx *ctx, uint32_t width, uint32_t height);
 lw_status lw_render_device(lw_ctx *ctx, const lw_params *params, uint32_t sample_start, uint32_t spp);
 lw_status lw_read_accumulator(lw_ctx *ctx, float *out_rgb);
 
+/* ---- allocation-free rendering ---------------------------------------------------------------
+ * No counterpart in the reference. For callers that must not allocate device memory once they run
+ * (an application that owns the GPU's memory budget, a per-frame loop that must not stall on
+ * cudaMalloc/cudaFree): after lw_ctx_create, lw_scene_upload and lw_sky_upload (which allocate),
+ * this adds samples [sample_start, sample_start + spp) of every pixel to `accum`, a device buffer
+ * the caller owns of frame[0] * frame[1] records of 8 floats (Kahan sum r, g, b, sample count;
+ * compensation r, g, b, unused; zero it before the first call), and allocates nothing: the
+ * render kernel's work counter and item sums live in a fixed 32 MiB array inside the library.
+ * The mean of a pixel is (sum - compensation) / count. Frames of more than 2,097,152 pixel slots
+ * (8x4-pixel tiles, about 1920x1088) are refused with LW_ERR_INVALID_ARGUMENT. The work is queued
+ * on the context's stream (lw_stream) and the call returns without waiting. Every call on every
+ * context of a device shares the one array: calls whose work overlaps on the GPU (from several
+ * threads, contexts or streams) race on it and must be serialised by the caller. The first call on
+ * a device looks the array's address up (cudaGetSymbolAddress); make that first call before any
+ * stream capture. */
+lw_status lw_render_accumulate_noalloc(lw_ctx *ctx, const lw_params *params, uint32_t sample_start, uint32_t spp,
+                                       void *accum);
+
 /* ---- parity entry points (the reference's kernel functions, one call per query) ----------
  * Per-sample radiance of `render_sample` (crates/lumenwright-kernel/src/integrator.rs:539-709)
  * for samples [sample_start, sample_start + count) of every pixel of the rectangle

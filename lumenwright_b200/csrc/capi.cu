@@ -517,6 +517,39 @@ lw_status lw_render_device(lw_ctx *c, const lw_params *params, uint32_t sample_s
     return render_batches(c, params, sample_start, spp, nullptr, nullptr, spp);
 }
 
+lw_status lw_render_accumulate_noalloc(lw_ctx *c, const lw_params *params, uint32_t sample_start, uint32_t spp,
+                                       void *accum) {
+    if (!c || !params || !accum || spp == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument or spp 0");
+    cudaSetDevice(c->device);
+    lw_status s = check_params(c, params, true);
+    if (s != LW_OK) return s;
+    const uint32_t w = params->frame[0], h = params->frame[1];
+    WorkDesc probe = work(c, 0, 0, w, h, 0, 1, 1);
+    if ((size_t)probe.n_slots > kNoallocPartials)
+        return fail(c, LW_ERR_INVALID_ARGUMENT,
+                    "a %ux%u frame needs %u pixel slots; the allocation-free entry point holds %zu (about 1920x1088)",
+                    w, h, probe.n_slots, kNoallocPartials);
+    float4 *scratch = nullptr;
+    CK(c, noalloc_scratch(c->device, &scratch), "looking up the scratch array");
+    Plan pl = plan(c, probe.n_slots, spp);
+    uint64_t subs = kNoallocPartials / probe.n_slots;
+    uint64_t batch = subs * pl.sub < spp ? subs * pl.sub : spp;
+    DevScene S = dev_scene(c);
+    DevParams P = dev_params(params);
+    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
+    for (uint32_t done = 0; done < spp;) {
+        uint32_t n = spp - done < batch ? spp - done : (uint32_t)batch;
+        WorkDesc W = work(c, 0, 0, w, h, sample_start + done, n, pl.sub);
+        W.counter = (uint32_t *)scratch;  // the header's first word; the item sums follow it
+        W.partials = scratch + 16;
+        CK(c, cudaMemsetAsync(W.counter, 0, sizeof(uint32_t), c->stream), "clearing the work counter");
+        CK(c, launch_render(MODE_ACCUM, S, P, W, c->shape_accum, c->stream), "launching the render kernel");
+        CK(c, launch_reduce(W, (Accum *)accum, w, c->stream), "launching the reduction");
+        done += n;
+    }
+    return LW_OK;
+}
+
 lw_status lw_read_accumulator(lw_ctx *c, float *out_rgb) {
     if (!c || !out_rgb) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
     cudaSetDevice(c->device);

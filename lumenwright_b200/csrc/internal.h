@@ -59,6 +59,10 @@ cudaError_t launch_refport(const void *grid, const void *models, const void *ref
                            cudaStream_t st);
 cudaError_t launch_refport_finalize(const float4 *acc, uint32_t n, float *out, cudaStream_t st);
 
+// noalloc.cu: the fixed scratch array of the allocation-free entry point.
+extern const size_t kNoallocPartials;
+cudaError_t noalloc_scratch(int device, float4 **out);
+
 // scene.cu
 struct SceneUploadDesc {
     const uint32_t *grid;  // device copy of the reference grid

@@ -28,7 +28,7 @@ EXPORTS = (
     "lw_elapsed_ms",
     "lw_scene_upload", "lw_render_hq", "lw_sky_upload", "lw_clear_accumulator", "lw_render_device",
     "lw_read_accumulator", "lw_render_samples", "lw_trace_rays", "lw_voxel_lookup", "lw_build_sky_cache",
-    "lw_blend_chunky_sky", "lw_render_hq_reference_port",
+    "lw_blend_chunky_sky", "lw_render_hq_reference_port", "lw_render_accumulate_noalloc",
 )
 
 
@@ -98,6 +98,7 @@ def load(path: str = LIB_PATH):
     L.lw_trace_rays.argtypes = [P, P, C.c_uint32, P, P, C.c_float, C.c_float, P]
     L.lw_voxel_lookup.argtypes = [P, C.c_uint32, P, P]
     L.lw_build_sky_cache.argtypes = [P, P, C.c_uint32, P]
+    L.lw_render_accumulate_noalloc.argtypes = [P, P, C.c_uint32, C.c_uint32, P]
     L.lw_render_hq_reference_port.argtypes = [P, P, P, C.c_uint64, C.c_uint32, P]
     L.lw_blend_chunky_sky.argtypes = [P, P, P, C.c_uint64, P, P, C.c_float]
     for name in EXPORTS:
@@ -222,6 +223,14 @@ class Context:
         p = self._params(params)
         self._keep = [p]
         self._check(self.L.lw_render_device(self.h, p.ctypes.data, sample_start, spp))
+
+    def render_accumulate_noalloc(self, params, sample_start, spp, accum_device_ptr: int):
+        """Adds samples to a caller-owned device accumulator (w*h records of 8 floats) without
+        allocating; queued on the context's stream."""
+        p = self._params(params)
+        self._keep = [p]
+        self._check(self.L.lw_render_accumulate_noalloc(self.h, p.ctypes.data, sample_start, spp,
+                                                         C.c_void_p(accum_device_ptr)))
 
     def read_accumulator(self, w, h):
         out = np.zeros((h, w, 3), np.float32)
