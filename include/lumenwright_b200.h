@@ -112,6 +112,16 @@ typedef struct {
     uint64_t samples;        /* path samples traced */
 } lw_stats;
 
+/* Launch tuning of the render kernel (the autotuner's knobs): threads per block (64, 128 or 256),
+ * the regrouping period (voxel visits a ray advances per loop iteration before its lane may shade
+ * and start its next ray; 0 = a whole traversal at once), and the samples per work item (0: chosen
+ * from the frame so every lane gets many items). */
+typedef struct {
+    uint32_t threads;
+    uint32_t budget;
+    uint32_t sub;
+} lw_tuning;
+
 /* ---- context ------------------------------------------------------------------------------
  * Replaces CudaBackend::new (crates/lumenwright/src/render/cuda.rs:55-63): opens `device`,
  * checks it is sm_100, creates the context's streams. */
@@ -122,6 +132,9 @@ const char *lw_last_error(const lw_ctx *ctx);
 /* The CUDA stream (cudaStream_t) the context launches its path-tracing kernels on. */
 void *lw_stream(lw_ctx *ctx);
 lw_status lw_get_stats(const lw_ctx *ctx, lw_stats *out);
+/* Sets / reads the launch tuning of a context (defaults: 128 threads, budget 0, sub automatic). */
+lw_status lw_set_tuning(lw_ctx *ctx, const lw_tuning *tuning);
+lw_status lw_get_tuning(const lw_ctx *ctx, lw_tuning *out);
 /* Asks a running render on `ctx` to stop; it returns LW_ERR_CANCELLED. Safe from any thread. */
 void lw_cancel(lw_ctx *ctx);
 /* Records timing mark `slot` (0..7), a CUDA event on the context's stream, and reads the time
@@ -154,6 +167,27 @@ lw_status lw_sky_upload(lw_ctx *ctx, const float *sky, uint64_t sky_len);
 lw_status lw_clear_accumulator(lw_ctx *ctx, uint32_t width, uint32_t height);
 lw_status lw_render_device(lw_ctx *ctx, const lw_params *params, uint32_t sample_start, uint32_t spp);
 lw_status lw_read_accumulator(lw_ctx *ctx, float *out_rgb);
+
+/* ---- the batched form ----------------------------------------------------------------------
+ * Many cameras of uneven resolution and spp over the uploaded scene in one persistent launch:
+ * every camera's work items go into one queue, so the GPU stays full until the last sample of
+ * the last camera. lw_batch_prepare uploads the cameras' skies (once per distinct host buffer),
+ * lays out their accumulators and partial sums, and captures clear + render + reduce into a CUDA
+ * graph; lw_batch_run replays the graph (asynchronously, on lw_stream); lw_batch_read waits and
+ * copies each camera's mean radiance to its `out_rgb` (skipped when NULL). lw_render_batch does
+ * all three. A camera's image is what lw_render_hq gives for the same Params, sky and spp. */
+typedef struct {
+    lw_params params;      /* the camera's frame: camera, frame size, bounces, sky and sun settings */
+    const float *sky;      /* the camera's sky buffer (HqFrame.sky) */
+    uint64_t sky_len;
+    uint32_t spp;          /* samples per pixel (at least 1) */
+    uint32_t sample_start; /* first sample index (0 for a fresh frame) */
+    float *out_rgb;        /* frame[0] * frame[1] * 3 floats, or NULL */
+} lw_camera_job;
+lw_status lw_batch_prepare(lw_ctx *ctx, const lw_camera_job *jobs, uint32_t n);
+lw_status lw_batch_run(lw_ctx *ctx);
+lw_status lw_batch_read(lw_ctx *ctx);
+lw_status lw_render_batch(lw_ctx *ctx, const lw_camera_job *jobs, uint32_t n);
 
 /* ---- allocation-free rendering ---------------------------------------------------------------
  * No counterpart in the reference. For callers that must not allocate device memory once they run

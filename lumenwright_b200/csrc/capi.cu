@@ -91,6 +91,19 @@ struct lw_ctx {
     DBuf<uint32_t> cancel_word;      // device word the render kernel polls; set by lw_cancel
     cudaStream_t aux = nullptr;      // lw_cancel's stream, so the write lands while a render runs
     lw_stats stats{};
+    lw_tuning tuning{128, 0, 0};
+    // the batched form
+    struct BatchSky { const float *host; uint64_t len; DBuf<float> dev; };
+    std::vector<BatchSky *> batch_skies;
+    DBuf<DevJob> batch_jobs;
+    DBuf<uint32_t> batch_item_begin, batch_slot_begin;
+    DBuf<Accum> batch_acc;
+    DBuf<float> batch_out;
+    DBuf<float4> batch_partials;
+    std::vector<lw_camera_job> batch_host;
+    std::vector<size_t> batch_out_off;
+    cudaGraphExec_t batch_graph = nullptr;
+    uint64_t batch_samples = 0;
     size_t partials_cap_bytes = size_t(4) << 30;
 };
 
@@ -155,7 +168,8 @@ DevScene dev_scene(const lw_ctx *c) {
 
 // Checks a frame's Params against the uploaded scene and sky: every index the kernels form from
 // them stays inside its buffer.
-lw_status check_params(lw_ctx *c, const lw_params *p, bool need_frame) {
+lw_status check_params(lw_ctx *c, const lw_params *p, bool need_frame, uint64_t sky_len = UINT64_MAX) {
+    if (sky_len == UINT64_MAX) sky_len = c->sky_len;
     if (!p) return fail(c, LW_ERR_INVALID_ARGUMENT, "params is null");
     if (!c->has_scene) return fail(c, LW_ERR_NO_SCENE, "no scene uploaded");
     for (int a = 0; a < 3; a++)
@@ -175,14 +189,14 @@ lw_status check_params(lw_ctx *c, const lw_params *p, bool need_frame) {
         double lens = (double)(uint64_t)p->sky_map[0] * (uint64_t)p->sky_map[1];
         double light = (double)(uint64_t)p->sky_map[2] * (uint64_t)p->sky_map[3];
         if (!(p->sky_map[1] >= 1.0f && p->sky_map[2] >= 1.0f && p->sky_map[3] >= 1.0f) ||
-            (lens + light) * 3.0 > (double)c->sky_len || p->sky_map[0] * p->sky_map[1] >= 4294967040.0f)
+            (lens + light) * 3.0 > (double)sky_len || p->sky_map[0] * p->sky_map[1] >= 4294967040.0f)
             return fail(c, LW_ERR_BUFFER_LENGTH, "sky maps %gx%g + %gx%g need more than the %llu sky floats", p->sky_map[0],
-                        p->sky_map[1], p->sky_map[2], p->sky_map[3], (unsigned long long)c->sky_len);
+                        p->sky_map[1], p->sky_map[2], p->sky_map[3], (unsigned long long)sky_len);
     } else if (p->misc_f[2] >= 1.0f) {
         double n = std::floor((double)p->misc_f[2]);
-        if ((n + 1.0) * (n + 1.0) * 3.0 > (double)c->sky_len)
+        if ((n + 1.0) * (n + 1.0) * 3.0 > (double)sky_len)
             return fail(c, LW_ERR_BUFFER_LENGTH, "sky cache of resolution %g needs %g floats, %llu given", n,
-                        (n + 1.0) * (n + 1.0) * 3.0, (unsigned long long)c->sky_len);
+                        (n + 1.0) * (n + 1.0) * 3.0, (unsigned long long)sky_len);
     }
     return LW_OK;
 }
@@ -203,6 +217,7 @@ Plan plan(const lw_ctx *c, uint64_t n_slots, uint32_t spp) {
     uint64_t total = n_slots * spp;
     uint64_t sub = total / (lanes * 16ull + 1ull);
     sub = sub < 1 ? 1 : (sub > 16 ? 16 : sub);
+    if (c->tuning.sub) sub = c->tuning.sub;
     uint64_t max_items = c->partials_cap_bytes / sizeof(float4);
     uint64_t max_sub_per_launch = max_items / (n_slots ? n_slots : 1);
     if (max_sub_per_launch < 1) max_sub_per_launch = 1;
@@ -225,6 +240,7 @@ WorkDesc work(lw_ctx *c, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint3
     W.sub = sub;
     W.n_sub = (spp + sub - 1) / sub;
     W.n_items = W.n_slots * W.n_sub;
+    W.budget = c->tuning.budget;
     W.counter = c->counter.p;
     W.partials = c->partials.p;
     W.samples_out = c->samples.p;
@@ -312,8 +328,8 @@ lw_status lw_ctx_create(int device, lw_ctx **out) {
     if ((e = ensure(c->gamma, 256)) != cudaSuccess) return bail(e, "allocating the gamma table");
     if ((e = cudaMemcpy(c->gamma.p, lut, sizeof lut, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "uploading the gamma table");
     if ((e = ensure(c->counter, 1)) != cudaSuccess || (e = ensure(c->error, 1)) != cudaSuccess) return bail(e, "allocating counters");
-    c->shape_accum = render_shape(MODE_ACCUM, device);
-    c->shape_samples = render_shape(MODE_SAMPLES, device);
+    c->shape_accum = render_shape(MODE_ACCUM, device, (int)c->tuning.threads);
+    c->shape_samples = render_shape(MODE_SAMPLES, device, (int)c->tuning.threads);
     *out = c;
     return LW_OK;
 }
@@ -331,6 +347,14 @@ void lw_ctx_destroy(lw_ctx *c) {
     c->emitters.free_();
     c->partials.free_();
     c->ref_quads.free_();
+    if (c->batch_graph) cudaGraphExecDestroy(c->batch_graph);
+    for (auto *b : c->batch_skies) { b->dev.free_(); delete b; }
+    c->batch_jobs.free_();
+    c->batch_item_begin.free_();
+    c->batch_slot_begin.free_();
+    c->batch_acc.free_();
+    c->batch_out.free_();
+    c->batch_partials.free_();
     for (auto *b : {&c->sky, &c->gamma, &c->out_rgb, &c->samples, &c->rays}) b->free_();
     c->acc.free_();
     c->hits.free_();
@@ -355,6 +379,24 @@ void lw_cancel(lw_ctx *c) {
     __atomic_store_n(c->cancel_host, 1, __ATOMIC_RELAXED);
     cudaSetDevice(c->device);
     cudaMemsetAsync(c->cancel_word.p, 0xFF, 4, c->aux);  // lands while a render kernel runs
+}
+
+lw_status lw_set_tuning(lw_ctx *c, const lw_tuning *t) {
+    if (!c || !t) return LW_ERR_INVALID_ARGUMENT;
+    if (t->threads != 64 && t->threads != 128 && t->threads != 256)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "threads per block %u (64, 128 or 256)", t->threads);
+    if (t->sub > 4096) return fail(c, LW_ERR_INVALID_ARGUMENT, "sub %u", t->sub);
+    cudaSetDevice(c->device);
+    c->tuning = *t;
+    c->shape_accum = render_shape(MODE_ACCUM, c->device, (int)t->threads);
+    c->shape_samples = render_shape(MODE_SAMPLES, c->device, (int)t->threads);
+    return LW_OK;
+}
+
+lw_status lw_get_tuning(const lw_ctx *c, lw_tuning *out) {
+    if (!c || !out) return LW_ERR_INVALID_ARGUMENT;
+    *out = c->tuning;
+    return LW_OK;
 }
 
 lw_status lw_mark(lw_ctx *c, uint32_t slot) {
@@ -690,6 +732,140 @@ lw_status lw_render_hq_reference_port(lw_ctx *c, const lw_params *params, const 
     }
     acc.free_();
     return result;
+}
+
+lw_status lw_batch_prepare(lw_ctx *c, const lw_camera_job *jobs, uint32_t n) {
+    if (!c || !jobs || n == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "no cameras");
+    cudaSetDevice(c->device);
+    if (c->batch_graph) {
+        cudaGraphExecDestroy(c->batch_graph);
+        c->batch_graph = nullptr;
+    }
+    // Skies: one device copy per distinct host buffer.
+    std::vector<const float *> sky_dev(n);
+    for (uint32_t i = 0; i < n; i++) {
+        lw_ctx::BatchSky *found = nullptr;
+        for (auto *b : c->batch_skies)
+            if (b->host == jobs[i].sky && b->len == jobs[i].sky_len) found = b;
+        if (!found) {
+            found = new lw_ctx::BatchSky{jobs[i].sky, jobs[i].sky_len, {}};
+            c->batch_skies.push_back(found);
+            if (jobs[i].sky_len) {
+                CK(c, ensure(found->dev, jobs[i].sky_len), "allocating a sky");
+                CK(c, cudaMemcpyAsync(found->dev.p, jobs[i].sky, jobs[i].sky_len * 4, cudaMemcpyHostToDevice, c->stream),
+                   "uploading a sky");
+            }
+        }
+        sky_dev[i] = found->dev.p;
+        lw_status s = check_params(c, &jobs[i].params, true, jobs[i].sky_len);
+        if (s != LW_OK) return s;
+        if (jobs[i].spp == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "camera %u has spp 0", i);
+    }
+    // Layout: items, slots, accumulators, images, item sums.
+    uint64_t total_samples = 0;
+    for (uint32_t i = 0; i < n; i++) total_samples += (uint64_t)jobs[i].params.frame[0] * jobs[i].params.frame[1] * jobs[i].spp;
+    uint64_t sub = (total_samples + (256ull << 20) - 1) / (256ull << 20);
+    sub = sub < 1 ? 1 : (sub > 64 ? 64 : sub);
+    if (c->tuning.sub) sub = c->tuning.sub;
+    std::vector<DevJob> dj(n);
+    std::vector<uint32_t> ib(n), sb(n);
+    uint64_t items = 0, slots = 0, pixels = 0, partials = 0;
+    c->batch_out_off.assign(n, 0);
+    for (uint32_t i = 0; i < n; i++) {
+        const lw_params &p = jobs[i].params;
+        DevJob &J = dj[i];
+        J.P = dev_params(&p);
+        J.sky = sky_dev[i];
+        J.w = p.frame[0];
+        J.h = p.frame[1];
+        J.tiles_x = (J.w + 7) / 8;
+        J.n_slots = J.tiles_x * ((J.h + 3) / 4) * 32u;
+        J.sample_start = jobs[i].sample_start;
+        J.spp = jobs[i].spp;
+        J.sub = (uint32_t)(sub < J.spp ? sub : J.spp);
+        J.n_sub = (J.spp + J.sub - 1) / J.sub;
+        J.item_begin = (uint32_t)items;
+        J.slot_begin = (uint32_t)slots;
+        J.partial_off = partials;
+        J.acc = nullptr;
+        J.out = nullptr;
+        ib[i] = J.item_begin;
+        sb[i] = J.slot_begin;
+        items += (uint64_t)J.n_slots * J.n_sub;
+        slots += J.n_slots;
+        partials += (uint64_t)J.n_slots * J.n_sub;
+        c->batch_out_off[i] = (size_t)pixels;
+        pixels += (uint64_t)J.w * J.h;
+    }
+    if (items >= 0xFFFFFFFFull || slots >= 0xFFFFFFFFull)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "the batch has %llu work items; at most 2^32 - 1 fit one launch",
+                    (unsigned long long)items);
+    CK(c, ensure(c->batch_acc, pixels), "allocating the accumulators");
+    CK(c, ensure(c->batch_out, 3 * pixels), "allocating the images");
+    CK(c, ensure(c->batch_partials, partials), "allocating the item sums");
+    for (uint32_t i = 0; i < n; i++) {
+        dj[i].acc = c->batch_acc.p + c->batch_out_off[i];
+        dj[i].out = c->batch_out.p + 3 * c->batch_out_off[i];
+    }
+    CK(c, ensure(c->batch_jobs, n), "allocating the job table");
+    CK(c, ensure(c->batch_item_begin, n), "allocating the job table");
+    CK(c, ensure(c->batch_slot_begin, n), "allocating the job table");
+    CK(c, cudaMemcpyAsync(c->batch_jobs.p, dj.data(), sizeof(DevJob) * n, cudaMemcpyHostToDevice, c->stream), "uploading jobs");
+    CK(c, cudaMemcpyAsync(c->batch_item_begin.p, ib.data(), 4 * n, cudaMemcpyHostToDevice, c->stream), "uploading jobs");
+    CK(c, cudaMemcpyAsync(c->batch_slot_begin.p, sb.data(), 4 * n, cudaMemcpyHostToDevice, c->stream), "uploading jobs");
+    CK(c, cudaStreamSynchronize(c->stream), "uploading jobs");
+    BatchDesc B{c->batch_jobs.p, c->batch_item_begin.p, c->batch_slot_begin.p, n, (uint32_t)items, (uint32_t)slots,
+                c->tuning.budget, c->counter.p, c->batch_partials.p, c->cancel_word.p};
+    LaunchShape shape = batch_shape(c->device, (int)c->tuning.threads, c->tuning.budget != 0);
+    // Clear, render, reduce: one CUDA graph, replayed by lw_batch_run.
+    cudaGraph_t graph = nullptr;
+    CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "starting the graph capture");
+    cudaError_t e = cudaMemsetAsync(c->counter.p, 0, 4, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->batch_acc.p, 0, sizeof(Accum) * pixels, c->stream);
+    if (e == cudaSuccess) e = launch_render_batch(dev_scene(c), B, shape, c->stream);
+    if (e == cudaSuccess) e = launch_reduce_batch(B, c->stream);
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&c->batch_graph, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(c, e, "capturing the batch graph");
+    c->batch_host.assign(jobs, jobs + n);
+    c->batch_samples = total_samples;
+    return LW_OK;
+}
+
+lw_status lw_batch_run(lw_ctx *c) {
+    if (!c || !c->batch_graph) return fail(c, LW_ERR_INVALID_ARGUMENT, "no batch prepared");
+    cudaSetDevice(c->device);
+    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
+    CK(c, cudaEventRecord(c->ev_a, c->stream), "recording an event");
+    CK(c, cudaGraphLaunch(c->batch_graph, c->stream), "launching the batch graph");
+    CK(c, cudaEventRecord(c->ev_b, c->stream), "recording an event");
+    c->stats.launches = 1;
+    c->stats.samples = c->batch_samples;
+    c->stats.kernel_ms = -1.0;
+    return LW_OK;
+}
+
+lw_status lw_batch_read(lw_ctx *c) {
+    if (!c || !c->batch_graph) return fail(c, LW_ERR_INVALID_ARGUMENT, "no batch prepared");
+    cudaSetDevice(c->device);
+    for (size_t i = 0; i < c->batch_host.size(); i++) {
+        const lw_camera_job &j = c->batch_host[i];
+        if (!j.out_rgb) continue;
+        size_t n = (size_t)j.params.frame[0] * j.params.frame[1] * 3;
+        CK(c, cudaMemcpyAsync(j.out_rgb, c->batch_out.p + 3 * c->batch_out_off[i], n * 4, cudaMemcpyDeviceToHost, c->stream),
+           "reading an image");
+    }
+    CK(c, cudaStreamSynchronize(c->stream), "reading the images");
+    return LW_OK;
+}
+
+lw_status lw_render_batch(lw_ctx *c, const lw_camera_job *jobs, uint32_t n) {
+    lw_status s = lw_batch_prepare(c, jobs, n);
+    if (s == LW_OK) s = lw_batch_run(c);
+    if (s == LW_OK) s = lw_batch_read(c);
+    return s;
 }
 
 lw_status lw_build_sky_cache(lw_ctx *c, const lw_params *params, uint32_t n, float *out) {

@@ -36,6 +36,10 @@ constexpr uint32_t MAX_EVENTS = 48u;    // integrator.rs:24
 constexpr uint32_t NO_QUAD = 0xFFFFFFFFu;
 constexpr float COPLANAR = 1e-5f;       // trace.rs:73
 
+#ifndef LW_SUBBLOCK_SKIP
+#define LW_SUBBLOCK_SKIP 0
+#endif
+
 struct __align__(16) DevQuad {
     float4 n_nn;      // n = eu x ev, w = n . n
     float4 p0_flags;  // p0, w = flags (bit cast)
@@ -181,19 +185,79 @@ LW_DI bool dda_advance(Dda &s, V3 o, V3 inv, int s0, int s1, int s2, int gs0, in
     return true;
 }
 
-// trace (trace.rs:137-290). The DDA is the reference's step for step; what differs is where the
-// words come from and how the lanes of a warp are kept together:
-//  * the brick's top and overlay entries and its occupancy mask are loaded once when the ray
-//    enters the brick and kept in registers; a voxel in an empty 4^3 sub-block of a brick without
-//    overlay is stepped over without reading its id (its model is 0 and it tests no quad);
-//  * the loop is split in two (a "while-while" traversal): an inner loop steps through empty
-//    bricks and empty voxels until the ray reaches a voxel with a model or overlay quads, then
-//    the quads of that voxel are tested. The lanes of a warp reach the quad tests together
-//    instead of testing quads one lane at a time while the others step.
-// Every visit (brick skip, empty voxel, voxel with quads) counts towards MAX_STEPS as one
-// iteration of the reference's loop does.
-LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, float tmax, uint32_t &steps) {
-    steps = 0;
+// Number of boundaries the DDA crosses along one axis from cell `c` before the crossing at `t_exit`
+// on the exit axis, at most `max_k`: crossing times (k - o) * inv (next_boundary) below t_exit, or
+// equal to it when this axis comes first in the DDA's tie rule (the higher axis index).
+LW_DI int crossings_before(int c, int max_k, float o, float inv, int st, float t_exit, bool first_on_tie) {
+    int k = 0;
+    for (int j = 0; j < max_k; j++) {
+        float tb = next_boundary(o, inv, c + j * st, st);
+        if (tb < t_exit || (tb == t_exit && first_on_tie)) k++;
+        else break;
+    }
+    return k;
+}
+
+// The DDA leaving an empty 4^3 sub-block (no voxel with a model, no overlay in the brick), in one
+// go. Stepping it voxel by voxel (trace.rs:267-287) takes the crossings of all three axes in the
+// order of their distances, ties to the higher axis; none of the voxels tests a quad. So the ray
+// leaves the sub-block through the face whose crossing comes first in that order, at exactly the
+// distance next_boundary gives for the last cell before that face, and on each other axis it has
+// crossed the boundaries that come before it in the same order. The resulting cell, distance and
+// next boundaries are the ones the voxel-by-voxel DDA reaches, bit for bit; the visits skipped are
+// counted towards MAX_STEPS. Returns -1 when the reference's loop would end inside (the range ends,
+// the grid is left, or the step budget runs out), 0 otherwise.
+LW_DI int skip_empty_sub_block(Dda &s, V3 o, V3 inv, int s0, int s1, int s2, int gs0, int gs1, int gs2, float t_end,
+                               uint32_t &it) {
+    const int b0 = s.c0 & ~3, b1 = s.c1 & ~3, b2 = s.c2 & ~3;
+    const int l0 = s0 > 0 ? b0 + 3 : b0, l1 = s1 > 0 ? b1 + 3 : b1, l2 = s2 > 0 ? b2 + 3 : b2;
+    float f0 = next_boundary(o.x, inv.x, l0, s0);
+    float f1 = next_boundary(o.y, inv.y, l1, s1);
+    float f2 = next_boundary(o.z, inv.z, l2, s2);
+    int axis = f0 < f1 ? (f0 < f2 ? 0 : 2) : (f1 < f2 ? 1 : 2);
+    float t_exit = axis == 0 ? f0 : (axis == 1 ? f1 : f2);
+    if (t_exit > t_end) return -1;
+    // Interior crossings: every one on the exit axis, and those before t_exit on the others.
+    int m0 = s0 == 0 ? 0 : (s0 > 0 ? l0 - s.c0 : s.c0 - l0);
+    int m1 = s1 == 0 ? 0 : (s1 > 0 ? l1 - s.c1 : s.c1 - l1);
+    int m2 = s2 == 0 ? 0 : (s2 > 0 ? l2 - s.c2 : s.c2 - l2);
+    int k0 = axis == 0 ? m0 : crossings_before(s.c0, m0, o.x, inv.x, s0, t_exit, 0 > axis);
+    int k1 = axis == 1 ? m1 : crossings_before(s.c1, m1, o.y, inv.y, s1, t_exit, 1 > axis);
+    int k2 = axis == 2 ? m2 : crossings_before(s.c2, m2, o.z, inv.z, s2, t_exit, 2 > axis);
+    uint32_t visits = (uint32_t)(k0 + k1 + k2);
+    if (it + visits > MAX_STEPS) return -1;
+    it += visits;
+    int n0c = s.c0 + k0 * s0, n1c = s.c1 + k1 * s1, n2c = s.c2 + k2 * s2;
+    // The exit crossing itself.
+    if (axis == 0) n0c += s0;
+    else if (axis == 1) n1c += s1;
+    else n2c += s2;
+    int ca = axis == 0 ? n0c : (axis == 1 ? n1c : n2c);
+    int ga = axis == 0 ? gs0 : (axis == 1 ? gs1 : gs2);
+    if (ca < 0 || ca >= ga) return -1;
+    s.c0 = n0c;
+    s.c1 = n1c;
+    s.c2 = n2c;
+    s.n0 = next_boundary(o.x, inv.x, n0c, s0);
+    s.n1 = next_boundary(o.y, inv.y, n1c, s1);
+    s.n2 = next_boundary(o.z, inv.z, n2c, s2);
+    s.t = t_exit;
+    return 0;
+}
+
+// The state of a traversal between two calls of trace_run: the DDA, the inverse direction, the
+// end of the range and the visit count. Everything else (the signs of the direction, the brick
+// cached in registers) is derived again when the traversal resumes.
+struct TraceState {
+    Dda s;
+    V3 inv;
+    float t_end;
+    uint32_t it;
+};
+
+// The set-up of trace (trace.rs:137-174): the slab test against the grid and the first cell.
+// False when the range misses the grid (trace returns None at once).
+LW_DI bool trace_begin(TraceState &ts, const DevParams &P, V3 o, V3 d, float tmax) {
     const uint32_t dx = P.grid_dims.x, dy = P.grid_dims.y, dz = P.grid_dims.z;
     V3 size = v3((float)(dx * 16u), (float)(dy * 16u), (float)(dz * 16u));
     V3 inv = v3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
@@ -202,32 +266,58 @@ LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, f
     float t_enter = fmax_r(fmax_r(fmin_r(ta.x, tb.x), fmin_r(ta.y, tb.y)), fmin_r(ta.z, tb.z));
     float t_exit = fmin_r(fmin_r(fmax_r(ta.x, tb.x), fmax_r(ta.y, tb.y)), fmax_r(ta.z, tb.z));
     float t0 = fmax_r(t_enter, 0.0f);
-    const float t_end = fmin_r(t_exit, tmax);
-    if (t0 > t_end) return no_hit();
-
+    float t_end = fmin_r(t_exit, tmax);
+    if (t0 > t_end) return false;
     V3 start = o + d * (t0 + 1e-4f);
+    const int s0 = sgn(d.x), s1 = sgn(d.y), s2 = sgn(d.z);
+    ts.s.c0 = clamp_i(to_i32(floorf(start.x)), 0, (int)dx * 16 - 1);
+    ts.s.c1 = clamp_i(to_i32(floorf(start.y)), 0, (int)dy * 16 - 1);
+    ts.s.c2 = clamp_i(to_i32(floorf(start.z)), 0, (int)dz * 16 - 1);
+    ts.s.n0 = next_boundary(o.x, inv.x, ts.s.c0, s0);
+    ts.s.n1 = next_boundary(o.y, inv.y, ts.s.c1, s1);
+    ts.s.n2 = next_boundary(o.z, inv.z, ts.s.c2, s2);
+    ts.s.t = t0;
+    ts.inv = inv;
+    ts.t_end = t_end;
+    ts.it = 0;
+    return true;
+}
+
+// The traversal loop of trace (trace.rs:176-289), run for at most `budget` voxel visits (0: no
+// limit). Returns 1 with the hit, -1 when the ray leaves without one, 0 when the budget ran out
+// first; trace_run then continues from `ts` exactly where it stopped.
+//
+// The DDA is the reference's step for step; what differs is where the words come from and how
+// the lanes of a warp are kept together:
+//  * the brick's top and overlay entries and its occupancy mask are loaded once when the ray
+//    enters the brick and kept in registers; a voxel in an empty 4^3 sub-block of a brick without
+//    overlay is not read (its model is 0, it tests no quad) and the rest of that sub-block is
+//    crossed in one step (skip_empty_sub_block);
+//  * the loop is split in two (a "while-while" traversal): an inner loop steps through empty
+//    bricks and empty voxels until the ray reaches a voxel with a model or overlay quads, then
+//    the quads of that voxel are tested, so the lanes of a warp reach the quad tests together.
+// Every visit (brick skip, empty voxel, voxel with quads) counts towards MAX_STEPS as one
+// iteration of the reference's loop does.
+LW_DI int trace_run(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, float tmin, uint32_t budget,
+                    Hit &out) {
+    const uint32_t dx = P.grid_dims.x, dy = P.grid_dims.y, dz = P.grid_dims.z;
     const int gs0 = (int)dx * 16, gs1 = (int)dy * 16, gs2 = (int)dz * 16;
     const int s0 = sgn(d.x), s1 = sgn(d.y), s2 = sgn(d.z);
-    Dda s;
-    s.c0 = clamp_i(to_i32(floorf(start.x)), 0, gs0 - 1);
-    s.c1 = clamp_i(to_i32(floorf(start.y)), 0, gs1 - 1);
-    s.c2 = clamp_i(to_i32(floorf(start.z)), 0, gs2 - 1);
-    s.n0 = next_boundary(o.x, inv.x, s.c0, s0);
-    s.n1 = next_boundary(o.y, inv.y, s.c1, s1);
-    s.n2 = next_boundary(o.z, inv.z, s.c2, s2);
-    s.t = t0;
+    const V3 inv = ts.inv;
+    const float t_end = ts.t_end;
     const float best_t = t_end + 1e-3f;
-
+    Dda &s = ts.s;
     uint32_t cur_b = 0xFFFFFFFFu, entry = EMPTY, ov = EMPTY;
     uint2 occ = make_uint2(0u, 0u);
-    uint32_t it = 0;
+    uint32_t n = 0;
     for (;;) {
         // Inner loop: empty space, up to the next voxel with a model or overlay quads.
         uint32_t model = 0;
         for (;;) {
-            if (it >= MAX_STEPS) return no_hit();
-            it++;
-            steps = it;
+            if (ts.it >= MAX_STEPS) return -1;
+            if (budget != 0u && n >= budget) return 0;
+            n++;
+            ts.it++;
             uint32_t bx = (uint32_t)(s.c0 >> 4), by = (uint32_t)(s.c1 >> 4), bz = (uint32_t)(s.c2 >> 4);
             uint32_t b = (by * dz + bz) * dx + bx;
             if (b != cur_b) {
@@ -254,14 +344,14 @@ LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, f
                     float tt = ((float)(s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
                     if (tt < t_out) { t_out = tt; axis = 2; }
                 }
-                if (t_out > t_end) return no_hit();
+                if (t_out > t_end) return -1;
                 V3 pos = o + d * t_out;
                 s.c0 = axis == 0 ? (s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
                 s.c1 = axis == 1 ? (s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
                 s.c2 = axis == 2 ? (s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
                 int ca = axis == 0 ? s.c0 : (axis == 1 ? s.c1 : s.c2);
                 int ga = axis == 0 ? gs0 : (axis == 1 ? gs1 : gs2);
-                if (ca < 0 || ca >= ga) return no_hit();
+                if (ca < 0 || ca >= ga) return -1;
                 s.n0 = next_boundary(o.x, inv.x, s.c0, s0);
                 s.n1 = next_boundary(o.y, inv.y, s.c1, s1);
                 s.n2 = next_boundary(o.z, inv.z, s.c2, s2);
@@ -277,10 +367,18 @@ LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, f
                 int lx = s.c0 & 15, ly = s.c1 & 15, lz = s.c2 & 15;
                 uint32_t sb = (uint32_t)(((ly >> 2) * 4 + (lz >> 2)) * 4 + (lx >> 2));
                 uint32_t word = sb < 32u ? occ.x : occ.y;
-                model = (word >> (sb & 31u)) & 1u ? brick_voxel(S, entry, lx, ly, lz) : 0u;
+                if ((word >> (sb & 31u)) & 1u) {
+                    model = brick_voxel(S, entry, lx, ly, lz);
+                } else if (LW_SUBBLOCK_SKIP && ov == EMPTY) {
+                    // An empty 4^3 sub-block: go to where the DDA would leave it.
+                    if (skip_empty_sub_block(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end, ts.it) < 0) return -1;
+                    continue;
+                } else {
+                    model = 0;
+                }
             }
             if (model != 0u || ov != EMPTY) break;
-            if (!dda_advance(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end)) return no_hit();
+            if (!dda_advance(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end)) return -1;
         }
 
         // The voxel's quads (trace.rs:228-264).
@@ -304,14 +402,21 @@ LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, f
                 test_quad(S, P, qi, o, d, t_lo, cand);
             }
         }
-        if (cand.quad != NO_QUAD) return cand;
-        if (!dda_advance(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end)) return no_hit();
+        if (cand.quad != NO_QUAD) {
+            out = cand;
+            return 1;
+        }
+        if (!dda_advance(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end)) return -1;
     }
 }
 
+// trace (trace.rs:137-290): the closest hit along o + t d, t in (tmin, tmax), in one go.
 LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, float tmax) {
-    uint32_t steps;
-    return trace(S, P, o, d, tmin, tmax, steps);
+    TraceState ts;
+    if (!trace_begin(ts, P, o, d, tmax)) return no_hit();
+    Hit h;
+    if (trace_run(S, P, ts, o, d, tmin, 0u, h) == 1) return h;
+    return no_hit();
 }
 
 // is_see_through / see_through_hit (trace.rs:113-131).

@@ -18,6 +18,7 @@ struct WorkDesc {
     uint32_t sub;                // samples per item
     uint32_t n_sub;              // items per pixel: ceil(spp / sub)
     uint32_t n_items;            // n_slots * n_sub
+    uint32_t budget;             // voxel visits per ray per loop iteration (0: no limit)
     uint32_t *counter;           // work counter (zeroed before the launch)
     float4 *partials;            // [n_sub][n_slots] compensated item sums (accumulating mode)
     float *samples_out;          // per-sample radiance (sample mode), [(py*w+px)*spp + k][3]
@@ -32,6 +33,29 @@ struct __align__(16) Accum {
 
 enum { MODE_ACCUM = 0, MODE_SAMPLES = 1 };
 
+// One camera of the batched form: its frame, its sky, where its items, sums and image live.
+struct __align__(16) DevJob {
+    DevParams P;
+    const float *sky;
+    Accum *acc;
+    float *out;             // its image, w * h * 3 floats
+    uint64_t partial_off;   // first item sum of the camera in the batch's partial sums
+    uint32_t item_begin;    // first item of the camera in the batch's queue
+    uint32_t slot_begin;    // first pixel slot of the camera among all cameras' slots
+    uint32_t w, h, tiles_x, n_slots, sample_start, spp, sub, n_sub;
+};
+
+struct BatchDesc {
+    const DevJob *jobs;
+    const uint32_t *item_begin;  // the jobs' item_begin, ascending (for the binary search)
+    const uint32_t *slot_begin;  // the jobs' slot_begin, ascending
+    uint32_t n_jobs, n_items, n_slots;
+    uint32_t budget;  // regrouping period (0: whole traversals)
+    uint32_t *counter;
+    float4 *partials;
+    const volatile uint32_t *cancel;
+};
+
 struct LaunchShape {
     int blocks, threads;
 };
@@ -39,7 +63,7 @@ struct LaunchShape {
 // render.cu
 cudaError_t launch_render(int mode, const DevScene &S, const DevParams &P, const WorkDesc &W, LaunchShape shape,
                           cudaStream_t st);
-LaunchShape render_shape(int mode, int device);
+LaunchShape render_shape(int mode, int device, int threads);
 cudaError_t launch_reduce(const WorkDesc &W, Accum *acc, uint32_t frame_w, cudaStream_t st);
 cudaError_t launch_finalize(const Accum *acc, uint32_t n, float *out_rgb, cudaStream_t st);
 cudaError_t launch_trace_rays(const DevScene &S, const DevParams &P, uint32_t n, const float *o, const float *d,
@@ -51,6 +75,11 @@ cudaError_t launch_voxel_lookup(const DevScene &S, const DevParams &P, uint32_t 
 cudaError_t launch_sky_cache(const DevParams &P, uint32_t n, float *out, cudaStream_t st);
 cudaError_t launch_blend_chunky(const DevScene &S, const DevParams &P, float *map, uint32_t w, uint32_t h, float weight,
                                 cudaStream_t st);
+
+// batch.cu
+LaunchShape batch_shape(int device, int threads, bool resume);
+cudaError_t launch_render_batch(const DevScene &S, const BatchDesc &B, LaunchShape shape, cudaStream_t st);
+cudaError_t launch_reduce_batch(const BatchDesc &B, cudaStream_t st);
 
 // refport.cu
 cudaError_t launch_refport(const void *grid, const void *models, const void *ref_quads, const void *atlas,

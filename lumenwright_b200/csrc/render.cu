@@ -1,389 +1,42 @@
 // The path-tracing kernels: the persistent render kernel with its per-lane path state machine
 // (replacing `pt_render`, crates/lumenwright-ptx/src/lib.rs:37-87), the per-pixel reduction of
 // its partial sums, and the parity kernels (trace, voxel lookup).
-#include "device_integrator.cuh"
+#include "device_path.cuh"
 #include "internal.h"
 
 namespace lw {
 
-// Next step of a lane's state machine after a trace or between two of them.
-enum Act : uint32_t {
-    A_TRACE,            // the lane's next ray is set: trace it
-    A_END,              // the path is over: `radiance` is the sample's value
-    A_CONTINUE,         // trace the next path ray, unless the path has had MAX_EVENTS events
-    A_SUN_DONE,         // add the sun's light (transmittance in `tr`)
-    A_EMIT_START,       // sample the emitters of the surface's cell
-    A_BEGIN_EMITTER,    // sample emitter `k` of the cell (or the one picked)
-    A_START_FACE,       // sample face `f` of the current emitter
-    A_FACE_DONE,        // a face gave `val`
-    A_EMITTER_DONE,     // an emitter gave `val`
-    A_EMIT_FINISH,      // the emitters gave `val`: add it
-    A_FINISH_SURFACE,   // Russian roulette and the next direction
-};
-
-// The camera ray of sample `sample` at pixel (px, py) (integrator.rs:545-569).
-LW_DI void begin_sample(Path &p, const DevParams &P, uint32_t px, uint32_t py, uint32_t sample) {
-    uint32_t width = P.frame.x, height = P.frame.y;
-    p.rng = rng_new(py * width + px, sample, P.misc_u.x);
-    float tan_half = P.cam_pos.w, aspect = P.cam_fwd.w;
-    float jx = rng_next(p.rng);
-    float jy = rng_next(p.rng);
-    float sx = (__fdiv_rn(2.0f * ((float)px + jx), (float)width) - 1.0f) * aspect * tan_half;
-    float sy = (1.0f - __fdiv_rn(2.0f * ((float)py + jy), (float)height)) * tan_half;
-    p.d = normalize(f4v(P.cam_fwd) + f4v(P.cam_right) * sx + f4v(P.cam_up) * sy);
-    p.o = f4v(P.cam_pos);
-    p.radiance = v3(0.0f, 0.0f, 0.0f);
-    p.beta = v3(1.0f, 1.0f, 1.0f);
-    p.bounces = 0;
-    p.events = 0;
-    p.specular = true;
-    p.in_water = false;
-    p.tmin = 0.0f;
-    p.tmax = kINF;
-    p.kind = K_EXTEND;
-}
-
-LW_DI uint32_t strategy_of(const DevParams &P) { return P.misc_u.w > 0u ? P.emitter.x : EMITTER_SAMPLING_NONE; }
-
-// The result of a path ray (the body of render_sample's event loop, integrator.rs:571-706).
-LW_DI Act on_extend(Path &p, const DevScene &S, const DevParams &P, Hit h) {
-    const float eps = P.misc_f.y;
-    p.events++;
-    bool found = h.quad != NO_QUAD;
-    bool forced = false;
-    if (p.bounces == 0 && P.see_through.y > 0u && found && !is_see_through(P, h.quad)) {
-        Hit st = see_through_hit(S, P, p.o, p.d, h.t);
-        if (st.quad != NO_QUAD) {
-            uint32_t sflags = __float_as_uint(ldg(&S.quads[st.quad].p0_flags).w);
-            if ((sflags & FLAG_ALPHA_MASK) == ALPHA_TRANSLUCENT) {
-                if (rng_next(p.rng) < __fdiv_rn((float)(st.texel >> 24), 255.0f)) {
-                    h = st;
-                    forced = true;
-                }
-            } else {
-                h = st;
-            }
-        }
-    }
-    const V3 sigma = f4v(P.water_color);
-    float tp;
-    if (water_plane(P, p.o, p.d, tp) && (!found || tp < h.t)) {
-        if (p.in_water) p.beta = vmul(p.beta, transmittance(sigma, tp));
-        bool front = p.d.y < 0.0f;
-        V3 n = v3(0.0f, front ? 1.0f : -1.0f, 0.0f);
-        V3 nd, no;
-        p.in_water = water_interface(P, p.o + p.d * tp, p.d, n, front, p.in_water, eps, p.rng, nd, no);
-        p.d = nd;
-        p.o = no;
-        p.specular = true;
-        p.tmin = 0.0f;
-        return A_CONTINUE;
-    }
-    if (!found) {
-        if (!p.in_water && !under_water_plane(P, p.o, p.d)) {
-            if (p.bounces == 0) p.radiance = p.radiance + vmul(p.beta, sky_lens(S, P, p.d));
-            else p.radiance = p.radiance + vmul(p.beta, sky_light(S, P, p.d));
-            if (p.specular && p.bounces == 0) p.radiance = p.radiance + vmul(p.beta, sun_texture(S, P, p.d));
-        }
-        return A_END;
-    }
-    if (p.in_water) p.beta = vmul(p.beta, transmittance(sigma, h.t));
-    const DevQuad *q = S.quads + h.quad;
-    float4 qn = ldg(&q->n_nn);
-    uint32_t flags = __float_as_uint(ldg(&q->p0_flags).w);
-    uint32_t tint = __float_as_uint(ldg(&q->eu_tint).w);
-    float qemit = ldg(&q->ev_em).w;
-    V3 pos = p.o + p.d * h.t;
-    float alpha = __fdiv_rn((float)(h.texel >> 24), 255.0f);
-    V3 albedo = vmul(linear_rgb(S.gamma, h.texel), linear_rgb(S.gamma, tint));
-    // shading_normal (integrator.rs:308-315): normal() = ev x eu = -(eu x ev), exactly.
-    V3 n = normalize(-f4v(qn));
-    bool front = true;
-    if (!(dot(n, p.d) < 0.0f)) {
-        n = -n;
-        front = false;
-    }
-    if (flags & FLAG_WATER) {
-        V3 nd, no;
-        p.in_water = water_interface(P, pos, p.d, n, front, p.in_water, eps, p.rng, nd, no);
-        p.d = nd;
-        p.o = no;
-        p.specular = true;
-        p.tmin = 0.0f;
-        return A_CONTINUE;
-    }
-    if (!forced && (flags & FLAG_ALPHA_MASK) == ALPHA_TRANSLUCENT && rng_next(p.rng) >= alpha) {
-        p.beta = vmul(p.beta, lerp(v3(1.0f, 1.0f, 1.0f), albedo, alpha));
-        p.o = pos + p.d * eps;
-        p.tmin = 0.0f;
-        return A_CONTINUE;
-    }
-    if (p.bounces >= P.frame.w) return A_END;
-    const uint32_t strategy = strategy_of(P);
-    float emittance = qemit * P.misc_f.x;
-    bool emits = emittance > 0.0f && (P.emitter.y == 0u || strategy == EMITTER_SAMPLING_NONE || p.bounces == 0u);
-    if (emits) p.radiance = p.radiance + vmul(p.beta, vmul(albedo, albedo)) * emittance;
-    p.bounces += 1;
-
-    p.n = n;
-    p.origin = pos + n * eps;
-    // beta.mul(albedo), the factor of the sun and emitter terms and the path's next beta.
-    p.beta = vmul(p.beta, albedo);
-    if (!emits && strategy != EMITTER_SAMPLING_NONE) {
-        emitter_cell(S, pos, p.list, p.count);  // no draw: evaluated here, used after the sun
-        p.emode = 1u;                           // emitters to sample
-    } else {
-        p.emode = 0u;
-    }
-
-    V3 sun = f4v(P.sun_dir);
-    float sin_r = __fsqrt_rn(fmax_r(1.0f - P.sun_dir.w * P.sun_dir.w, 0.0f));
-    bool lit = P.sun_color.x > 0.0f || P.sun_color.y > 0.0f || P.sun_color.z > 0.0f;
-    if (lit && dot(n, sun) > -sin_r && P.sun_dir.y > -sin_r) {
-        V3 l = sample_sun(P, p.rng);
-        float cos_l = dot(n, l);
-        if (cos_l > 0.0f && l.y >= 0.0f) {
-            // shadow (integrator.rs:319-346): the first segment.
-            p.cos_l = cos_l;
-            p.tr = v3(1.0f, 1.0f, 1.0f);
-            p.seg = 0;
-            p.o = p.origin;
-            p.d = l;
-            p.tmin = eps;
-            p.tmax = kINF;
-            p.kind = K_SHADOW;
-            return A_TRACE;
-        }
-    }
-    return A_EMIT_START;
-}
-
-// A shadow segment's result (integrator.rs:322-345).
-LW_DI Act on_shadow(Path &p, const DevScene &S, const DevParams &P, const Hit &h) {
-    const float eps = P.misc_f.y;
-    if (h.quad == NO_QUAD) return A_SUN_DONE;
-    const DevQuad *q = S.quads + h.quad;
-    uint32_t flags = __float_as_uint(ldg(&q->p0_flags).w);
-    if (flags & FLAG_WATER) {
-        V3 qn = f4v(ldg(&q->n_nn));
-        if (-dot(qn, p.d) > 0.0f) p.tr = vmul(p.tr, transmittance(f4v(P.water_color), h.t));
-    } else if ((flags & FLAG_ALPHA_MASK) == ALPHA_TRANSLUCENT) {
-        float a = __fdiv_rn((float)(h.texel >> 24), 255.0f);
-        uint32_t tint = __float_as_uint(ldg(&q->eu_tint).w);
-        V3 col = vmul(linear_rgb(S.gamma, h.texel), linear_rgb(S.gamma, tint));
-        p.tr = vmul(p.tr, lerp(v3(1.0f, 1.0f, 1.0f), col, a));
-    } else {
-        p.tr = v3(0.0f, 0.0f, 0.0f);
-        return A_SUN_DONE;
-    }
-    p.o = p.o + p.d * (h.t + eps);
-    p.tmax -= h.t + eps;
-    p.seg++;
-    if (p.seg < 8u) return A_TRACE;
-    return A_SUN_DONE;
-}
-
-// An emitter visibility ray's result: the rest of sample_emitter_face (integrator.rs:402-413).
-LW_DI Act on_emit(Path &p, const DevScene &S, const DevParams &P, const Hit &h, V3 &val) {
-    const float eps = P.misc_f.y;
-    val = v3(0.0f, 0.0f, 0.0f);
-    if (h.quad == NO_QUAD) return A_FACE_DONE;
-    if (fabs_r(h.t - p.dist) >= 2.0f * eps) return A_FACE_DONE;
-    const DevQuad *q = S.quads + p.first + p.f;
-    V3 nq = -f4v(ldg(&q->n_nn));
-    float area = vlength(nq);
-    float cos_l = __fdiv_rn(fabs_r(dot(nq, p.d)), area);
-    const DevQuad *hq = S.quads + h.quad;
-    uint32_t tint = __float_as_uint(ldg(&hq->eu_tint).w);
-    V3 c = vmul(linear_rgb(S.gamma, h.texel), linear_rgb(S.gamma, tint));
-    float scaler = p.fmode == E_SINGLE ? 1.0f : __fdiv_rn(1.0f, (float)p.faces);
-    val = c * (__fdiv_rn(cos_l, fmax_r(p.dist * p.dist, 1.0f)) * area * ldg(&q->ev_em).w * P.misc_f.x * scaler);
-    return A_FACE_DONE;
-}
-
-// Runs the state machine from `act` until the lane needs a trace or its path ends.
-LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 val) {
-    const float eps = P.misc_f.y;
-    for (;;) {
-        switch (act) {
-        case A_TRACE:
-        case A_END:
-            return act;
-        case A_CONTINUE:
-            if (p.events >= MAX_EVENTS) return A_END;
-            p.kind = K_EXTEND;
-            p.tmax = kINF;
-            return A_TRACE;
-        case A_SUN_DONE:
-            p.radiance = p.radiance + vmul(vmul(p.beta, f4v(P.sun_color)), p.tr) * p.cos_l;
-            act = A_EMIT_START;
-            break;
-        case A_EMIT_START: {
-            // sample_emitters (integrator.rs:441-469).
-            if (p.emode == 0u) {
-                act = A_FINISH_SURFACE;
-                break;
-            }
-            if (p.count == 0u) {
-                val = v3(0.0f, 0.0f, 0.0f);
-                act = A_EMIT_FINISH;
-                break;
-            }
-            const uint32_t *g = S.emitter_grid;
-            uint32_t start = p.list;
-            p.list = EMITTER_GRID_HEADER + ldg(g + 1) * ldg(g + 2) * ldg(g + 3) * 2u + start;
-            uint32_t strategy = strategy_of(P);
-            if (strategy == EMITTER_SAMPLING_ONE || strategy == EMITTER_SAMPLING_ONE_BLOCK) {
-                p.emode = E_SINGLE;
-                p.k = pick(p.count, rng_next(p.rng));
-                act = A_BEGIN_EMITTER;
-            } else if (strategy == EMITTER_SAMPLING_ALL) {
-                p.emode = E_ALL;
-                p.esum = v3(0.0f, 0.0f, 0.0f);
-                p.k = 0;
-                act = A_BEGIN_EMITTER;
-            } else {
-                val = v3(0.0f, 0.0f, 0.0f);
-                act = A_EMIT_FINISH;
-            }
-            break;
-        }
-        case A_BEGIN_EMITTER: {
-            // sample_emitter (integrator.rs:419-433) for emitter list[k].
-            uint32_t i = ldg(S.emitter_grid + p.list + p.k);
-            float4 e0 = ldg(S.emitters + 2u * i);
-            float4 e1 = ldg(S.emitters + 2u * i + 1u);
-            p.eoff = f4v(e0);
-            p.first = __float_as_uint(e0.w);
-            p.faces = __float_as_uint(e1.x);
-            if (p.faces == 0u) {
-                val = v3(0.0f, 0.0f, 0.0f);
-                act = A_EMITTER_DONE;
-                break;
-            }
-            if (P.emitter.x == EMITTER_SAMPLING_ONE) {
-                p.fmode = E_SINGLE;
-                p.f = pick(p.faces, rng_next(p.rng));
-            } else {
-                p.fmode = E_ALL;
-                p.fsum = v3(0.0f, 0.0f, 0.0f);
-                p.f = 0;
-            }
-            act = A_START_FACE;
-            break;
-        }
-        case A_START_FACE: {
-            // sample_emitter_face (integrator.rs:381-401), up to its visibility trace.
-            const DevQuad *q = S.quads + p.first + p.f;
-            float s = rng_next(p.rng);
-            float t = rng_next(p.rng);
-            V3 at = p.eoff + f4v(ldg(&q->p0_flags)) + f4v(ldg(&q->eu_tint)) * s + f4v(ldg(&q->ev_em)) * t;
-            V3 to = at - p.origin;
-            if (dot(to, p.n) <= 0.0f) {
-                val = v3(0.0f, 0.0f, 0.0f);
-                act = A_FACE_DONE;
-                break;
-            }
-            p.dist = vlength(to);
-            p.o = p.origin;
-            p.d = vdiv(to, p.dist);
-            p.tmin = eps;
-            p.tmax = p.dist + 2.0f * eps;
-            p.kind = K_EMIT;
-            return A_TRACE;
-        }
-        case A_FACE_DONE:
-            if (p.fmode == E_SINGLE) {
-                act = A_EMITTER_DONE;
-            } else {
-                p.fsum = p.fsum + val;
-                p.f++;
-                if (p.f < p.faces) {
-                    act = A_START_FACE;
-                } else {
-                    val = p.fsum;
-                    act = A_EMITTER_DONE;
-                }
-            }
-            break;
-        case A_EMITTER_DONE:
-            if (p.emode == E_SINGLE) {
-                val = val * kPI;
-                act = A_EMIT_FINISH;
-            } else {
-                p.esum = p.esum + val;
-                p.k++;
-                if (p.k < p.count) {
-                    act = A_BEGIN_EMITTER;
-                } else {
-                    val = p.esum * __fdiv_rn(kPI, (float)p.count);
-                    act = A_EMIT_FINISH;
-                }
-            }
-            break;
-        case A_EMIT_FINISH:
-            p.radiance = p.radiance + vmul(p.beta, val);
-            act = A_FINISH_SURFACE;
-            break;
-        case A_FINISH_SURFACE:
-            // integrator.rs:695-705.
-            if (p.bounces >= 3u) {
-                float q_rr = clamp_r(max_elem(p.beta), 0.05f, 0.95f);
-                if (rng_next(p.rng) > q_rr) return A_END;
-                p.beta = vdiv(p.beta, q_rr);
-            }
-            p.d = cosine_hemisphere(p.n, p.rng);
-            p.o = p.origin;
-            p.tmin = 0.0f;
-            p.specular = false;
-            act = A_CONTINUE;
-            break;
-        }
-    }
-}
-
-LW_DI Act shade(Path &p, const DevScene &S, const DevParams &P, const Hit &h) {
-    V3 val = v3(0.0f, 0.0f, 0.0f);
-    Act a;
-    if (p.kind == K_EXTEND) a = on_extend(p, S, P, h);
-    else if (p.kind == K_SHADOW) a = on_shadow(p, S, P, h);
-    else a = on_emit(p, S, P, h, val);
-    return advance(p, S, P, a, val);
-}
-
-LW_DI void kahan_add(float &s, float &c, float x) {
-    float y = x - c;
-    float t = s + y;
-    c = (t - s) - y;
-    s = t;
-}
-
-LW_DI bool finite3(V3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
 
 #ifndef LW_STATS
 #define LW_STATS 0
 #endif
 #if LW_STATS
 // Divergence counters of the instrumented build (not part of the product build):
-// [0] loop iterations per warp, [1] lanes active in them, [2] lanes tracing, [3] lane DDA
-// steps, [4] warp DDA steps (the slowest lane's), [5..7] lanes shading a path/shadow/emitter
-// ray, [8] lanes ending a path, [9] iterations with a lane taking work
+// [0] loop iterations per warp, [1] lanes active in them, [2] lanes tracing, [3] lanes whose ray
+// goes on to the next iteration, [4] warp shading passes, [5..7] lanes shading a path/shadow/emitter
+// ray
 __device__ unsigned long long g_stats[16];
 #endif
-constexpr int kThreads = 128;
 #ifndef LW_MIN_BLOCKS
 #define LW_MIN_BLOCKS 4
 #endif
+constexpr int kThreads = 128;
 
 // The persistent render kernel. Each lane takes an item (sub consecutive samples of one pixel),
-// traces its samples one after another, and takes the next item as soon as it is done; each
-// loop iteration traces one ray per active lane.
-template <int MODE>
-__global__ void __launch_bounds__(kThreads, LW_MIN_BLOCKS) k_render(const DevScene S, const DevParams P, const WorkDesc W) {
+// traces its samples one after another, and takes the next item as soon as it is done. Each loop
+// iteration traces one ray per active lane and shades it. With RESUME, an iteration advances each
+// lane's ray by at most `W.budget` voxel visits instead (the regrouping period): a lane whose ray
+// ends shades it and sets up its next ray, a lane whose ray is still on its way keeps it for the
+// next iteration, so no lane waits longer than one budget for the longest traversal of its warp;
+// the price is the traversal state kept live across iterations (more registers).
+template <int MODE, int THREADS, bool RESUME>
+__global__ void __launch_bounds__(THREADS, THREADS == 128 ? LW_MIN_BLOCKS : (THREADS == 64 ? 2 * LW_MIN_BLOCKS : 2))
+k_render(const DevScene S, const DevParams P, const WorkDesc W) {
     const uint32_t lane = threadIdx.x & 31u;
     const unsigned FULL = 0xFFFFFFFFu;
     Path p;
-    bool active = false, exhausted = false;
+    TraceState ts;  // only kept across iterations when RESUME
+    bool active = false, exhausted = false, tracing = false;
     uint32_t px = 0, py = 0, slot = 0, j = 0, sample = 0, s_end = 0;
     float s0 = 0.f, s1 = 0.f, s2 = 0.f, c0 = 0.f, c1 = 0.f, c2 = 0.f;
     for (;;) {
@@ -418,6 +71,7 @@ __global__ void __launch_bounds__(kThreads, LW_MIN_BLOCKS) k_render(const DevSce
                         s0 = s1 = s2 = c0 = c1 = c2 = 0.0f;
                         begin_sample(p, P, px, py, sample);
                         active = true;
+                        tracing = false;
                     }
                 }
             }
@@ -429,41 +83,51 @@ __global__ void __launch_bounds__(kThreads, LW_MIN_BLOCKS) k_render(const DevSce
             if (lane == 0) {
                 atomicAdd(&g_stats[0], 1ull);
                 atomicAdd(&g_stats[1], (unsigned long long)__popc(act));
-                if (mask) atomicAdd(&g_stats[9], 1ull);
             }
         }
 #endif
         if (!active) continue;
 
+        Hit h = no_hit();
+        int r = -1;
+        if (!RESUME) {
+            // The whole traversal at once: nothing of it lives on past this iteration.
+            h = trace(S, P, p.o, p.d, p.tmin, p.tmax);
+            r = h.quad != NO_QUAD ? 1 : -1;
+        } else {
+        if (!tracing) tracing = trace_begin(ts, P, p.o, p.d, p.tmax);
+        if (tracing) {
+            r = trace_run(S, P, ts, p.o, p.d, p.tmin, W.budget, h);
 #if LW_STATS
-        uint32_t steps = 0;
-        Hit h = trace(S, P, p.o, p.d, p.tmin, p.tmax, steps);
+            {
+                unsigned am = __activemask();
+                unsigned cont = __ballot_sync(am, r == 0);
+                if ((int)lane == __ffs(am) - 1) {
+                    atomicAdd(&g_stats[2], (unsigned long long)__popc(am));
+                    atomicAdd(&g_stats[3], (unsigned long long)__popc(cont));
+                }
+            }
+#endif
+            if (r == 0) continue;  // the ray goes on in the next iteration
+            tracing = false;
+        }
+        }
+        if (r != 1) h = no_hit();
+#if LW_STATS
         {
             unsigned am = __activemask();
-            uint32_t lsum = __reduce_add_sync(am, steps), lmax = __reduce_max_sync(am, steps);
             uint32_t kind = p.kind;
             unsigned k0 = __ballot_sync(am, kind == K_EXTEND), k1 = __ballot_sync(am, kind == K_SHADOW);
             unsigned k2 = __ballot_sync(am, kind == K_EMIT);
             if ((int)lane == __ffs(am) - 1) {
-                atomicAdd(&g_stats[2], (unsigned long long)__popc(am));
-                atomicAdd(&g_stats[3], (unsigned long long)lsum);
-                atomicAdd(&g_stats[4], (unsigned long long)lmax);
+                atomicAdd(&g_stats[4], 1ull);
                 atomicAdd(&g_stats[5], (unsigned long long)__popc(k0));
                 atomicAdd(&g_stats[6], (unsigned long long)__popc(k1));
                 atomicAdd(&g_stats[7], (unsigned long long)__popc(k2));
             }
         }
-#else
-        Hit h = trace(S, P, p.o, p.d, p.tmin, p.tmax);
 #endif
         Act a = shade(p, S, P, h);
-#if LW_STATS
-        {
-            unsigned am = __activemask();
-            unsigned e = __ballot_sync(am, a == A_END);
-            if ((int)lane == __ffs(am) - 1) atomicAdd(&g_stats[8], (unsigned long long)__popc(e));
-        }
-#endif
         if (a == A_END) {
             if (MODE == MODE_SAMPLES) {
                 size_t at = ((size_t)((py - W.y0) * W.w + (px - W.x0)) * W.spp + (sample - W.sample_start)) * 3u;
@@ -551,20 +215,34 @@ extern "C" int lw_debug_counters(unsigned long long *out, int reset) {
 }
 #endif
 
-LaunchShape render_shape(int mode, int device) {
+template <int MODE, bool RESUME>
+static const void *kernel_for_r(int threads) {
+    if (threads == 64) return (const void *)k_render<MODE, 64, RESUME>;
+    if (threads == 256) return (const void *)k_render<MODE, 256, RESUME>;
+    return (const void *)k_render<MODE, 128, RESUME>;
+}
+template <int MODE>
+static const void *kernel_for(int threads, bool resume = false) {
+    return resume ? kernel_for_r<MODE, true>(threads) : kernel_for_r<MODE, false>(threads);
+}
+
+LaunchShape render_shape(int mode, int device, int threads) {
+    if (threads != 64 && threads != 256) threads = 128;
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (mode == MODE_SAMPLES) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render<MODE_SAMPLES>, kThreads, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render<MODE_ACCUM>, kThreads, 0);
+    const void *k = mode == MODE_SAMPLES ? kernel_for<MODE_SAMPLES>(threads) : kernel_for<MODE_ACCUM>(threads);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, threads, 0);
     if (per_sm < 1) per_sm = 1;
-    return LaunchShape{sms * per_sm, kThreads};
+    return LaunchShape{sms * per_sm, threads};
 }
 
 cudaError_t launch_render(int mode, const DevScene &S, const DevParams &P, const WorkDesc &W, LaunchShape shape,
                           cudaStream_t st) {
-    if (mode == MODE_SAMPLES) k_render<MODE_SAMPLES><<<shape.blocks, shape.threads, 0, st>>>(S, P, W);
-    else k_render<MODE_ACCUM><<<shape.blocks, shape.threads, 0, st>>>(S, P, W);
-    return cudaGetLastError();
+    void *args[] = {(void *)&S, (void *)&P, (void *)&W};
+    const bool resume = W.budget != 0u;
+    const void *k = mode == MODE_SAMPLES ? kernel_for<MODE_SAMPLES>(shape.threads, resume)
+                                         : kernel_for<MODE_ACCUM>(shape.threads, resume);
+    return cudaLaunchKernel(k, dim3(shape.blocks), dim3(shape.threads), args, 0, st);
 }
 
 cudaError_t launch_reduce(const WorkDesc &W, Accum *acc, uint32_t frame_w, cudaStream_t st) {

@@ -25,10 +25,11 @@ STATUS = {
 # Every symbol the header declares, for the load check.
 EXPORTS = (
     "lw_ctx_create", "lw_ctx_destroy", "lw_last_error", "lw_stream", "lw_get_stats", "lw_cancel", "lw_mark",
-    "lw_elapsed_ms",
+    "lw_elapsed_ms", "lw_set_tuning", "lw_get_tuning",
     "lw_scene_upload", "lw_render_hq", "lw_sky_upload", "lw_clear_accumulator", "lw_render_device",
     "lw_read_accumulator", "lw_render_samples", "lw_trace_rays", "lw_voxel_lookup", "lw_build_sky_cache",
-    "lw_blend_chunky_sky", "lw_render_hq_reference_port", "lw_render_accumulate_noalloc",
+    "lw_blend_chunky_sky", "lw_render_hq_reference_port", "lw_render_accumulate_noalloc", "lw_batch_prepare",
+    "lw_batch_run", "lw_batch_read", "lw_render_batch",
 )
 
 
@@ -55,6 +56,16 @@ class SceneDesc(C.Structure):
 class Stats(C.Structure):
     _fields_ = [("kernel_ms", C.c_double), ("upload_ms", C.c_double), ("launches", C.c_uint32),
                 ("blocks", C.c_uint32), ("threads", C.c_uint32), ("samples", C.c_uint64)]
+
+
+class Tuning(C.Structure):
+    _fields_ = [("threads", C.c_uint32), ("budget", C.c_uint32), ("sub", C.c_uint32)]
+
+
+class CameraJob(C.Structure):
+    """`lw_camera_job`: one camera of the batched form."""
+    _fields_ = [("params", C.c_uint8 * 432), ("sky", C.c_void_p), ("sky_len", C.c_uint64), ("spp", C.c_uint32),
+                ("sample_start", C.c_uint32), ("out_rgb", C.c_void_p)]
 
 
 class HitRec(C.Structure):
@@ -88,6 +99,8 @@ def load(path: str = LIB_PATH):
     L.lw_cancel.restype = None
     L.lw_scene_upload.argtypes = [P, C.POINTER(SceneDesc)]
     L.lw_mark.argtypes = [P, C.c_uint32]
+    L.lw_set_tuning.argtypes = [P, C.POINTER(Tuning)]
+    L.lw_get_tuning.argtypes = [P, C.POINTER(Tuning)]
     L.lw_elapsed_ms.argtypes = [P, C.c_uint32, C.c_uint32, C.POINTER(C.c_double)]
     L.lw_render_hq.argtypes = [P, P, P, C.c_uint64, C.c_uint32, PROGRESS_FN, P, P]
     L.lw_sky_upload.argtypes = [P, P, C.c_uint64]
@@ -99,6 +112,10 @@ def load(path: str = LIB_PATH):
     L.lw_voxel_lookup.argtypes = [P, C.c_uint32, P, P]
     L.lw_build_sky_cache.argtypes = [P, P, C.c_uint32, P]
     L.lw_render_accumulate_noalloc.argtypes = [P, P, C.c_uint32, C.c_uint32, P]
+    L.lw_batch_prepare.argtypes = [P, P, C.c_uint32]
+    L.lw_batch_run.argtypes = [P]
+    L.lw_batch_read.argtypes = [P]
+    L.lw_render_batch.argtypes = [P, P, C.c_uint32]
     L.lw_render_hq_reference_port.argtypes = [P, P, P, C.c_uint64, C.c_uint32, P]
     L.lw_blend_chunky_sky.argtypes = [P, P, P, C.c_uint64, P, P, C.c_float]
     for name in EXPORTS:
@@ -151,6 +168,15 @@ class Context:
 
     def cancel(self):
         self.L.lw_cancel(self.h)
+
+    def set_tuning(self, threads=128, budget=0, sub=0):
+        """Launch tuning of the render kernel (see `lw_tuning`)."""
+        self._check(self.L.lw_set_tuning(self.h, C.byref(Tuning(threads, budget, sub))))
+
+    def get_tuning(self) -> dict:
+        t = Tuning()
+        self._check(self.L.lw_get_tuning(self.h, C.byref(t)))
+        return {"threads": t.threads, "budget": t.budget, "sub": t.sub}
 
     def mark(self, slot: int):
         """Records a CUDA event on the context's stream."""
@@ -231,6 +257,36 @@ class Context:
         self._keep = [p]
         self._check(self.L.lw_render_accumulate_noalloc(self.h, p.ctypes.data, sample_start, spp,
                                                          C.c_void_p(accum_device_ptr)))
+
+    def batch_prepare(self, jobs):
+        """The batched form: ``jobs`` is a list of (params, sky, spp[, sample_start]); returns the
+        output images (h, w, 3) that lw_batch_read fills."""
+        arr = (CameraJob * len(jobs))()
+        keep, outs = [], []
+        for i, jb in enumerate(jobs):
+            params, sky, spp = jb[0], jb[1], jb[2]
+            start = jb[3] if len(jb) > 3 else 0
+            p = self._params(params)
+            sky = np.ascontiguousarray(sky if sky is not None else np.zeros(0), np.float32)
+            w, h = int(p["frame"][0]), int(p["frame"][1])
+            out = np.zeros((h, w, 3), np.float32)
+            C.memmove(arr[i].params, p.ctypes.data, 432)
+            arr[i].sky = _ptr(sky)
+            arr[i].sky_len = sky.size
+            arr[i].spp = spp
+            arr[i].sample_start = start
+            arr[i].out_rgb = out.ctypes.data
+            keep += [p, sky, out]
+            outs.append(out)
+        self._batch_keep = (arr, keep)
+        self._check(self.L.lw_batch_prepare(self.h, C.cast(arr, C.c_void_p), len(jobs)))
+        return outs
+
+    def batch_run(self):
+        self._check(self.L.lw_batch_run(self.h))
+
+    def batch_read(self):
+        self._check(self.L.lw_batch_read(self.h))
 
     def read_accumulator(self, w, h):
         out = np.zeros((h, w, 3), np.float32)
