@@ -243,6 +243,55 @@ lw_status lw_build_sky_cache(lw_ctx *ctx, const lw_params *params, uint32_t n, f
 lw_status lw_blend_chunky_sky(lw_ctx *ctx, const lw_params *params, const float *cache, uint64_t cache_len,
                               float *maps, const float sizes[4], float weight);
 
+/* ---- the differentiable form ------------------------------------------------------------------
+ * No counterpart in the reference: the forward/backward pair of an image loss's gradient with
+ * respect to parameters theta of an hq frame on the uploaded scene. theta is
+ *   - a linear RGB albedo per texel parameter, replacing gamma_to_linear of the texel's bytes
+ *     (crates/lumenwright-kernel/src/integrator.rs:27-34, :634) for every atlas texel mapped to it,
+ *   - an intensity per emitter group (LW_EMITTER_GROUPS groups, a hash of the emitting block's
+ *     voxel) multiplying the emitter intensity params->misc_f[0],
+ *   - the frame's sun direction (params->sun_dir) and sky buffer, which the caller derives from a
+ *     sun azimuth, altitude and turbidity.
+ * At the decoded albedos, unit group intensities and the frame's own sky the forward image is
+ * lw_render_hq's. The adjoint replays each sample's path (path replay backpropagation) with the
+ * Russian roulette probability detached; visibility changes have no interior derivative and
+ * their boundary terms are not estimated. Sums are FP64. */
+#define LW_EMITTER_GROUPS 32
+typedef struct {
+    const lw_params *params;      /* the frame under theta */
+    const float *sky;             /* its sky buffer under theta (the Chunky cache, or game-sky maps) */
+    uint64_t sky_len;
+    const float *albedo;          /* n_params * 3 linear RGB albedos */
+    uint32_t n_params;
+    const int32_t *texel_param;   /* one per atlas texel: its parameter, or -1 to decode the texel */
+    uint64_t texel_param_len;     /* the atlas's texel count */
+    const float *emitter_scale;   /* LW_EMITTER_GROUPS group intensities */
+} lw_adj_frame;
+
+/* d loss / d theta. */
+typedef struct {
+    double *albedo;        /* n_params * 3 */
+    double *emitter_scale; /* LW_EMITTER_GROUPS */
+    double *sky;           /* sky_len: per sky float (the Chunky cache's entries; zeros for game-sky maps) */
+    double sun_dir[3];     /* per component of params->sun_dir, through the sun's next-event estimates */
+} lw_gradient;
+
+/* The mean radiance per pixel of samples [0, spp) under theta, FP64, frame[0] * frame[1] * 3. */
+lw_status lw_adjoint_forward(lw_ctx *ctx, const lw_adj_frame *frame, uint32_t spp, double *out_rgb);
+/* The gradient of a loss whose derivative with respect to the forward image is `d_rgb`
+ * (frame[0] * frame[1] * 3 doubles), over the same samples; overwrites `out`. */
+lw_status lw_adjoint_backward(lw_ctx *ctx, const lw_adj_frame *frame, uint32_t spp, const double *d_rgb,
+                              lw_gradient *out);
+/* Paired finite differences: every sample under `plus` and under `minus` (same size, same
+ * parameter count), with the roulette's probabilities and decisions of the `nominal` albedos and
+ * the shadow rays along nominal->params->sun_dir; writes per pixel the mean of the paired
+ * differences (plus - minus) and of the pairs' midpoints. */
+lw_status lw_adjoint_fd(lw_ctx *ctx, const lw_adj_frame *plus, const lw_adj_frame *minus, const lw_adj_frame *nominal,
+                        uint32_t spp, double *diff_rgb, double *mean_rgb);
+/* The byte-to-linear table the kernels decode texels with: gamma_to_linear(k / 255) for k in
+ * 0..255 (crates/lumenwright-kernel/src/math.rs:183-216), so a caller can form nominal albedos. */
+lw_status lw_gamma_table(float out[256]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -105,6 +105,10 @@ struct lw_ctx {
     cudaGraphExec_t batch_graph = nullptr;
     uint64_t batch_samples = 0;
     size_t partials_cap_bytes = size_t(4) << 30;
+    // the differentiable form: per frame slot (0 and 1: the frames, 2: the nominal frame)
+    DBuf<float> adj_albedo[3], adj_sky[3], adj_emit[3];
+    DBuf<int32_t> adj_tparam[3];
+    DBuf<double> adj_img, adj_img2, adj_g;
 };
 
 namespace {
@@ -355,6 +359,13 @@ void lw_ctx_destroy(lw_ctx *c) {
     c->batch_acc.free_();
     c->batch_out.free_();
     c->batch_partials.free_();
+    for (int k = 0; k < 3; k++) {
+        c->adj_albedo[k].free_();
+        c->adj_sky[k].free_();
+        c->adj_emit[k].free_();
+        c->adj_tparam[k].free_();
+    }
+    for (auto *b : {&c->adj_img, &c->adj_img2, &c->adj_g}) b->free_();
     for (auto *b : {&c->sky, &c->gamma, &c->out_rgb, &c->samples, &c->rays}) b->free_();
     c->acc.free_();
     c->hits.free_();
@@ -910,6 +921,156 @@ lw_status lw_blend_chunky_sky(lw_ctx *c, const lw_params *params, const float *c
     cbuf.free_();
     mbuf.free_();
     if (e != cudaSuccess) return cuda_fail(c, e, "blending the sky maps");
+    return LW_OK;
+}
+
+lw_status lw_gamma_table(float out[256]) {
+    if (!out) return LW_ERR_INVALID_ARGUMENT;
+    for (int k = 0; k < 256; k++) out[k] = ref_gamma_to_linear((float)k / 255.0f);
+    return LW_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Checks one frame of the differentiable form and copies its theta and sky to slot `k`. A null
+// `n_params_out` demands the frame's parameter count equal *n_params_in.
+lw_status adj_upload(lw_ctx *c, const lw_adj_frame *f, int k, AdjFrame &out, uint32_t *n_params) {
+    if (!f || !f->params || !f->texel_param || !f->emitter_scale || !f->sky || (f->n_params && !f->albedo))
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "adjoint frame %d: null argument", k);
+    lw_status s = check_params(c, f->params, true, f->sky_len);
+    if (s != LW_OK) return s;
+    if (f->params->misc_f[2] >= 1.0f && f->params->sky_map[0] < 1.0f) {
+        double n = std::floor((double)f->params->misc_f[2]);
+        if ((n + 1.0) * (n + 1.0) * 3.0 > (double)f->sky_len) return fail(c, LW_ERR_BUFFER_LENGTH, "sky cache too short");
+    }
+    if (f->texel_param_len != c->atlas_len)
+        return fail(c, LW_ERR_BUFFER_LENGTH, "texel_param has %llu entries, the atlas %llu texels",
+                    (unsigned long long)f->texel_param_len, (unsigned long long)c->atlas_len);
+    if (*n_params != UINT32_MAX && *n_params != f->n_params)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "frames with %u and %u parameters", *n_params, f->n_params);
+    *n_params = f->n_params;
+    for (uint64_t i = 0; i < f->texel_param_len; i++)
+        if (f->texel_param[i] < -1 || f->texel_param[i] >= (int64_t)f->n_params)
+            return fail(c, LW_ERR_BUFFER_LENGTH, "texel_param[%llu] = %d outside [-1, %u)", (unsigned long long)i,
+                        f->texel_param[i], f->n_params);
+    CK(c, upload(c, c->adj_albedo[k], f->albedo, (size_t)f->n_params * 3, 4), "uploading the albedo parameters");
+    CK(c, upload(c, c->adj_tparam[k], f->texel_param, f->texel_param_len, 4), "uploading the texel parameters");
+    CK(c, upload(c, c->adj_emit[k], f->emitter_scale, LW_EMITTER_GROUPS, 4), "uploading the emitter intensities");
+    CK(c, upload(c, c->adj_sky[k], f->sky, f->sky_len, 4), "uploading the sky");
+    out.P = dev_params(f->params);
+    out.sky = c->adj_sky[k].p;
+    out.albedo = c->adj_albedo[k].p;
+    out.texel_param = c->adj_tparam[k].p;
+    out.emit_mult = c->adj_emit[k].p;
+    return LW_OK;
+}
+
+lw_status adj_begin(lw_ctx *c) {
+    if (!c) return LW_ERR_INVALID_ARGUMENT;
+    if (!c->has_scene) return fail(c, LW_ERR_NO_SCENE, "no scene uploaded");
+    cudaSetDevice(c->device);
+    return LW_OK;
+}
+
+lw_status adj_timed(lw_ctx *c, cudaError_t (*launch)(lw_ctx *, void *), void *arg, uint64_t samples) {
+    CK(c, cudaEventRecord(c->ev_a, c->stream), "recording an event");
+    CK(c, launch(c, arg), "launching the adjoint kernel");
+    CK(c, cudaEventRecord(c->ev_b, c->stream), "recording an event");
+    CK(c, cudaEventSynchronize(c->ev_b), "running the adjoint kernel");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, c->ev_a, c->ev_b);
+    c->stats.kernel_ms = ms;
+    c->stats.launches = 1;
+    c->stats.samples = samples;
+    return LW_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+lw_status lw_adjoint_forward(lw_ctx *c, const lw_adj_frame *frame, uint32_t spp, double *out_rgb) {
+    lw_status s = adj_begin(c);
+    if (s != LW_OK) return s;
+    if (!out_rgb || !spp) return fail(c, LW_ERR_INVALID_ARGUMENT, "bad argument");
+    AdjFrame F;
+    uint32_t np = UINT32_MAX;
+    if ((s = adj_upload(c, frame, 0, F, &np)) != LW_OK) return s;
+    size_t n = (size_t)F.P.frame.x * F.P.frame.y * 3;
+    CK(c, ensure(c->adj_img, n), "allocating the image");
+    CK(c, cudaMemsetAsync(c->adj_img.p, 0, n * 8, c->stream), "clearing the image");
+    struct A { DevScene S; AdjFrame F; uint32_t spp; double *img; } a{dev_scene(c), F, spp, c->adj_img.p};
+    s = adj_timed(c, [](lw_ctx *cc, void *p) {
+        A &x = *(A *)p;
+        return launch_adj_forward(x.S, x.F, x.spp, x.img, cc->stream);
+    }, &a, (uint64_t)n / 3 * spp);
+    if (s != LW_OK) return s;
+    CK(c, cudaMemcpy(out_rgb, c->adj_img.p, n * 8, cudaMemcpyDeviceToHost), "reading the image");
+    return LW_OK;
+}
+
+lw_status lw_adjoint_backward(lw_ctx *c, const lw_adj_frame *frame, uint32_t spp, const double *d_rgb, lw_gradient *out) {
+    lw_status s = adj_begin(c);
+    if (s != LW_OK) return s;
+    if (!d_rgb || !out || !spp || !out->emitter_scale || !out->sky || (frame && frame->n_params && !out->albedo))
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "bad argument");
+    AdjFrame F;
+    uint32_t np = UINT32_MAX;
+    if ((s = adj_upload(c, frame, 0, F, &np)) != LW_OK) return s;
+    size_t n = (size_t)F.P.frame.x * F.P.frame.y * 3;
+    size_t ng = (size_t)np * 3 + LW_EMITTER_GROUPS + frame->sky_len + 3;
+    CK(c, ensure(c->adj_img, n), "allocating the image gradient");
+    CK(c, ensure(c->adj_g, ng), "allocating the gradient");
+    CK(c, cudaMemcpyAsync(c->adj_img.p, d_rgb, n * 8, cudaMemcpyHostToDevice, c->stream), "uploading the image gradient");
+    CK(c, cudaMemsetAsync(c->adj_g.p, 0, ng * 8, c->stream), "clearing the gradient");
+    AdjGrad G;
+    G.albedo = c->adj_g.p;
+    G.emit = G.albedo + (size_t)np * 3;
+    G.cache = G.emit + LW_EMITTER_GROUPS;
+    G.sun = G.cache + frame->sky_len;
+    struct A { DevScene S; AdjFrame F; uint32_t spp; const double *d; AdjGrad G; } a{dev_scene(c), F, spp, c->adj_img.p, G};
+    s = adj_timed(c, [](lw_ctx *cc, void *p) {
+        A &x = *(A *)p;
+        return launch_adj_backward(x.S, x.F, x.spp, x.d, x.G, cc->stream);
+    }, &a, (uint64_t)n / 3 * spp * 2);
+    if (s != LW_OK) return s;
+    if (np) CK(c, cudaMemcpy(out->albedo, G.albedo, (size_t)np * 3 * 8, cudaMemcpyDeviceToHost), "reading the gradient");
+    CK(c, cudaMemcpy(out->emitter_scale, G.emit, LW_EMITTER_GROUPS * 8, cudaMemcpyDeviceToHost), "reading the gradient");
+    CK(c, cudaMemcpy(out->sky, G.cache, frame->sky_len * 8, cudaMemcpyDeviceToHost), "reading the gradient");
+    CK(c, cudaMemcpy(out->sun_dir, G.sun, 3 * 8, cudaMemcpyDeviceToHost), "reading the gradient");
+    return LW_OK;
+}
+
+lw_status lw_adjoint_fd(lw_ctx *c, const lw_adj_frame *plus, const lw_adj_frame *minus, const lw_adj_frame *nominal,
+                        uint32_t spp, double *diff_rgb, double *mean_rgb) {
+    lw_status s = adj_begin(c);
+    if (s != LW_OK) return s;
+    if (!diff_rgb || !mean_rgb || !spp) return fail(c, LW_ERR_INVALID_ARGUMENT, "bad argument");
+    AdjFrame Fp, Fm, F0;
+    uint32_t np = UINT32_MAX;
+    if ((s = adj_upload(c, plus, 0, Fp, &np)) != LW_OK) return s;
+    if ((s = adj_upload(c, minus, 1, Fm, &np)) != LW_OK) return s;
+    if ((s = adj_upload(c, nominal, 2, F0, &np)) != LW_OK) return s;
+    for (int k = 0; k < 2; k++)
+        if (Fm.P.frame.x != Fp.P.frame.x || Fm.P.frame.y != Fp.P.frame.y || F0.P.frame.x != Fp.P.frame.x ||
+            F0.P.frame.y != Fp.P.frame.y)
+            return fail(c, LW_ERR_INVALID_ARGUMENT, "the frames differ in size");
+    size_t n = (size_t)Fp.P.frame.x * Fp.P.frame.y * 3;
+    CK(c, ensure(c->adj_img, n), "allocating the differences");
+    CK(c, ensure(c->adj_img2, n), "allocating the means");
+    CK(c, cudaMemsetAsync(c->adj_img.p, 0, n * 8, c->stream), "clearing the differences");
+    CK(c, cudaMemsetAsync(c->adj_img2.p, 0, n * 8, c->stream), "clearing the means");
+    struct A { DevScene S; AdjFrame Fp, Fm; const float *a0; float4 sun0; uint32_t spp; double *d, *m; } a{
+        dev_scene(c), Fp, Fm, F0.albedo, F0.P.sun_dir, spp, c->adj_img.p, c->adj_img2.p};
+    s = adj_timed(c, [](lw_ctx *cc, void *p) {
+        A &x = *(A *)p;
+        return launch_adj_fd(x.S, x.Fp, x.Fm, x.a0, x.sun0, x.spp, x.d, x.m, cc->stream);
+    }, &a, (uint64_t)n / 3 * spp * 2);
+    if (s != LW_OK) return s;
+    CK(c, cudaMemcpy(diff_rgb, c->adj_img.p, n * 8, cudaMemcpyDeviceToHost), "reading the differences");
+    CK(c, cudaMemcpy(mean_rgb, c->adj_img2.p, n * 8, cudaMemcpyDeviceToHost), "reading the means");
     return LW_OK;
 }
 

@@ -81,6 +81,27 @@ LaunchShape batch_shape(int device, int threads, bool resume);
 cudaError_t launch_render_batch(const DevScene &S, const BatchDesc &B, LaunchShape shape, cudaStream_t st);
 cudaError_t launch_reduce_batch(const BatchDesc &B, cudaStream_t st);
 
+// adjoint.cu: the differentiable form.
+#define LW_ADJ_EMITTER_GROUPS 32
+struct AdjFrame {
+    DevParams P;                 // the frame with this theta's sun and sky
+    const float *sky;            // the sky buffer of this theta
+    const float *albedo;         // [params][3] linear albedo per texel parameter
+    const int32_t *texel_param;  // per atlas texel: its parameter, or -1 (the decoded texel)
+    const float *emit_mult;      // [LW_ADJ_EMITTER_GROUPS] emitter group intensities
+};
+struct AdjGrad {
+    double *albedo;  // [params][3]
+    double *emit;    // [LW_ADJ_EMITTER_GROUPS]
+    double *cache;   // one per sky float
+    double *sun;     // [3]: d / d sun_dir.xyz
+};
+cudaError_t launch_adj_forward(const DevScene &S, const AdjFrame &F, uint32_t spp, double *img, cudaStream_t st);
+cudaError_t launch_adj_backward(const DevScene &S, const AdjFrame &F, uint32_t spp, const double *d_img,
+                                const AdjGrad &G, cudaStream_t st);
+cudaError_t launch_adj_fd(const DevScene &S, const AdjFrame &plus, const AdjFrame &minus, const float *albedo0,
+                          float4 sun0, uint32_t spp, double *diff, double *mean, cudaStream_t st);
+
 // refport.cu
 cudaError_t launch_refport(const void *grid, const void *models, const void *ref_quads, const void *atlas,
                            const void *emitters, const void *egrid, const float *sky, const float *gamma,

@@ -29,8 +29,11 @@ EXPORTS = (
     "lw_scene_upload", "lw_render_hq", "lw_sky_upload", "lw_clear_accumulator", "lw_render_device",
     "lw_read_accumulator", "lw_render_samples", "lw_trace_rays", "lw_voxel_lookup", "lw_build_sky_cache",
     "lw_blend_chunky_sky", "lw_render_hq_reference_port", "lw_render_accumulate_noalloc", "lw_batch_prepare",
-    "lw_batch_run", "lw_batch_read", "lw_render_batch",
+    "lw_batch_run", "lw_batch_read", "lw_render_batch", "lw_adjoint_forward", "lw_adjoint_backward", "lw_adjoint_fd",
+    "lw_gamma_table",
 )
+
+EMITTER_GROUPS = 32  # LW_EMITTER_GROUPS
 
 
 class LwError(RuntimeError):
@@ -66,6 +69,19 @@ class CameraJob(C.Structure):
     """`lw_camera_job`: one camera of the batched form."""
     _fields_ = [("params", C.c_uint8 * 432), ("sky", C.c_void_p), ("sky_len", C.c_uint64), ("spp", C.c_uint32),
                 ("sample_start", C.c_uint32), ("out_rgb", C.c_void_p)]
+
+
+class AdjFrame(C.Structure):
+    """`lw_adj_frame`: a frame of the differentiable form and its parameters theta."""
+    _fields_ = [("params", C.c_void_p), ("sky", C.c_void_p), ("sky_len", C.c_uint64), ("albedo", C.c_void_p),
+                ("n_params", C.c_uint32), ("texel_param", C.c_void_p), ("texel_param_len", C.c_uint64),
+                ("emitter_scale", C.c_void_p)]
+
+
+class Gradient(C.Structure):
+    """`lw_gradient`."""
+    _fields_ = [("albedo", C.c_void_p), ("emitter_scale", C.c_void_p), ("sky", C.c_void_p),
+                ("sun_dir", C.c_double * 3)]
 
 
 class HitRec(C.Structure):
@@ -118,6 +134,10 @@ def load(path: str = LIB_PATH):
     L.lw_render_batch.argtypes = [P, P, C.c_uint32]
     L.lw_render_hq_reference_port.argtypes = [P, P, P, C.c_uint64, C.c_uint32, P]
     L.lw_blend_chunky_sky.argtypes = [P, P, P, C.c_uint64, P, P, C.c_float]
+    L.lw_adjoint_forward.argtypes = [P, C.POINTER(AdjFrame), C.c_uint32, P]
+    L.lw_adjoint_backward.argtypes = [P, C.POINTER(AdjFrame), C.c_uint32, P, C.POINTER(Gradient)]
+    L.lw_adjoint_fd.argtypes = [P, C.POINTER(AdjFrame), C.POINTER(AdjFrame), C.POINTER(AdjFrame), C.c_uint32, P, P]
+    L.lw_gamma_table.argtypes = [P]
     for name in EXPORTS:
         if name not in ("lw_ctx_destroy", "lw_last_error", "lw_stream", "lw_cancel"):
             getattr(L, name).restype = C.c_int
@@ -127,6 +147,15 @@ def load(path: str = LIB_PATH):
 
 def _ptr(a):
     return a.ctypes.data if a is not None and a.size else None
+
+
+def gamma_table() -> np.ndarray:
+    """The byte-to-linear table the kernels decode texels with (256 floats)."""
+    out = np.zeros(256, np.float32)
+    st = load().lw_gamma_table(out.ctypes.data)
+    if st:
+        raise LwError(st, "lw_gamma_table")
+    return out
 
 
 class Context:
@@ -327,6 +356,54 @@ class Context:
         self._check(self.L.lw_blend_chunky_sky(self.h, p.ctypes.data, cache.ctypes.data, cache.size, out.ctypes.data,
                                                sz.ctypes.data, float(weight)))
         return out
+
+    # ---- the differentiable form --------------------------------------------------------------
+    def _adj_frame(self, params, sky, albedo, texel_param, emitter_scale):
+        """An `lw_adj_frame` and the arrays it points to (kept alive by the caller)."""
+        p = self._params(params)
+        sky = np.ascontiguousarray(sky, np.float32)
+        albedo = np.ascontiguousarray(albedo, np.float32).reshape(-1, 3)
+        tp = np.ascontiguousarray(texel_param, np.int32)
+        es = np.ascontiguousarray(emitter_scale, np.float32)
+        if es.size != EMITTER_GROUPS:
+            raise ValueError(f"{EMITTER_GROUPS} emitter group intensities expected, {es.size} given")
+        f = AdjFrame(p.ctypes.data, _ptr(sky), sky.size, _ptr(albedo), albedo.shape[0], _ptr(tp), tp.size,
+                     es.ctypes.data)
+        return f, (p, sky, albedo, tp, es)
+
+    def adjoint_forward(self, params, sky, albedo, texel_param, emitter_scale, spp):
+        """The mean radiance under theta, FP64, shape (h, w, 3)."""
+        f, keep = self._adj_frame(params, sky, albedo, texel_param, emitter_scale)
+        w, h = int(keep[0]["frame"][0]), int(keep[0]["frame"][1])
+        out = np.zeros((h, w, 3), np.float64)
+        self._check(self.L.lw_adjoint_forward(self.h, C.byref(f), spp, out.ctypes.data))
+        return out
+
+    def adjoint_backward(self, params, sky, albedo, texel_param, emitter_scale, spp, d_rgb):
+        """d loss / d theta for d loss / d image = ``d_rgb``: a dict with ``albedo`` (n, 3),
+        ``emitter_scale`` (32), ``sky`` (per sky float) and ``sun_dir`` (3)."""
+        f, keep = self._adj_frame(params, sky, albedo, texel_param, emitter_scale)
+        d = np.ascontiguousarray(d_rgb, np.float64)
+        ga = np.zeros((keep[2].shape[0], 3), np.float64)
+        ge = np.zeros(EMITTER_GROUPS, np.float64)
+        gs = np.zeros(keep[1].size, np.float64)
+        g = Gradient(_ptr(ga), ge.ctypes.data, _ptr(gs))
+        self._check(self.L.lw_adjoint_backward(self.h, C.byref(f), spp, d.ctypes.data, C.byref(g)))
+        return {"albedo": ga, "emitter_scale": ge, "sky": gs, "sun_dir": np.array(list(g.sun_dir))}
+
+    def adjoint_fd(self, plus, minus, nominal, spp):
+        """Paired finite differences; ``plus``, ``minus``, ``nominal`` are (params, sky, albedo,
+        texel_param, emitter_scale). Returns (mean of plus - minus, mean of the midpoints), each
+        shape (h, w, 3), FP64."""
+        fp, kp = self._adj_frame(*plus)
+        fm, km = self._adj_frame(*minus)
+        f0, k0 = self._adj_frame(*nominal)
+        w, h = int(kp[0]["frame"][0]), int(kp[0]["frame"][1])
+        diff = np.zeros((h, w, 3), np.float64)
+        mean = np.zeros((h, w, 3), np.float64)
+        self._check(self.L.lw_adjoint_fd(self.h, C.byref(fp), C.byref(fm), C.byref(f0), spp, diff.ctypes.data,
+                                         mean.ctypes.data))
+        return diff, mean
 
     def voxel_lookup(self, xyz):
         xyz = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)

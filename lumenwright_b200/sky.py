@@ -113,9 +113,13 @@ class Preetham:
         zenith_lum = abs((4.0453 * T - 4.9710) * math.tan(chi) - 0.2155 * T + 2.4192)
         zx, zy = chroma(sun_theta, self.X_ZENITH), chroma(sun_theta, self.Y_ZENITH)
         f0 = lambda c: 1.0 / perez_f(1.0, sun_theta, cos2_theta, c)  # noqa: E731
+        # f64 values (the adjoint's sky Jacobian) and the f32 Params fields cast from them.
+        self.sun64 = sun
+        self.zenith64 = np.array([zx * f0(cx), zy * f0(cy), zenith_lum * f0(cl)])
+        self.perez64 = np.array([[cx[i], cy[i], cl[i]] for i in range(5)])
         self.sun = sun.astype(F32)
-        self.zenith = np.array([zx * f0(cx), zy * f0(cy), zenith_lum * f0(cl)], F32)
-        self.perez = np.array([[cx[i], cy[i], cl[i]] for i in range(5)], F32)
+        self.zenith = self.zenith64.astype(F32)
+        self.perez = self.perez64.astype(F32)
         self.turbidity = T
 
 
