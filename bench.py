@@ -259,6 +259,54 @@ def run_batched(args):
     ctx.close()
 
 
+def run_adjoint(args):
+    """The differentiable form: one gradient of the L2 image loss on the differentiation workload
+    (8x8-chunk world with emitters, 512x288, 64 spp, 4 bounces, Chunky sky) per step: the FP64
+    forward image then the two-replay backward. `value` counts the forward's samples per second of
+    forward + backward kernel time; `e2e` times `DiffProblem.gradient` (host set-up, copies and the
+    sky Jacobian included)."""
+    from lumenwright_b200 import adjoint as A
+    from lumenwright_b200.native import Context
+    ctx = Context(0)
+    prob = A.DiffProblem(ctx)
+    theta = prob.theta0
+    args_ = prob._args(theta)
+    samples = prob.width * prob.height * prob.spp
+    for _ in range(args.warmup):
+        img = ctx.adjoint_forward(*args_, prob.spp)
+        ctx.adjoint_backward(*args_, prob.spp, 2.0 * (img - prob.target))
+    fwd_ms = bwd_ms = 0.0
+    with ClockSampler(0) as clocks:
+        for _ in range(args.steps):
+            img = ctx.adjoint_forward(*args_, prob.spp)
+            fwd_ms += ctx.stats()["kernel_ms"]
+            ctx.adjoint_backward(*args_, prob.spp, 2.0 * (img - prob.target))
+            bwd_ms += ctx.stats()["kernel_ms"]
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        prob.gradient(theta)
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    ms = (fwd_ms + bwd_ms) / args.steps
+    frame_in = args_[2].nbytes + args_[3].nbytes + args_[4].nbytes + args_[1].nbytes
+    print(json.dumps({
+        "metric": "Msamples/s (adjoint: forward + path-replay backward)", "value": samples / ms / 1e3,
+        "unit": "Msamples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 sums)",
+        "data": "synthetic",
+        "config": {"workload": "c4: 8x8-chunk world with emitters, 512x288, 64 spp, 4 bounces, Chunky sky",
+                   "forward_ms": fwd_ms / args.steps, "backward_ms": bwd_ms / args.steps,
+                   "parameters": A.N_THETA},
+        "e2e": {"value": samples / e2e_s / 1e6, "unit": "Msamples/s",
+                # forward and backward each upload theta, the texel map, the sky and the params;
+                # the backward also the image gradient
+                "h2d_bytes_per_step": int(2 * (frame_in + 432) + img.nbytes),
+                # the sky cache built on the device, the image, the gradient
+                "d2h_bytes_per_step": int(args_[1].nbytes + img.nbytes + (A.N_ALBEDO + A.GROUPS + args_[1].size + 3) * 8)},
+        "gpu_launches": 2 * args.steps, "clocks": clocks.summary(),
+    }), flush=True)
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -267,8 +315,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--spp", type=int, default=1024)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="c2", choices=["c2", "c3"],
-                    help="c2: the drop-in frame (default); c3: the batched form, 64 cameras")
+    ap.add_argument("--workload", default="c2", choices=["c2", "c3", "c4"],
+                    help="c2: the drop-in frame (default); c3: the batched form, 64 cameras; "
+                         "c4: the differentiable form, one loss gradient")
     ap.add_argument("--c3-scale", type=float, default=0.25, help="spp scale of the 64 cameras (c3)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -283,6 +332,9 @@ def main():
 
     if args.workload == "c3":
         run_batched(args)
+        return
+    if args.workload == "c4":
+        run_adjoint(args)
         return
 
     dist = None

@@ -116,6 +116,7 @@ class Config:
     seed: int = 1
     eye: tuple = (32.0, 100.0, 32.0)
     target: tuple = (0.0, 64.0, 0.0)
+    origin_x: float = 0.0  # world x of the grid's first column (the world is translated by it)
     notes: dict = field(default_factory=dict)
 
 
@@ -126,6 +127,10 @@ CONFIGS = {
     "c2": Config("c2", 12, 1280, 720, 1024, 8, 12800, "game", emitters=True, water_plane=63.0),
     # Differentiation world.
     "c4": Config("c4", 8, 512, 288, 64, 4, 4000, "chunky"),
+    # Precision: 32x32 chunks translated to x = 1,000,000, the camera at a fractional position
+    # there; the host rebases it to the grid in f64 before the f32 cast.
+    "c5": Config("c5", 32, 3840, 2160, 4096, 8, 4000, "chunky", emitters=True, water_plane=63.0,
+                 eye=(1_000_256.37, 120.61, 256.29), target=(1_000_128.5, 70.0, 128.5), origin_x=1_000_000.0),
 }
 
 
@@ -145,12 +150,14 @@ def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None)
         own = sky_backend = Context(0)
     try:
         world = S.generate_world(cfg.chunks, cfg.seed, emitters=cfg.emitters)
+        world.origin = (cfg.origin_x, world.origin[1], world.origin[2])
         atlas = S.build_atlas(cfg.seed)
         hq = build_hq(world, atlas)
         yaw, pitch = Camera.look_at(cfg.eye, cfg.target)
         cam = Camera(cfg.eye, float(yaw), float(pitch), 70.0)
         origin = world.origin
-        eye = [F32(cfg.eye[i] - origin[i]) for i in range(3)]  # f64 difference, then f32
+        eye64 = tuple(float(cfg.eye[i]) - float(origin[i]) for i in range(3))
+        eye = [F32(e) for e in eye64]  # f64 difference, then f32
         sun_dir = SK.sun_direction_from_angle(SK.celestial_angle(cfg.time))
         weight = F32(1.0) if cfg.look == "chunky" else SK.dusk_day_weight(cfg.time)
         intensity = SK.default_emitter_intensity(False, weight)
@@ -178,4 +185,4 @@ def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None)
             own.close()
     cfg.notes.update(dict(weight=float(weight), emitter_intensity=float(intensity), stats=vars(hq.stats),
                           emitters=world.emitters_placed, solid=world.solid_blocks))
-    return HqFrame(scene=hq, params=p, spp=spp, sky=sky)
+    return HqFrame(scene=hq, params=p, spp=spp, sky=sky, eye64=eye64)

@@ -63,6 +63,9 @@ class HqFrame:
     params: np.ndarray  # PARAMS_DTYPE record
     spp: int
     sky: np.ndarray     # f32: the sky cache, or the lens map then the light map
+    # The eye relative to the grid origin in f64 (the rebasing of request.rs:640-644 before its
+    # cast to f32); FP64 references start their camera rays here.
+    eye64: Optional[Tuple[float, float, float]] = None
 
     def __post_init__(self):
         self.params = np.array(self.params, dtype=PARAMS_DTYPE, order="C").reshape(())
