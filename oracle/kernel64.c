@@ -71,3 +71,68 @@ void lwo64_render_mean(const lwo_scene *s, const lwo_camera64 *cam, uint32_t x0,
             o[2] = acc[2] / (double)spp;
         }
 }
+
+__thread const lwo_theta *lwo_th;
+
+void lwo64_render_mean_theta(const lwo_scene *s, const lwo_camera64 *cam, const lwo_theta *th, uint32_t x0,
+                             uint32_t y0, uint32_t w, uint32_t h, uint32_t spp, double *out, int threads) {
+    Cam c = cam64(s, cam);
+    if (spp < 1) spp = 1;
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel num_threads(threads)
+    {
+        lwo_th = th;
+#pragma omp for schedule(dynamic, 1)
+        for (uint32_t py = 0; py < h; py++)
+            for (uint32_t px = 0; px < w; px++) {
+                double acc[3] = {0, 0, 0};
+                for (uint32_t k = 0; k < spp; k++) {
+                    V3 r = render_sample(s, &c, x0 + px, y0 + py, k);
+                    if (isfinite(r.x) && isfinite(r.y) && isfinite(r.z)) {
+                        acc[0] += r.x;
+                        acc[1] += r.y;
+                        acc[2] += r.z;
+                    }
+                }
+                double *o = out + (uint64_t)(py * w + px) * 3u;
+                for (int j = 0; j < 3; j++) o[j] = acc[j] / (double)spp;
+            }
+        lwo_th = NULL;
+    }
+}
+
+void lwo64_render_fd_theta(const lwo_scene *s, const lwo_camera64 *cam, const lwo_theta *plus,
+                           const lwo_theta *minus, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                           uint32_t spp, double *diff, double *mean, int threads) {
+    Cam c = cam64(s, cam);
+    if (spp < 1) spp = 1;
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel num_threads(threads)
+    {
+#pragma omp for schedule(dynamic, 1)
+        for (uint32_t py = 0; py < h; py++)
+            for (uint32_t px = 0; px < w; px++) {
+                double dd[3] = {0, 0, 0}, mm[3] = {0, 0, 0};
+                for (uint32_t k = 0; k < spp; k++) {
+                    lwo_th = plus;
+                    V3 a = render_sample(s, &c, x0 + px, y0 + py, k);
+                    lwo_th = minus;
+                    V3 b = render_sample(s, &c, x0 + px, y0 + py, k);
+                    if (!(isfinite(a.x) && isfinite(a.y) && isfinite(a.z) && isfinite(b.x) && isfinite(b.y) && isfinite(b.z)))
+                        continue;
+                    dd[0] += a.x - b.x;
+                    dd[1] += a.y - b.y;
+                    dd[2] += a.z - b.z;
+                    mm[0] += 0.5 * (a.x + b.x);
+                    mm[1] += 0.5 * (a.y + b.y);
+                    mm[2] += 0.5 * (a.z + b.z);
+                }
+                lwo_th = NULL;
+                uint64_t i = (uint64_t)(py * w + px) * 3u;
+                for (int j = 0; j < 3; j++) {
+                    diff[i + j] = dd[j] / (double)spp;
+                    mean[i + j] = mm[j] / (double)spp;
+                }
+            }
+    }
+}

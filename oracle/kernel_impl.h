@@ -43,6 +43,14 @@ extern __thread lwo_counters *lwo_cnt;
         if (lwo_cnt) lwo_cnt->f++; \
     } while (0)
 
+/* The differentiable form's theta (FP64 build only; the FP32 build never has one). */
+#ifdef LWO_F64
+extern __thread const lwo_theta *lwo_th;
+#define TH lwo_th
+#else
+#define TH ((const lwo_theta *)0)
+#endif
+
 static inline float f32_of(uint32_t u) {
     float f;
     memcpy(&f, &u, 4);
@@ -101,6 +109,10 @@ static inline lwo_emitter EMITTER(const lwo_scene *s, uint64_t i) {
     return s->emitters[i];
 }
 static inline REAL SKY(const lwo_scene *s, uint64_t i) {
+    if (TH && TH->sky64) {
+        if (i >= TH->sky64_len) { bounds_error(); return 0; }
+        return (REAL)TH->sky64[i];
+    }
     if (i >= s->sky_len) { bounds_error(); return 0; }
     return (REAL)s->sky[i];
 }
@@ -243,6 +255,19 @@ static inline uint32_t quad_texel(const lwo_scene *s, const lwo_quad *q, REAL ss
     REAL u = (REAL)q->uv[0] + ss * (REAL)q->uv[2] + t * (REAL)q->uvt[0];
     REAL v = (REAL)q->uv[1] + ss * (REAL)q->uv[3] + t * (REAL)q->uvt[1];
     return texel(s, u, v);
+}
+
+/* The atlas index quad_texel reads. */
+static inline uint64_t quad_texel_index(const lwo_scene *s, const lwo_quad *q, REAL ss, REAL t) {
+    ss = rmin(rmax(ss, K(0.0005)), K(0.9995));
+    t = rmin(rmax(t, K(0.0005)), K(0.9995));
+    REAL u = (REAL)q->uv[0] + ss * (REAL)q->uv[2] + t * (REAL)q->uvt[0];
+    REAL v = (REAL)q->uv[1] + ss * (REAL)q->uv[3] + t * (REAL)q->uvt[1];
+    int32_t w = (int32_t)s->params->off2[1];
+    int32_t h = (int32_t)s->params->off2[2];
+    int32_t x = clamp_i32(to_i32(R_FLOOR(u)), 0, w - 1);
+    int32_t y = clamp_i32(to_i32(R_FLOOR(v)), 0, h - 1);
+    return (uint64_t)(uint32_t)(y * w + x);
 }
 
 #define COPLANAR K(1e-5) /* trace.rs:73 */
@@ -617,6 +642,70 @@ static V3 shadow(const lwo_scene *s, V3 o, V3 d, REAL tmax) {
     return tr;
 }
 
+/* ---- the differentiable form's theta (test infrastructure for the reference gradient) ---- */
+/* The emitter group of the block at voxel (x, y, z). */
+static inline uint32_t emitter_group(int32_t x, int32_t y, int32_t z) {
+    return pcg_hash((uint32_t)x * 73856093u ^ (uint32_t)y * 19349663u ^ (uint32_t)z * 83492791u) & 31u;
+}
+
+/* A hit's linear texel colour under theta and its parameter (-1: the decoded texel). */
+static inline V3 theta_texel(const lwo_scene *s, const lwo_quad *q, const Hit *h, int32_t *param) {
+    *param = -1;
+    if (TH) {
+        uint64_t i = quad_texel_index(s, q, h->s, h->tt);
+        if (i < TH->texel_param_len) *param = TH->texel_param[i];
+        else bounds_error();
+        if (*param >= (int32_t)TH->n_params) { bounds_error(); *param = -1; }
+        if (*param >= 0) return v3((REAL)TH->albedo[3 * *param], (REAL)TH->albedo[3 * *param + 1], (REAL)TH->albedo[3 * *param + 2]);
+    }
+    return linear_rgb(h->texel);
+}
+
+/* sample_sun's cone direction about `axis` for the draws r1, r2 (integrator.rs:291-302). */
+static inline V3 cone_dir(V3 axis, REAL cos_max, REAL r1, REAL r2) {
+    REAL cos_t = K(1.0) - r1 * (K(1.0) - cos_max);
+    REAL sin_t = R_SQRT(rmax(K(1.0) - cos_t * cos_t, K(0.0)));
+    REAL sin_phi, cos_phi;
+    R_SINCOS_TURNS(r2, &sin_phi, &cos_phi);
+    V3 t, b;
+    onb(axis, &t, &b);
+    return vnormalize(vadd(vadd(vmuls(t, sin_t * cos_phi), vmuls(b, sin_t * sin_phi)), vmuls(axis, cos_t)));
+}
+
+/* shadow (integrator.rs:319-346) with the visibility of direction l0: the segments are traced
+ * along l0, and the water they cross is measured along l through the same surfaces (each hit
+ * surface's plane, met from `o` along l). */
+static V3 shadow_frozen(const lwo_scene *s, V3 o, V3 l0, V3 l) {
+    REAL eps = (REAL)s->params->misc_f[1];
+    V3 tr = V3_ONE, so = o;
+    REAL tmax = (REAL)INFINITY, u_prev = K(0.0);
+    for (int i = 0; i < 8; i++) {
+        Hit h = trace(s, so, l0, eps, tmax);
+        if (h.quad == NO_QUAD) return tr;
+        const lwo_quad *q = QUAD(s, h.quad);
+        uint32_t flags = q_flags(q);
+        V3 nq = q_normal(q);
+        REAL u = vdot(vsub(vadd(so, vmuls(l0, h.t)), o), nq) / vdot(l, nq);
+        if (flags & FLAG_WATER) {
+            if (vdot(nq, l0) > K(0.0)) {
+                REAL t = i == 0 ? u : u - (u_prev + eps);
+                tr = vmul(tr, vtransmittance(v3f4(s->params->water_color), t));
+            }
+        } else if ((flags & FLAG_ALPHA_MASK) == ALPHA_TRANSLUCENT) {
+            REAL a = (REAL)(h.texel >> 24) / K(255.0);
+            int32_t param;
+            V3 col = vmul(theta_texel(s, q, &h, &param), linear_rgb(q_tint(q)));
+            tr = vmul(tr, vlerp(V3_ONE, col, a));
+        } else {
+            return V3_ZERO;
+        }
+        so = vadd(so, vmuls(l0, h.t + eps));
+        tmax -= h.t + eps;
+        u_prev = u;
+    }
+    return tr;
+}
+
 /* pick (integrator.rs:350-353). */
 static inline uint32_t pick(uint32_t n, REAL u) {
     uint32_t i = to_u32(u * (REAL)n);
@@ -662,8 +751,11 @@ static V3 sample_emitter_face(const lwo_scene *s, V3 origin, V3 n, const lwo_emi
     REAL area = vlength(nq);
     REAL cos_l = rabs(vdot(nq, l)) / area;
     const lwo_quad *hq = QUAD(s, h.quad);
-    V3 c = vmul(linear_rgb(h.texel), linear_rgb(q_tint(hq)));
-    return vmuls(c, cos_l / rmax(dist * dist, K(1.0)) * area * q_emittance(q) * (REAL)p->misc_f[0] * scaler);
+    int32_t param;
+    V3 c = vmul(theta_texel(s, hq, &h, &param), linear_rgb(q_tint(hq)));
+    REAL intensity = (REAL)p->misc_f[0];
+    if (TH) intensity = intensity * (REAL)TH->emit_mult[emitter_group(to_i32((REAL)e->pos[0]), to_i32((REAL)e->pos[1]), to_i32((REAL)e->pos[2]))];
+    return vmuls(c, cos_l / rmax(dist * dist, K(1.0)) * area * q_emittance(q) * intensity * scaler);
 }
 
 /* sample_emitter (integrator.rs:419-433). */
@@ -770,7 +862,7 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
     V3 d = vnormalize(vadd(vadd(cam->fwd, vmuls(cam->right, sx)), vmuls(cam->up, sy)));
     V3 o = cam->pos;
 
-    V3 radiance = V3_ZERO, beta = V3_ONE;
+    V3 radiance = V3_ZERO, beta = V3_ONE, beta0 = V3_ONE; /* beta0: the frozen roulette's throughput */
     uint32_t bounces = 0;
     int specular = 1, in_water = 0;
     uint32_t strategy = p->misc_u[3] > 0 ? p->emitter[0] : EMITTER_SAMPLING_NONE;
@@ -798,7 +890,10 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
         }
         REAL tp;
         if (water_plane(s, o, d, &tp) && (!found || tp < hit.t)) {
-            if (in_water) beta = vmul(beta, vtransmittance(sigma, tp));
+            if (in_water) {
+                beta = vmul(beta, vtransmittance(sigma, tp));
+                if (TH) beta0 = vmul(beta0, vtransmittance(sigma, tp));
+            }
             int front = d.y < K(0.0);
             V3 n = v3(K(0.0), front ? K(1.0) : K(-1.0), K(0.0));
             V3 nd, no;
@@ -817,12 +912,20 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
             }
             break;
         }
-        if (in_water) beta = vmul(beta, vtransmittance(sigma, hit.t));
+        if (in_water) {
+            beta = vmul(beta, vtransmittance(sigma, hit.t));
+            if (TH) beta0 = vmul(beta0, vtransmittance(sigma, hit.t));
+        }
         const lwo_quad *q = QUAD(s, hit.quad);
         uint32_t flags = q_flags(q);
         V3 pos = vadd(o, vmuls(d, hit.t));
         REAL alpha = (REAL)(hit.texel >> 24) / K(255.0);
-        V3 albedo = vmul(linear_rgb(hit.texel), linear_rgb(q_tint(q)));
+        int32_t param;
+        V3 albedo = vmul(theta_texel(s, q, &hit, &param), linear_rgb(q_tint(q)));
+        V3 albedo0 = albedo;
+        if (TH && TH->frozen && param >= 0)
+            albedo0 = vmul(v3((REAL)TH->albedo0[3 * param], (REAL)TH->albedo0[3 * param + 1], (REAL)TH->albedo0[3 * param + 2]),
+                           linear_rgb(q_tint(q)));
         int front;
         V3 n = shading_normal(q, d, &front);
 
@@ -837,6 +940,7 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
         }
         if (!forced && (flags & FLAG_ALPHA_MASK) == ALPHA_TRANSLUCENT && rng_next(&rng) >= alpha) {
             beta = vmul(beta, vlerp(V3_ONE, albedo, alpha));
+            if (TH) beta0 = vmul(beta0, vlerp(V3_ONE, albedo0, alpha));
             o = vadd(pos, vmuls(d, eps));
             tmin = K(0.0);
             continue;
@@ -844,19 +948,33 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
         if (bounces >= max_bounces) break;
         REAL emittance = q_emittance(q) * (REAL)p->misc_f[0];
         int emits = emittance > K(0.0) && (p->emitter[1] == 0 || strategy == EMITTER_SAMPLING_NONE || bounces == 0);
+        if (emits && TH) {
+            V3 inside = vsub(pos, vmuls(n, K(1e-3)));
+            emittance = emittance * (REAL)TH->emit_mult[emitter_group(to_i32(R_FLOOR(inside.x)), to_i32(R_FLOOR(inside.y)),
+                                                                       to_i32(R_FLOOR(inside.z)))];
+        }
         if (emits) radiance = vadd(radiance, vmuls(vmul(beta, vmul(albedo, albedo)), emittance));
         bounces += 1;
 
         V3 origin = vadd(pos, vmuls(n, eps));
-        V3 sun = v3f4(p->sun_dir);
-        REAL sd3 = (REAL)p->sun_dir[3];
+        V3 sun = TH ? v3((REAL)TH->sun[0], (REAL)TH->sun[1], (REAL)TH->sun[2]) : v3f4(p->sun_dir);
+        REAL sd3 = TH ? (REAL)TH->sun[3] : (REAL)p->sun_dir[3];
         REAL sin_r = R_SQRT(rmax(K(1.0) - sd3 * sd3, K(0.0)));
         int lit = p->sun_color[0] > 0.0f || p->sun_color[1] > 0.0f || p->sun_color[2] > 0.0f;
-        if (lit && vdot(n, sun) > -sin_r && (REAL)p->sun_dir[1] > -sin_r) {
-            V3 l = sample_sun(s, &rng);
+        if (lit && vdot(n, sun) > -sin_r && sun.y > -sin_r) {
+            V3 l, l0;
+            if (TH) {
+                REAL r1 = rng_next(&rng);
+                REAL r2 = rng_next(&rng);
+                l = cone_dir(sun, sd3, r1, r2);
+                l0 = TH->frozen ? cone_dir(v3((REAL)TH->sun0[0], (REAL)TH->sun0[1], (REAL)TH->sun0[2]), (REAL)TH->sun0[3], r1, r2) : l;
+            } else {
+                l = sample_sun(s, &rng);
+                l0 = l;
+            }
             REAL cos_l = vdot(n, l);
             if (cos_l > K(0.0) && l.y >= K(0.0)) {
-                V3 tr = shadow(s, origin, l, (REAL)INFINITY);
+                V3 tr = TH && TH->frozen ? shadow_frozen(s, origin, l0, l) : shadow(s, origin, l, (REAL)INFINITY);
                 radiance = vadd(radiance, vmuls(vmul(vmul(vmul(beta, albedo), v3f4(p->sun_color)), tr), cos_l));
             }
         }
@@ -864,10 +982,12 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
             radiance = vadd(radiance, vmul(vmul(beta, albedo), sample_emitters(s, pos, origin, n, &rng)));
 
         beta = vmul(beta, albedo);
+        if (TH) beta0 = vmul(beta0, albedo0);
         if (bounces >= 3) {
-            REAL q_rr = rclamp(vmax_elem(beta), K(0.05), K(0.95));
+            REAL q_rr = rclamp(vmax_elem(TH && TH->frozen ? beta0 : beta), K(0.05), K(0.95));
             if (rng_next(&rng) > q_rr) break;
             beta = vdivs(beta, q_rr);
+            if (TH) beta0 = vdivs(beta0, q_rr);
         }
         d = cosine_hemisphere(n, &rng);
         o = origin;

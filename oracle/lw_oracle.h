@@ -91,6 +91,27 @@ typedef struct {
     double tan_half, aspect;
 } lwo_camera64;
 
+/* Parameters theta of the differentiable form, for the FP64 build's reference gradient. With a
+ * theta, a hit's albedo is the parameter of its atlas texel (texel_param, -1 = the decoded
+ * texel) times the decoded tint; an emitter's intensity is scaled by its group's entry of
+ * emit_mult (group = pcg_hash of its voxel, 32 groups); the sun direction is `sun` and the Chunky
+ * sky cache `sky64`. With `frozen`, the Russian roulette takes its probability and decision from
+ * the `albedo0` throughput and the shadow rays run along `sun0` (the crossed water's length
+ * follows `sun` through the same surfaces): the estimator whose derivative the adjoint forms. */
+typedef struct {
+    const double *albedo;      /* n_params * 3 */
+    const double *albedo0;     /* n_params * 3, the nominal albedos (frozen roulette) */
+    uint32_t n_params;
+    int32_t frozen;
+    const int32_t *texel_param; /* one per atlas texel */
+    uint64_t texel_param_len;
+    const double *emit_mult;   /* 32 */
+    const double *sky64;       /* the sky cache under theta, or NULL for the scene's sky */
+    uint64_t sky64_len;
+    double sun[4];             /* sun direction, cos of the sun's angular radius */
+    double sun0[4];            /* nominal sun direction (frozen shadow rays) */
+} lwo_theta;
+
 /* Work counters of the instrumented FP32 build (algorithmic bytes per sample). */
 typedef struct {
     uint64_t samples, events, traces, dda_steps, brick_skips, voxel_lookups, model_fetches,
@@ -147,6 +168,14 @@ void lwo64_render_sample(const lwo_scene *s, const lwo_camera64 *cam, uint32_t p
                          uint32_t sample, double out[3]);
 void lwo64_render_mean(const lwo_scene *s, const lwo_camera64 *cam, uint32_t x0, uint32_t y0,
                        uint32_t w, uint32_t h, uint32_t spp, double *out, int threads);
+/* lwo64_render_mean under a theta. */
+void lwo64_render_mean_theta(const lwo_scene *s, const lwo_camera64 *cam, const lwo_theta *th, uint32_t x0,
+                             uint32_t y0, uint32_t w, uint32_t h, uint32_t spp, double *out, int threads);
+/* Every sample under `plus` and under `minus`: per pixel the mean of the paired differences and
+ * of the pairs' midpoints (the FP64 reference gradient's finite differences). */
+void lwo64_render_fd_theta(const lwo_scene *s, const lwo_camera64 *cam, const lwo_theta *plus,
+                           const lwo_theta *minus, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                           uint32_t spp, double *diff, double *mean, int threads);
 
 #ifdef __cplusplus
 }

@@ -65,6 +65,24 @@ class Camera64(C.Structure):
                 ("up", C.c_double * 3), ("tan_half", C.c_double), ("aspect", C.c_double)]
 
 
+class Theta(C.Structure):
+    """`lwo_theta`: parameters of the differentiable form for the FP64 build."""
+    _fields_ = [("albedo", C.c_void_p), ("albedo0", C.c_void_p), ("n_params", C.c_uint32), ("frozen", C.c_int32),
+                ("texel_param", C.c_void_p), ("texel_param_len", C.c_uint64), ("emit_mult", C.c_void_p),
+                ("sky64", C.c_void_p), ("sky64_len", C.c_uint64), ("sun", C.c_double * 4), ("sun0", C.c_double * 4)]
+
+
+def make_theta(albedo, albedo0, texel_param, emit_mult, sky64, sun, sun0, frozen=True):
+    """A `Theta` and the arrays it points to (keep both alive while it is used)."""
+    keep = [np.ascontiguousarray(albedo, np.float64).reshape(-1, 3), np.ascontiguousarray(albedo0, np.float64).reshape(-1, 3),
+            np.ascontiguousarray(texel_param, np.int32), np.ascontiguousarray(emit_mult, np.float64),
+            None if sky64 is None else np.ascontiguousarray(sky64, np.float64)]
+    t = Theta(keep[0].ctypes.data, keep[1].ctypes.data, keep[0].shape[0], int(frozen), keep[2].ctypes.data,
+              keep[2].size, keep[3].ctypes.data, None if keep[4] is None else keep[4].ctypes.data,
+              0 if keep[4] is None else keep[4].size, (C.c_double * 4)(*sun), (C.c_double * 4)(*sun0))
+    return t, keep
+
+
 class Counters(C.Structure):
     _fields_ = [(n, C.c_uint64) for n in (
         "samples", "events", "traces", "dda_steps", "brick_skips", "voxel_lookups", "model_fetches",
@@ -114,6 +132,9 @@ def _declare(L):
     L.lwo_bounds_errors.restype = C.c_uint64
     L.lwo64_render_sample.argtypes = [sp, P(Camera64), C.c_uint32, C.c_uint32, C.c_uint32, D3]
     L.lwo64_render_mean.argtypes = [sp, P(Camera64)] + [C.c_uint32] * 5 + [C.c_void_p, C.c_int]
+    L.lwo64_render_mean_theta.argtypes = [sp, P(Camera64), P(Theta)] + [C.c_uint32] * 5 + [C.c_void_p, C.c_int]
+    L.lwo64_render_fd_theta.argtypes = [sp, P(Camera64), P(Theta), P(Theta)] + [C.c_uint32] * 5 + \
+        [C.c_void_p, C.c_void_p, C.c_int]
 
 
 def _arr(a, dtype):
@@ -243,6 +264,21 @@ class OracleScene:
         lib().lwo64_render_mean(self.ref, C.byref(cam) if cam is not None else None, x0, y0, w, h, spp,
                                 out.ctypes.data, threads)
         return out
+
+    def render_mean_theta(self, theta, x0, y0, w, h, spp, cam=None, threads=0):
+        """The FP64 mean radiance under a `Theta`, shape (h, w, 3)."""
+        out = np.zeros((h, w, 3), dtype=np.float64)
+        lib().lwo64_render_mean_theta(self.ref, C.byref(cam) if cam is not None else None, C.byref(theta), x0, y0, w,
+                                      h, spp, out.ctypes.data, threads)
+        return out
+
+    def render_fd_theta(self, plus, minus, x0, y0, w, h, spp, cam=None, threads=0):
+        """FP64 paired differences under two `Theta`s: (mean of plus - minus, mean of midpoints)."""
+        diff = np.zeros((h, w, 3), dtype=np.float64)
+        mean = np.zeros((h, w, 3), dtype=np.float64)
+        lib().lwo64_render_fd_theta(self.ref, C.byref(cam) if cam is not None else None, C.byref(plus),
+                                    C.byref(minus), x0, y0, w, h, spp, diff.ctypes.data, mean.ctypes.data, threads)
+        return diff, mean
 
     def count_work(self, x0, y0, w, h, spp):
         c = Counters()

@@ -81,3 +81,39 @@ def test_texel_parameters_cover_the_textures():
     sun = atlas.sprites["sun"]
     assert (tp2[sun.y:sun.y + sun.h, sun.x:sun.x + sun.w] == -1).all()
     assert tp.max() < A.SLOTS * A.TEXELS and math.prod(atlas.pixels.shape) == tp.size
+
+
+class OracleSky:
+    """Sky set-up through the oracle's f32 cache builder (no device needed)."""
+
+    def build_sky_cache(self, params, n):
+        return O.OracleScene(params, None, None, None, None, None, None).build_sky_cache(n)
+
+
+def test_fp64_oracle_theta_hooks_leave_the_nominal_render():
+    # At albedos equal to the decoded texels, unit emitter groups, the frame's own sun and sky,
+    # the FP64 oracle under a theta renders what it renders without one; freezing the roulette and
+    # the shadow rays at that same theta changes nothing beyond rounding.
+    from lumenwright_b200 import request as R
+    cfg = R.Config("t", 2, 24, 14, 4, 4, 4000, "chunky", emitters=True)
+    frame = R.make_frame(cfg, sky_backend=OracleSky())
+    view = O.OracleScene.from_frame(frame)
+    p = frame.params
+    atlas = S.build_atlas(cfg.seed)
+    tp, _ = A.texel_parameters(atlas, np.zeros(256, np.float32))
+    alb = np.zeros((A.SLOTS * A.TEXELS, 3))
+    px = atlas.pixels.ravel()
+    m = tp >= 0
+    for c in range(3):
+        alb[tp[m], c] = (((px[m] >> (8 * c)) & 0xFF) / 255.0) ** 2.2
+    sun = [float(x) for x in p["sun_dir"]]
+    th, keep = O.make_theta(alb, alb, tp, np.ones(A.GROUPS), frame.sky.astype(np.float64), sun, sun, frozen=False)
+    want = view.render_mean64(0, 0, 24, 14, 4)
+    got = view.render_mean_theta(th, 0, 0, 24, 14, 4)
+    assert np.allclose(got, want, rtol=1e-12, atol=1e-15)
+    thf, keepf = O.make_theta(alb, alb, tp, np.ones(A.GROUPS), frame.sky.astype(np.float64), sun, sun, frozen=True)
+    assert np.allclose(view.render_mean_theta(thf, 0, 0, 24, 14, 4), want, rtol=1e-9, atol=1e-12)
+    # paired differences of a theta with itself vanish
+    diff, mean = view.render_fd_theta(thf, thf, 0, 0, 24, 14, 4)
+    assert not diff.any() and np.allclose(mean, want, rtol=1e-9, atol=1e-12)
+    assert O.bounds_errors() == 0

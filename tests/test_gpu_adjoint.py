@@ -1,6 +1,11 @@
 """The differentiable form on the GPU: at the nominal parameters the forward image is the plain
 renderer's, and the path-replay adjoint matches paired central finite differences (h = 1e-3) to
-1e-3 relative on sky, emitter and albedo parameters of a small frame of the differentiation world."""
+1e-3 relative on sky, emitter and albedo parameters of a small frame of the differentiation world,
+and agrees with the FP64 CPU reference gradient (central differences of the FP64 oracle under
+theta)."""
+
+import json
+import os
 
 import numpy as np
 import pytest
@@ -8,13 +13,15 @@ import pytest
 from lumenwright_b200 import adjoint as A
 
 pytestmark = pytest.mark.gpu
+FULL = os.environ.get("LW_ADJ_FULL") == "1"
 
 
 @pytest.fixture(scope="module")
 def problem():
     from lumenwright_b200.native import Context
     c = Context(0)
-    p = A.DiffProblem(c, width=96, height=54, spp=8)
+    # LW_ADJ_FULL=1: the differentiation workload itself (512x288, 64 spp)
+    p = A.DiffProblem(c, 512, 288, 64) if FULL else A.DiffProblem(c, width=96, height=54, spp=8)
     yield p
     c.close()
 
@@ -43,3 +50,58 @@ def test_adjoint_matches_central_differences(problem):
         floor = 1e-6 * np.abs(fd[m]).max()
         bad = np.abs(ad[m] - fd[m]) > 1e-3 * np.maximum(np.abs(fd[m]), np.abs(ad[m])) + floor
         assert not bad.any(), [rows[i] for i in np.nonzero(m)[0][bad]]
+
+
+def fp64_reference_gradient(p, ks, h=1e-6):
+    """The FP64 CPU reference gradient: central differences (step h, in FP64) of the FP64 oracle's
+    loss under theta, every sample paired, the roulette and the shadow rays frozen at the nominal
+    theta (the estimator the adjoint differentiates)."""
+    from oracle import oracle as O
+    sp = A.split(p.theta0)
+    params, cache = p.frame(sp.sky)
+    hq = p.hq
+    view = O.OracleScene(params, hq.grid, hq.models, hq.quads, hq.atlas, hq.emitters, hq.emitter_grid, sky=cache)
+    t0 = p.theta0.astype(np.float64)
+    alb0 = t0[:A.N_ALBEDO]
+    cos_max = float(params["sun_dir"][3])
+
+    def theta(t):
+        az, alt, tb = t[A.N_ALBEDO + A.GROUPS:]
+        sun = list(A.sun_vector(az, alt)) + [cos_max]
+        sun0 = list(A.sun_vector(*t0[A.N_ALBEDO + A.GROUPS:A.N_ALBEDO + A.GROUPS + 2])) + [cos_max]
+        return O.make_theta(t[:A.N_ALBEDO], alb0, p.texel_param, t[A.N_ALBEDO:A.N_ALBEDO + A.GROUPS],
+                            A.sky_cache_f64(az, alt, tb), sun, sun0, frozen=True)
+
+    out = []
+    for k in ks:
+        tp, tm = t0.copy(), t0.copy()
+        tp[k] += h
+        tm[k] -= h
+        (a, ka), (b, kb) = theta(tp), theta(tm)
+        diff, mean = view.render_fd_theta(a, b, 0, 0, p.width, p.height, p.spp)
+        out.append(float(np.sum(diff * 2.0 * (mean - p.target))) / (2.0 * h))
+    assert O.bounds_errors() == 0
+    return np.array(out)
+
+
+def test_adjoint_against_fp64_reference_gradient(problem):
+    p = problem
+    idx = p.check_indices(n=64 if FULL else 48, seed=4)
+    loss, g = p.gradient(p.theta0)
+    ref = fp64_reference_gradient(p, idx)
+    ad = g[idx]
+    rel = np.abs(ad - ref) / np.maximum(np.maximum(np.abs(ad), np.abs(ref)), 1e-300)
+    report = {"frame": [p.width, p.height, p.spp], "params": len(idx), "nonzero": int(np.count_nonzero(ref)),
+              "median_rel": float(np.median(rel)), "max_rel": float(rel.max()),
+              "within_1e-3": int(np.count_nonzero(rel <= 1e-3)), "within_1e-2": int(np.count_nonzero(rel <= 1e-2)),
+              "rows": [{"name": A.name_of(int(k)), "adjoint": float(a), "fp64": float(r), "rel": float(e)}
+                       for k, a, r, e in zip(idx, ad, ref, rel)]}
+    out = os.environ.get("LW_REPORT_DIR")
+    if out:
+        os.makedirs(out, exist_ok=True)
+        with open(os.path.join(out, "adjoint_fp64_reference.json"), "w") as f:
+            json.dump(report, f, indent=1)
+    # The FP32 adjoint and the FP64 reference differ only where a sample's path splits between the
+    # two precisions (an edge met, a roulette or Fresnel draw at its threshold).
+    assert np.count_nonzero(ref) >= 24
+    assert rel.max() < 1e-3, report
