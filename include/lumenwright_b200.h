@@ -112,14 +112,27 @@ typedef struct {
     uint64_t samples;        /* path samples traced */
 } lw_stats;
 
-/* Launch tuning of the render kernel (the autotuner's knobs): threads per block (64, 128 or 256),
- * the regrouping period (voxel visits a ray advances per loop iteration before its lane may shade
- * and start its next ray; 0 = a whole traversal at once), and the samples per work item (0: chosen
- * from the frame so every lane gets many items). */
+/* Launch tuning of the render (the autotuner's knobs).
+ * engine: how lw_render_hq / lw_render_device run: LW_ENGINE_WAVEFRONT (the default) keeps each
+ *   path in a slot of a pool in device memory and alternates a shading kernel with a tracing kernel
+ *   whose lanes take the next queued ray as soon as theirs ends; LW_ENGINE_MEGAKERNEL runs one
+ *   persistent kernel in which each lane follows its own paths. Both give the same image, bit for
+ *   bit. The batched form, the per-sample entry point and lw_render_accumulate_noalloc always run
+ *   the megakernel.
+ * threads: threads per block of the megakernel (64, 128 or 256).
+ * budget: voxel visits a ray advances before its lane may take up other work: the megakernel's
+ *   regrouping period (0 = a whole traversal at once), the wavefront's visits between queue
+ *   fetches (0 = 4).
+ * sub: samples per work item (0: chosen from the frame so every lane gets many items).
+ * paths: path slots of the wavefront (0: sized from each launch's sample count, 2^16 to 2^23). */
+#define LW_ENGINE_WAVEFRONT 0u
+#define LW_ENGINE_MEGAKERNEL 1u
 typedef struct {
     uint32_t threads;
     uint32_t budget;
     uint32_t sub;
+    uint32_t engine;
+    uint32_t paths;
 } lw_tuning;
 
 /* ---- context ------------------------------------------------------------------------------
@@ -132,7 +145,8 @@ const char *lw_last_error(const lw_ctx *ctx);
 /* The CUDA stream (cudaStream_t) the context launches its path-tracing kernels on. */
 void *lw_stream(lw_ctx *ctx);
 lw_status lw_get_stats(const lw_ctx *ctx, lw_stats *out);
-/* Sets / reads the launch tuning of a context (defaults: 128 threads, budget 0, sub automatic). */
+/* Sets / reads the launch tuning of a context (defaults: wavefront engine with automatic path
+ * slots, 128 threads, budget 0, sub automatic). */
 lw_status lw_set_tuning(lw_ctx *ctx, const lw_tuning *tuning);
 lw_status lw_get_tuning(const lw_ctx *ctx, lw_tuning *out);
 /* Asks a running render on `ctx` to stop; it returns LW_ERR_CANCELLED. Safe from any thread. */

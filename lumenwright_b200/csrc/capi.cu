@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -91,7 +92,7 @@ struct lw_ctx {
     DBuf<uint32_t> cancel_word;      // device word the render kernel polls; set by lw_cancel
     cudaStream_t aux = nullptr;      // lw_cancel's stream, so the write lands while a render runs
     lw_stats stats{};
-    lw_tuning tuning{128, 0, 0};
+    lw_tuning tuning{128, 0, 0, LW_ENGINE_WAVEFRONT, 0};
     // the batched form
     struct BatchSky { const float *host; uint64_t len; DBuf<float> dev; };
     std::vector<BatchSky *> batch_skies;
@@ -105,6 +106,13 @@ struct lw_ctx {
     cudaGraphExec_t batch_graph = nullptr;
     uint64_t batch_samples = 0;
     size_t partials_cap_bytes = size_t(4) << 30;
+    // the wavefront engine: path slots (grown to the largest pool used), queue fetch settings
+    uint32_t wf_tail = 4;
+    LaunchShape shape_wf{};
+    DBuf<float4> wf_state, wf_hit0, wf_ts;
+    DBuf<float> wf_hit1;
+    DBuf<uint32_t> wf_queue, wf_ctr;
+    uint32_t *wf_host = nullptr;  // pinned word the iteration count is read into
     // the differentiable form: per frame slot (0 and 1: the frames, 2: the nominal frame)
     DBuf<float> adj_albedo[3], adj_sky[3], adj_emit[3];
     DBuf<int32_t> adj_tparam[3];
@@ -259,6 +267,42 @@ lw_status ensure_accum(lw_ctx *c, uint32_t w, uint32_t h) {
     return LW_OK;
 }
 
+// One launch's items through the wavefront iterations, until no slot has a ray left. The pool
+// holds one slot per 16 samples of the launch (a power of two from 2^16 to 2^23, and no more slots
+// than items): a larger pool keeps more rays in each iteration, so the iterations' fixed costs and
+// their last long traversals weigh less, at 328 bytes of device memory per slot.
+lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const WorkDesc &W) {
+    uint32_t n = c->tuning.paths;
+    if (n == 0) {
+        uint64_t want = (uint64_t)W.w * W.h * W.spp / 16u;
+        n = 1u << 16;
+        while (n < want && n < (1u << 23)) n <<= 1;
+        while (n > (1u << 10) && (n >> 1) >= W.n_items) n >>= 1;
+    }
+    const uint32_t budget = c->tuning.budget ? c->tuning.budget : 4u;
+    CK(c, ensure(c->wf_state, (size_t)kWfWords * n), "allocating the path slots");
+    CK(c, ensure(c->wf_hit0, n), "allocating the hits");
+    CK(c, ensure(c->wf_ts, (size_t)3 * n), "allocating the carried traversals");
+    CK(c, ensure(c->wf_hit1, n), "allocating the hits");
+    CK(c, ensure(c->wf_queue, n), "allocating the ray queue");
+    CK(c, ensure(c->wf_ctr, 8), "allocating the queue counters");
+    if (!c->wf_host) CK(c, cudaMallocHost((void **)&c->wf_host, 4), "allocating a pinned word");
+    WfState F{c->wf_state.p, n, c->wf_queue.p, c->wf_hit0.p, c->wf_hit1.p, c->wf_ctr.p, c->wf_ts.p};
+    CK(c, cudaMemsetAsync(c->wf_state.p + (size_t)4 * n, 0, (size_t)n * sizeof(float4), c->stream), "clearing the slots");
+    CK(c, cudaMemsetAsync(c->wf_ctr.p, 0, 8 * sizeof(uint32_t), c->stream), "clearing the queue counters");
+    CK(c, cudaMemsetAsync(c->wf_hit0.p, 0, (size_t)n * sizeof(float4), c->stream), "clearing the hits");
+    for (uint32_t t = 0;; t++) {
+        CK(c, launch_wf_iteration(S, P, W, F, c->shape_wf, t & 1u, budget, c->wf_tail, c->stream), "launching an iteration");
+        if ((t & 15u) == 15u) {
+            CK(c, cudaMemcpyAsync(c->wf_host, c->wf_ctr.p + 4 * (t & 1u), 4, cudaMemcpyDeviceToHost, c->stream),
+               "reading the queue length");
+            CK(c, cudaStreamSynchronize(c->stream), "running the iterations");
+            if (*(volatile uint32_t *)c->wf_host == 0u) break;
+        }
+    }
+    return LW_OK;
+}
+
 // Launches the accumulating render of samples [s0, s0 + spp) over the whole frame, in batches.
 // With `progress`, each batch is waited for and reported; without it nothing waits.
 lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32_t spp, lw_progress_fn progress,
@@ -275,7 +319,12 @@ lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32
         WorkDesc W = work(c, 0, 0, w, h, s0 + done, n, pl.sub);
         CK(c, cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream), "clearing the work counter");
         CK(c, cudaEventRecord(c->ev_a, c->stream), "recording an event");
-        CK(c, launch_render(MODE_ACCUM, S, P, W, c->shape_accum, c->stream), "launching the render kernel");
+        if (c->tuning.engine == LW_ENGINE_WAVEFRONT) {
+            lw_status ws = run_wavefront(c, S, P, W);
+            if (ws != LW_OK) return ws;
+        } else {
+            CK(c, launch_render(MODE_ACCUM, S, P, W, c->shape_accum, c->stream), "launching the render kernel");
+        }
         CK(c, cudaEventRecord(c->ev_b, c->stream), "recording an event");
         CK(c, launch_reduce(W, c->acc.p, w, c->stream), "launching the reduction");
         c->stats.launches++;
@@ -332,6 +381,7 @@ lw_status lw_ctx_create(int device, lw_ctx **out) {
     if ((e = ensure(c->gamma, 256)) != cudaSuccess) return bail(e, "allocating the gamma table");
     if ((e = cudaMemcpy(c->gamma.p, lut, sizeof lut, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "uploading the gamma table");
     if ((e = ensure(c->counter, 1)) != cudaSuccess || (e = ensure(c->error, 1)) != cudaSuccess) return bail(e, "allocating counters");
+    c->shape_wf = wf_trace_shape(device);
     c->shape_accum = render_shape(MODE_ACCUM, device, (int)c->tuning.threads);
     c->shape_samples = render_shape(MODE_SAMPLES, device, (int)c->tuning.threads);
     *out = c;
@@ -366,6 +416,13 @@ void lw_ctx_destroy(lw_ctx *c) {
         c->adj_tparam[k].free_();
     }
     for (auto *b : {&c->adj_img, &c->adj_img2, &c->adj_g}) b->free_();
+    c->wf_state.free_();
+    c->wf_hit0.free_();
+    c->wf_ts.free_();
+    c->wf_hit1.free_();
+    c->wf_queue.free_();
+    c->wf_ctr.free_();
+    if (c->wf_host) cudaFreeHost(c->wf_host);
     for (auto *b : {&c->sky, &c->gamma, &c->out_rgb, &c->samples, &c->rays}) b->free_();
     c->acc.free_();
     c->hits.free_();
@@ -397,6 +454,9 @@ lw_status lw_set_tuning(lw_ctx *c, const lw_tuning *t) {
     if (t->threads != 64 && t->threads != 128 && t->threads != 256)
         return fail(c, LW_ERR_INVALID_ARGUMENT, "threads per block %u (64, 128 or 256)", t->threads);
     if (t->sub > 4096) return fail(c, LW_ERR_INVALID_ARGUMENT, "sub %u", t->sub);
+    if (t->engine != LW_ENGINE_WAVEFRONT && t->engine != LW_ENGINE_MEGAKERNEL)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "engine %u", t->engine);
+    if (t->paths > (1u << 26)) return fail(c, LW_ERR_INVALID_ARGUMENT, "paths %u (at most 2^26)", t->paths);
     cudaSetDevice(c->device);
     c->tuning = *t;
     c->shape_accum = render_shape(MODE_ACCUM, c->device, (int)t->threads);

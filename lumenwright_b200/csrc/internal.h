@@ -81,6 +81,22 @@ LaunchShape batch_shape(int device, int threads, bool resume);
 cudaError_t launch_render_batch(const DevScene &S, const BatchDesc &B, LaunchShape shape, cudaStream_t st);
 cudaError_t launch_reduce_batch(const BatchDesc &B, cudaStream_t st);
 
+// wavefront.cu: the render as shade / trace iterations over a pool of path slots.
+constexpr int kWfWords = 16;
+struct WfState {
+    float4 *state;    // kWfWords float4 per slot, word k of slot i at state[k * n + i]
+    uint32_t n;       // slots
+    uint32_t *queue;  // slot ids of the rays to trace this iteration
+    float4 *hit0;     // per slot: t, quad, texel, s of its last ray
+    float *hit1;      // per slot: tt
+    uint32_t *ctr;    // per iteration parity: queue length, trace fetch counter, -, -
+    float4 *ts;       // 3 float4 per slot (word k at ts[k * n + i]): a carried-over traversal
+};
+LaunchShape wf_trace_shape(int device);
+cudaError_t launch_wf_iteration(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F,
+                                LaunchShape trace_shape, uint32_t parity, uint32_t budget, uint32_t tail,
+                                cudaStream_t st);
+
 // adjoint.cu: the differentiable form.
 #define LW_ADJ_EMITTER_GROUPS 32
 struct AdjFrame {

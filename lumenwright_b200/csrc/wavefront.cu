@@ -1,0 +1,310 @@
+// The wavefront form of the render: the persistent megakernel's lanes wait, at every ray, for the
+// longest traversal of their warp (traversal lengths are heavy-tailed: a ray along the terrain
+// visits hundreds of voxels, most visit a few). Here the path state lives in a pool of slots in
+// device memory and each iteration runs two kernels:
+//   k_wf_shade  one thread per slot: the state machine of device_path.cuh on the slot's last hit
+//               (or a new item), up to the slot's next ray, whose slot id it appends to the queue;
+//   k_wf_trace  a small persistent kernel: each lane takes the next queued ray as soon as its
+//               current one is done (dynamic fetch, a few voxel visits between fetches), so the
+//               warps stay full until the queue runs dry.
+// Items, samples per item and the order of every Kahan addition are the megakernel's, so the
+// partial sums and the image are bit-identical to it.
+#include "device_path.cuh"
+#include "internal.h"
+
+namespace lw {
+namespace {
+
+enum : uint32_t { F_ACTIVE = 1u, F_DEAD = 2u };
+// hit0.y of a slot whose ray is still being traversed (carried over to the next iteration).
+constexpr uint32_t RESUME_MARK = 0xFFFFFFFEu;
+
+// Slot words (float4, word k of slot i at state[k * n + i]). The core words are read and written
+// at every shading step; the next-event words only while a shadow or emitter ray is on its way
+// (before a step whose ray was one, after a step that queues one); the item words only when a
+// sample ends.
+enum {
+    W_O = 0,       // o.xyz, tmin
+    W_D = 1,       // d.xyz, tmax
+    W_RAD = 2,     // radiance.xyz, kind
+    W_BETA = 3,    // beta.xyz, rng
+    W_CORE = 4,    // bounces, events, specular | in_water << 1, flags (F_ACTIVE, F_DEAD)
+    W_N = 5,       // n.xyz, cos_l          (next-event words)
+    W_ORIGIN = 6,  // origin.xyz, seg
+    W_TR = 7,      // tr.xyz, dist
+    W_ESUM = 8,    // esum.xyz, list
+    W_FSUM = 9,    // fsum.xyz, count
+    W_EOFF = 10,   // eoff.xyz, k
+    W_E1 = 11,     // first, faces, f, emode | fmode << 1
+    W_ITEM = 12,   // px, py, sample, s_end (item words)
+    W_ITEM2 = 13,  // j, pixel slot, -, -
+    W_SUM = 14,    // s0, s1, s2, c0
+    W_SUM2 = 15,   // c1, c2, -, -
+};
+
+LW_DI float4 ld(const WfState &F, int k, uint32_t i) { return F.state[(size_t)k * F.n + i]; }
+LW_DI void st(const WfState &F, int k, uint32_t i, float4 v) { F.state[(size_t)k * F.n + i] = v; }
+LW_DI float4 pk(V3 a, float w) { return make_float4(a.x, a.y, a.z, w); }
+LW_DI float4 pku(V3 a, uint32_t w) { return make_float4(a.x, a.y, a.z, __uint_as_float(w)); }
+LW_DI float4 u4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
+    return make_float4(__uint_as_float(a), __uint_as_float(b), __uint_as_float(c), __uint_as_float(d));
+}
+LW_DI uint32_t fu(float x) { return __float_as_uint(x); }
+
+LW_DI void load_core(const WfState &F, uint32_t i, Path &p, float4 core) {
+    float4 a = ld(F, W_O, i), b = ld(F, W_D, i), c = ld(F, W_RAD, i), d = ld(F, W_BETA, i);
+    p.o = f4v(a);
+    p.tmin = a.w;
+    p.d = f4v(b);
+    p.tmax = b.w;
+    p.radiance = f4v(c);
+    p.kind = fu(c.w);
+    p.beta = f4v(d);
+    p.rng = fu(d.w);
+    p.bounces = fu(core.x);
+    p.events = fu(core.y);
+    p.specular = (fu(core.z) & 1u) != 0u;
+    p.in_water = (fu(core.z) & 2u) != 0u;
+}
+
+LW_DI void load_nee(const WfState &F, uint32_t i, Path &p) {
+    float4 a = ld(F, W_N, i), b = ld(F, W_ORIGIN, i), c = ld(F, W_TR, i), d = ld(F, W_ESUM, i);
+    p.n = f4v(a);
+    p.cos_l = a.w;
+    p.origin = f4v(b);
+    p.seg = fu(b.w);
+    p.tr = f4v(c);
+    p.dist = c.w;
+    p.esum = f4v(d);
+    p.list = fu(d.w);
+    a = ld(F, W_FSUM, i), b = ld(F, W_EOFF, i), c = ld(F, W_E1, i);
+    p.fsum = f4v(a);
+    p.count = fu(a.w);
+    p.eoff = f4v(b);
+    p.k = fu(b.w);
+    p.first = fu(c.x);
+    p.faces = fu(c.y);
+    p.f = fu(c.z);
+    p.emode = fu(c.w) & 1u;
+    p.fmode = fu(c.w) >> 1;
+}
+
+LW_DI void store_core(const WfState &F, uint32_t i, const Path &p, uint32_t flags) {
+    st(F, W_O, i, pk(p.o, p.tmin));
+    st(F, W_D, i, pk(p.d, p.tmax));
+    st(F, W_RAD, i, pku(p.radiance, p.kind));
+    st(F, W_BETA, i, pku(p.beta, p.rng));
+    st(F, W_CORE, i, u4(p.bounces, p.events, (p.specular ? 1u : 0u) | (p.in_water ? 2u : 0u), flags));
+}
+
+LW_DI void store_nee(const WfState &F, uint32_t i, const Path &p) {
+    st(F, W_N, i, pk(p.n, p.cos_l));
+    st(F, W_ORIGIN, i, pku(p.origin, p.seg));
+    st(F, W_TR, i, pk(p.tr, p.dist));
+    st(F, W_ESUM, i, pku(p.esum, p.list));
+    st(F, W_FSUM, i, pku(p.fsum, p.count));
+    st(F, W_EOFF, i, pku(p.eoff, p.k));
+    st(F, W_E1, i, u4(p.first, p.faces, p.f, p.emode | (p.fmode << 1)));
+}
+
+// One ticket per calling lane from `ctr`, one atomic per group of converged lanes.
+LW_DI uint32_t ticket(uint32_t *ctr) {
+    unsigned am = __activemask();
+    uint32_t lane = threadIdx.x & 31u;
+    int leader = __ffs(am) - 1;
+    uint32_t base = 0;
+    if ((int)lane == leader) base = atomicAdd(ctr, (uint32_t)__popc(am));
+    base = __shfl_sync(am, base, leader);
+    return base + (uint32_t)__popc(am & ((1u << lane) - 1u));
+}
+
+// The next item of the launch, or W.n_items when none is left (or the render is cancelled: the
+// cancel word is read when an item number crosses a multiple of 4096, as the megakernel does).
+LW_DI uint32_t next_item(const WorkDesc &W) {
+    uint32_t item = ticket(W.counter);
+    if ((item & 4095u) == 0u && *W.cancel) atomicMax(W.counter, W.n_items);
+    return item;
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(128) k_wf_shade(const DevScene S, const DevParams P, const WorkDesc W, const WfState F,
+                                                  uint32_t parity) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0) {
+        // The queue counters of the next iteration (the trace kernel of the previous one is done).
+        F.ctr[4 * (parity ^ 1u)] = 0u;
+        F.ctr[4 * (parity ^ 1u) + 1] = 0u;
+    }
+    if (i >= F.n) return;
+    float4 core = ld(F, W_CORE, i);
+    uint32_t flags = fu(core.w);
+    if (flags & F_DEAD) return;
+    Path p;
+    Act a = A_END;
+    if (flags & F_ACTIVE) {
+        float4 h0 = F.hit0[i];
+        if (fu(h0.y) == RESUME_MARK) return;  // its ray is still on its way: nothing to shade yet
+        load_core(F, i, p, core);
+        if (p.kind != K_EXTEND) load_nee(F, i, p);
+        Hit h{h0.x, fu(h0.y), fu(h0.z), h0.w, F.hit1[i]};
+        a = shade(p, S, P, h);
+    }
+    if (a == A_END) {
+        // The sample is over: the item's sums, then its next sample or the next item.
+        float4 it = ld(F, W_ITEM, i), it2 = ld(F, W_ITEM2, i), sa = ld(F, W_SUM, i), sb = ld(F, W_SUM2, i);
+        uint32_t px = fu(it.x), py = fu(it.y), sample = fu(it.z), s_end = fu(it.w);
+        uint32_t j = fu(it2.x), pslot = fu(it2.y);
+        float s0 = sa.x, s1 = sa.y, s2 = sa.z, c0 = sa.w, c1 = sb.x, c2 = sb.y;
+        while (a == A_END) {
+            if (flags & F_ACTIVE) {
+                if (finite3(p.radiance)) {
+                    kahan_add(s0, c0, p.radiance.x);
+                    kahan_add(s1, c1, p.radiance.y);
+                    kahan_add(s2, c2, p.radiance.z);
+                }
+                sample++;
+                if (sample < s_end) {
+                    begin_sample(p, P, px, py, sample);
+                    a = A_TRACE;
+                    break;
+                }
+                W.partials[(size_t)j * W.n_slots + pslot] = make_float4(s0 - c0, s1 - c1, s2 - c2, 0.0f);
+                flags &= ~F_ACTIVE;
+            }
+            uint32_t item = next_item(W);
+            if (item >= W.n_items) {
+                flags |= F_DEAD;
+                break;
+            }
+            j = item / W.n_slots;
+            pslot = item - j * W.n_slots;
+            uint32_t tile = pslot >> 5, in = pslot & 31u;
+            uint32_t rx = (tile % W.tiles_x) * 8u + (in & 7u);
+            uint32_t ry = (tile / W.tiles_x) * 4u + (in >> 3);
+            if (rx < W.w && ry < W.h) {
+                px = W.x0 + rx;
+                py = W.y0 + ry;
+                sample = W.sample_start + j * W.sub;
+                s_end = min(sample + W.sub, W.sample_start + W.spp);
+                s0 = s1 = s2 = c0 = c1 = c2 = 0.0f;
+                begin_sample(p, P, px, py, sample);
+                flags |= F_ACTIVE;
+                a = A_TRACE;
+            }
+        }
+        st(F, W_ITEM, i, u4(px, py, sample, s_end));
+        st(F, W_ITEM2, i, u4(j, pslot, 0u, 0u));
+        st(F, W_SUM, i, make_float4(s0, s1, s2, c0));
+        st(F, W_SUM2, i, make_float4(c1, c2, 0.0f, 0.0f));
+    }
+    if (a == A_TRACE) {
+        F.queue[ticket(&F.ctr[4 * parity])] = i;
+        store_core(F, i, p, flags);
+        if (p.kind != K_EXTEND) store_nee(F, i, p);
+    } else {
+        st(F, W_CORE, i, u4(0u, 0u, 0u, flags));
+    }
+}
+
+#ifndef LW_WF_TRACE_MINB
+#define LW_WF_TRACE_MINB 8
+#endif
+// Traces the queued rays of this iteration: each lane takes a ray, advances it by at most `budget`
+// voxel visits per round, and takes the next queued ray as soon as its ray ends. Once the queue
+// has run dry, a ray still on its way after `tail` more rounds saves its traversal state and goes
+// to the next iteration's queue, so an iteration does not wait for its single longest ray.
+__global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevScene S, const DevParams P, const WfState F,
+                                                                      uint32_t parity, uint32_t budget, uint32_t tail) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t count = *(volatile uint32_t *)&F.ctr[4 * parity];
+    uint32_t *fetch = &F.ctr[4 * parity + 1];
+    TraceState ts;
+    V3 o = v3(0.0f, 0.0f, 0.0f), d = o;
+    float tmin = 0.0f;
+    uint32_t slot = 0, rounds = 0;
+    bool have = false, done = false;
+    for (;;) {
+        bool need = !have && !done;
+        unsigned m = __ballot_sync(FULL, need);
+        if (m) {
+            int leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(fetch, (uint32_t)__popc(m));
+            base = __shfl_sync(FULL, base, leader);
+            if (need) {
+                uint32_t q = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+                if (q >= count) {
+                    done = true;
+                } else {
+                    slot = F.queue[q];
+                    float4 a = ld(F, W_O, slot), b = ld(F, W_D, slot);
+                    o = f4v(a);
+                    tmin = a.w;
+                    d = f4v(b);
+                    if (fu(F.hit0[slot].y) == RESUME_MARK) {
+                        // a ray carried over from the previous iteration
+                        float4 t0 = F.ts[slot], t1 = F.ts[F.n + slot], t2 = F.ts[2 * (size_t)F.n + slot];
+                        ts.s.c0 = (int)fu(t0.x);
+                        ts.s.c1 = (int)fu(t0.y);
+                        ts.s.c2 = (int)fu(t0.z);
+                        ts.s.n0 = t0.w;
+                        ts.s.n1 = t1.x;
+                        ts.s.n2 = t1.y;
+                        ts.s.t = t1.z;
+                        ts.inv = v3(t1.w, t2.x, t2.y);
+                        ts.t_end = t2.z;
+                        ts.it = fu(t2.w);
+                        have = true;
+                    } else if (trace_begin(ts, P, o, d, b.w)) {
+                        have = true;
+                    } else {
+                        F.hit0[slot] = make_float4(kINF, __uint_as_float(NO_QUAD), 0.0f, 0.0f);
+                        F.hit1[slot] = 0.0f;
+                    }
+                }
+            }
+        }
+        if (__all_sync(FULL, done && !have)) break;
+        if (__any_sync(FULL, done)) rounds++;  // the queue is dry: count the tail rounds
+        if (have) {
+            Hit h = no_hit();
+            int r = trace_run(S, P, ts, o, d, tmin, budget, h);
+            if (r != 0) {
+                if (r != 1) h = no_hit();
+                F.hit0[slot] = make_float4(h.t, __uint_as_float(h.quad), __uint_as_float(h.texel), h.s);
+                F.hit1[slot] = h.tt;
+                have = false;
+            } else if (rounds > tail) {
+                F.ts[slot] = u4((uint32_t)ts.s.c0, (uint32_t)ts.s.c1, (uint32_t)ts.s.c2, fu(ts.s.n0));
+                F.ts[F.n + slot] = make_float4(ts.s.n1, ts.s.n2, ts.s.t, ts.inv.x);
+                F.ts[2 * (size_t)F.n + slot] = make_float4(ts.inv.y, ts.inv.z, ts.t_end, __uint_as_float(ts.it));
+                F.hit0[slot] = make_float4(0.0f, __uint_as_float(RESUME_MARK), 0.0f, 0.0f);
+                F.queue[ticket(&F.ctr[4 * (parity ^ 1u)])] = slot;
+                have = false;
+                done = true;
+            }
+        }
+    }
+}
+
+LaunchShape wf_trace_shape(int device) {
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_wf_trace, 128, 0);
+    if (per_sm < 1) per_sm = 1;
+    return LaunchShape{sms * per_sm, 128};
+}
+
+cudaError_t launch_wf_iteration(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F,
+                                LaunchShape trace_shape, uint32_t parity, uint32_t budget, uint32_t tail,
+                                cudaStream_t st) {
+    k_wf_shade<<<(F.n + 127) / 128, 128, 0, st>>>(S, P, W, F, parity);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_wf_trace<<<trace_shape.blocks, trace_shape.threads, 0, st>>>(S, P, F, parity, budget, tail);
+    return cudaGetLastError();
+}
+
+}  // namespace lw

@@ -62,7 +62,12 @@ class Stats(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("threads", C.c_uint32), ("budget", C.c_uint32), ("sub", C.c_uint32)]
+    _fields_ = [("threads", C.c_uint32), ("budget", C.c_uint32), ("sub", C.c_uint32), ("engine", C.c_uint32),
+                ("paths", C.c_uint32)]
+
+
+ENGINE_WAVEFRONT = 0  # LW_ENGINE_WAVEFRONT
+ENGINE_MEGAKERNEL = 1  # LW_ENGINE_MEGAKERNEL
 
 
 class CameraJob(C.Structure):
@@ -198,14 +203,18 @@ class Context:
     def cancel(self):
         self.L.lw_cancel(self.h)
 
-    def set_tuning(self, threads=128, budget=0, sub=0):
-        """Launch tuning of the render kernel (see `lw_tuning`)."""
-        self._check(self.L.lw_set_tuning(self.h, C.byref(Tuning(threads, budget, sub))))
+    def set_tuning(self, threads=None, budget=None, sub=None, engine=None, paths=None):
+        """Launch tuning of the render (see `lw_tuning`); the knobs not given keep their values."""
+        t = self.get_tuning()
+        for k, v in (("threads", threads), ("budget", budget), ("sub", sub), ("engine", engine), ("paths", paths)):
+            if v is not None:
+                t[k] = int(v)
+        self._check(self.L.lw_set_tuning(self.h, C.byref(Tuning(**t))))
 
     def get_tuning(self) -> dict:
         t = Tuning()
         self._check(self.L.lw_get_tuning(self.h, C.byref(t)))
-        return {"threads": t.threads, "budget": t.budget, "sub": t.sub}
+        return {"threads": t.threads, "budget": t.budget, "sub": t.sub, "engine": t.engine, "paths": t.paths}
 
     def mark(self, slot: int):
         """Records a CUDA event on the context's stream."""

@@ -79,3 +79,20 @@ def test_c1_render_hq_matches_the_cpu_backend(ctx, c1):
     print(f"C1 mean: {ok:.5f} of pixels within 1e-4; mean {img.mean():.6f} vs {want.mean():.6f}")
     assert ok >= 0.99
     assert abs(img.mean() - want.mean()) <= 1e-4 * abs(want.mean())
+
+
+@pytest.mark.parametrize("paths", [0, 1 << 12])
+def test_wavefront_and_megakernel_give_the_same_image(ctx, c2, paths):
+    # The wavefront engine (path slots, shade and trace iterations, rays carried across iterations)
+    # and the persistent megakernel take the same items in the same order of Kahan additions: the
+    # images are equal bit for bit, with the automatic pool and with a small one that carries many
+    # rays over.
+    from lumenwright_b200.native import ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT
+    p = c2.params
+    ctx.upload_hq_scene(c2.scene)
+    ctx.set_tuning(engine=ENGINE_MEGAKERNEL)
+    want = ctx.render_hq(p, c2.sky, 12)
+    ctx.set_tuning(engine=ENGINE_WAVEFRONT, paths=paths)
+    got = ctx.render_hq(p, c2.sky, 12)
+    ctx.set_tuning(engine=ENGINE_WAVEFRONT, paths=0)
+    assert np.array_equal(got, want)
