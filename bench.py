@@ -88,36 +88,12 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def algorithmic_bytes_per_sample(frame, cache_path):
-    """Bytes the kernel must read per path sample, counted by the instrumented FP32 oracle over a
-    sample of the frame (a 40x24 sub-grid of pixels, 8 spp), with the per-access sizes of the
-    hot-path scope table: 8 B per DDA step (top + overlay entry), 2 B per non-uniform voxel id,
-    16 B per model, 80 B per quad test, 4 B per texel, 48 B per sky-cache read, 96 B per map
-    read (4 corners x 3 f32 x 2 rows), 8 B per emitter cell, 4 B per index, 32 B per emitter,
-    16 B per accumulated sample."""
-    if os.path.exists(cache_path):
-        with open(cache_path) as f:
-            d = json.load(f)
-        if d.get("workload") == WORKLOAD:
-            return d
-    from oracle import oracle as O
-    v = O.OracleScene.from_frame(frame)
-    w, h = int(frame.params["frame"][0]), int(frame.params["frame"][1])
-    total = None
-    # 40x24 pixels spread over the frame: each counted at 8 spp.
-    for y in np.linspace(0, h - 1, 24).astype(int):
-        c = v.count_work(0, int(y), w, 1, 1)  # a full row at 1 spp keeps the cost bounded
-        total = c if total is None else {k: total[k] + c[k] for k in c}
-    n = total["samples"]
-    b = (8 * total["dda_steps"] + 2 * total["voxel_lookups"] + 16 * total["model_fetches"] + 80 * total["quad_tests"]
-         + 4 * total["texel_fetches"] + 8 * total["overlay_reads"] + 48 * total["sky_reads"] + 96 * total["map_reads"]
-         + 8 * total["emitter_cell_reads"] + 4 * total["emitter_index_reads"] + 32 * total["emitter_reads"] + 16 * n)
-    d = {"workload": WORKLOAD, "bytes_per_sample": b / n, "counts_per_sample": {k: total[k] / n for k in total},
-         "sampled": n}
-    os.makedirs(os.path.dirname(cache_path), exist_ok=True)
-    with open(cache_path, "w") as f:
-        json.dump(d, f, indent=1)
-    return d
+def algorithmic_bytes(path):
+    """Bytes per path sample the tracing and shading kernels must read, from the committed counts
+    of the instrumented FP32 oracle on the c2 frame (tests/test_work_counts.py recounts them and
+    holds the per-access byte sizes)."""
+    with open(path) as f:
+        return json.load(f)
 
 
 def cpu_baseline(frame, budget_s=15.0):
@@ -212,9 +188,10 @@ class OracleSkyOnHost:
 
 def run_batched(args):
     """The batched form: 64 seeded cameras (320x180..1920x1080, spp from {16, 64, 256, 1024} scaled
-    by --c3-scale, 4-8 bounces, ticks 4000/12800) over the 12x12-chunk world in one graph-captured
-    persistent launch, tuned by the autotuner, against the same cameras as 64 separate plain
-    launches (each with its own launch and reduction)."""
+    by --c3-scale, 4-8 bounces, ticks 4000/12800) over the 12x12-chunk world in one CUDA graph (the
+    wavefront engine's device-side iteration loop, or the persistent megakernel, as the autotuner
+    picks), against the same cameras as 64 separate plain renders (`lw_render_device` with the
+    default tuning, each with its own iterations and reduction)."""
     from lumenwright_b200 import batch as BT
     from lumenwright_b200.native import Context
     ctx = Context(0)
@@ -232,7 +209,7 @@ def run_batched(args):
     ctx.mark(1)
     batched_ms = ctx.elapsed(0, 1) / args.steps
     # The same cameras as separate plain launches.
-    ctx.set_tuning(128, 0, 0)
+    ctx.set_tuning(threads=128, budget=0, sub=0, engine=0, paths=0)
     sep_ms = 0.0
     order = sorted(range(len(jobs)), key=lambda i: id(jobs[i][1]))
     last_sky = None
@@ -370,13 +347,17 @@ def main():
         dist.barrier()
     ctx.mark(0)
     launches = 0
-    kernel_ms = 0.0
+    trace_ms = shade_ms = kernel_ms = 0.0
+    trace_launches = 0
     with ClockSampler(local) as clocks:
         for i in range(args.steps):
             device_step(args.warmup + i)
             st = ctx.stats()
-            launches += st["launches"] * 2  # render + reduce per batch
+            launches += st["launches"]
             kernel_ms += st["kernel_ms"]
+            trace_ms += st["trace_ms"]
+            shade_ms += st["shade_ms"]
+            trace_launches += st["trace_launches"]
         ctx.mark(1)
         total_ms = ctx.elapsed(0, 1)
     if dist:
@@ -387,7 +368,6 @@ def main():
         # The frame: every rank's mean over its samples, reduced to rank 0 (one NCCL reduce).
         shard.reduce_means(ctx.read_accumulator(w, h), dist, device=f"cuda:{local}")
     value = samples_per_step * args.steps * world / (total_ms / 1e3) / 1e6
-    avg_launch_ms = kernel_ms / max(1, launches // 2)
 
     # End to end through the public render_hq with host buffers, every step.
     from lumenwright_b200.native import B200Backend
@@ -413,22 +393,31 @@ def main():
 
     if rank == 0:
         peak, peak_kind = peaks()
-        alg = algorithmic_bytes_per_sample(frame, os.path.join(ROOT, "profiles", "algorithmic_bytes_c2.json"))
-        achieved = alg["bytes_per_sample"] * samples_per_step / (avg_launch_ms / 1e3) / 1e9
+        alg = algorithmic_bytes(os.path.join(ROOT, "profiles", "algorithmic_bytes_c2.json"))
+        # The dominant kernel is the wavefront's tracing kernel: the scene bytes its traversals read
+        # per launch over its average launch time (CUDA events around each launch).
+        my_samples = samples_per_step * args.steps
+        trace_bytes = alg["trace_bytes_per_sample"] * my_samples
+        achieved = trace_bytes / (trace_ms / 1e3) / 1e9 if trace_ms > 0 else None
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "width": w, "height": h, "spp": spp, "bounces": int(p["frame"][3]),
                        "parallelism": f"sample ranges x{world}" if world > 1 else "1 GPU",
-                       "l2": "inputs (scene + sky maps, ~30 MB) stay L2-resident by design; the per-step "
-                             "accumulator and partial sums are written fresh each step",
+                       "engine": "wavefront", "tuning": ctx.get_tuning(),
+                       "l2": "the scene and sky maps (~30 MB) stay L2-resident by design; the path slots "
+                             "(up to 2.7 GB) and the partial sums are larger than L2",
                        "emitters": cfg.notes.get("emitters"), "day_weight": cfg.notes.get("weight")},
             "e2e": {"value": e2e, "unit": "Msamples/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                         "traffic": None, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_sample": alg["bytes_per_sample"]},
+            "kernels": {"trace_ms": trace_ms, "shade_ms": shade_ms, "other_ms": kernel_ms - trace_ms - shade_ms,
+                        "trace_launches": trace_launches},
+            "roofline": {"bound": "hbm", "kernel": "k_wf_trace", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak if achieved else None, "traffic": None, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": trace_bytes / max(1, trace_launches),
+                         "avg_launch_ms": trace_ms / max(1, trace_launches),
+                         "trace_bytes_per_sample": alg["trace_bytes_per_sample"]},
             "clocks": clocks.summary(),
         }
         if not args.no_cpu_baseline:

@@ -107,9 +107,12 @@ typedef void (*lw_progress_fn)(uint32_t done, uint32_t total, void *user);
 typedef struct {
     double kernel_ms;        /* CUDA-event time of the path-tracing launches */
     double upload_ms;        /* host-to-device copies and the grid re-layout of the last upload */
-    uint32_t launches;       /* path-tracing kernel launches */
-    uint32_t blocks, threads; /* launch shape (persistent: blocks = SMs x resident blocks) */
+    uint32_t launches;       /* kernel launches of the render (path tracing and reductions) */
+    uint32_t blocks, threads; /* launch shape of the megakernel (blocks = SMs x resident blocks) */
     uint64_t samples;        /* path samples traced */
+    /* the wavefront engine: CUDA-event time and launches of its tracing and shading kernels */
+    double trace_ms, shade_ms;
+    uint32_t trace_launches, shade_launches;
 } lw_stats;
 
 /* Launch tuning of the render (the autotuner's knobs).

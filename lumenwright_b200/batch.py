@@ -3,8 +3,9 @@
 ``c3_jobs`` builds the 64 seeded cameras of the batching configuration over the 12x12-chunk
 world: resolutions drawn uniformly from 320x180 to 1920x1080 (16:9), spp from {16, 64, 256, 1024},
 4 to 8 bounces, times of day 4000 (Chunky's sky) or 12800 (the game sky at dusk). ``Autotuner``
-picks the launch tuning (threads per block, regrouping period, samples per work item) by timing
-short trial batches, and keeps the winner per workload class in a JSON cache.
+picks the launch tuning (engine, queue depth, visits between queue fetches or regrouping period,
+threads per block, samples per work item) by timing short trial batches, and keeps the winner per
+workload class in a JSON cache.
 """
 
 import hashlib
@@ -96,17 +97,29 @@ def c3_jobs(sky_backend, cams=None, spp_scale=1.0):
 
 
 class Autotuner:
-    """Picks the render kernel's launch tuning for a workload by timing trial renders.
+    """Picks the batched render's launch tuning for a workload by timing trial renders.
 
-    Candidates: threads per block {64, 128, 256} x regrouping period {0 (whole traversals), 24}
-    x samples per work item {automatic, 16, 64}. A trial renders the workload with every camera's
-    spp cut to ``trial_fraction`` of it (at least 1). The winner is cached per workload class (the
-    rounded totals of pixels and samples and the bounce range) in ``$LUMENWRIGHT_CACHE/autotune.json``
+    Candidates: the wavefront engine with queue depth (path slots) {automatic, 2^22, 2^23} x visits
+    between queue fetches {4, 8}, and the persistent megakernel with threads per block {64, 128,
+    256} x regrouping period {0 (whole traversals), 24}; each with samples per work item
+    {automatic, 16}. A trial renders the workload with every camera's spp cut to
+    ``trial_fraction`` of it (at least 1). The winner is cached per workload class (the rounded
+    totals of pixels and samples and the bounce range) in ``$LUMENWRIGHT_CACHE/autotune.json``
     (default ``~/.cache/lumenwright_b200``)."""
 
-    THREADS = (128, 64, 256)
-    BUDGETS = (0, 24)
-    SUBS = (0, 16, 64)
+    SUBS = (0, 16)
+
+    @classmethod
+    def candidates(cls):
+        out = []
+        for sub in cls.SUBS:
+            for paths in (0, 1 << 22, 1 << 23):
+                for budget in (4, 8):
+                    out.append({"engine": 0, "threads": 128, "budget": budget, "sub": sub, "paths": paths})
+            for threads in (128, 64, 256):
+                for budget in (0, 24):
+                    out.append({"engine": 1, "threads": threads, "budget": budget, "sub": sub, "paths": 0})
+        return out
 
     def __init__(self, ctx, cache_dir=None, trial_fraction=1 / 32):
         self.ctx = ctx
@@ -139,22 +152,20 @@ class Autotuner:
         """Sets and returns the best tuning for ``jobs`` (a list of (params, sky, spp))."""
         h, key = self.workload_class(jobs)
         table = self._load()
-        if not force and h in table:
+        if not force and h in table and set(table[h]["tuning"]) == set(self.candidates()[0]):
             t = table[h]["tuning"]
             self.ctx.set_tuning(**t)
             return t, table[h]
         trial = [(p, sky, max(1, int(round(spp * self.trial_fraction)))) for p, sky, spp in jobs]
         results = []
-        for threads in self.THREADS:
-            for budget in self.BUDGETS:
-                for sub in self.SUBS:
-                    self.ctx.set_tuning(threads, budget, sub)
-                    self.ctx.batch_prepare(trial)
-                    self.ctx.batch_run()  # warm
-                    self.ctx.stats()
-                    self.ctx.batch_run()
-                    ms = self.ctx.stats()["kernel_ms"]
-                    results.append(({"threads": threads, "budget": budget, "sub": sub}, ms))
+        for t in self.candidates():
+            self.ctx.set_tuning(**t)
+            self.ctx.batch_prepare(trial)
+            self.ctx.batch_run()  # warm
+            self.ctx.stats()
+            self.ctx.batch_run()
+            ms = self.ctx.stats()["kernel_ms"]
+            results.append((t, ms))
         best = min(results, key=lambda r: r[1])
         entry = {"key": key, "tuning": best[0], "trial_ms": best[1],
                  "trials": [{"tuning": t, "ms": ms} for t, ms in results]}

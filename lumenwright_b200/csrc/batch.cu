@@ -9,17 +9,6 @@
 
 namespace lw {
 
-// The index of the job whose range [begin, next begin) holds `x` (begins ascending, first 0).
-LW_DI uint32_t find_job(const uint32_t *begins, uint32_t n, uint32_t x) {
-    uint32_t lo = 0, hi = n;
-    while (hi - lo > 1) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (ldg(begins + mid) <= x) lo = mid;
-        else hi = mid;
-    }
-    return lo;
-}
-
 // RESUME: advance each ray by at most B.budget voxel visits per loop iteration (the regrouping
 // period), as k_render does with it.
 template <int THREADS, bool RESUME>

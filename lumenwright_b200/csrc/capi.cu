@@ -91,6 +91,7 @@ struct lw_ctx {
     int *cancel_host = nullptr;      // host flag, read between launches
     DBuf<uint32_t> cancel_word;      // device word the render kernel polls; set by lw_cancel
     cudaStream_t aux = nullptr;      // lw_cancel's stream, so the write lands while a render runs
+    cudaStream_t cap = nullptr;      // the stream a graph's loop body is captured on
     lw_stats stats{};
     lw_tuning tuning{128, 0, 0, LW_ENGINE_WAVEFRONT, 0};
     // the batched form
@@ -109,10 +110,22 @@ struct lw_ctx {
     // the wavefront engine: path slots (grown to the largest pool used), queue fetch settings
     uint32_t wf_tail = 4;
     LaunchShape shape_wf{};
-    DBuf<float4> wf_state, wf_hit0, wf_ts;
-    DBuf<float> wf_hit1;
-    DBuf<uint32_t> wf_queue, wf_ctr;
+    struct WfBufs {
+        DBuf<float4> state, hit0, ts;
+        DBuf<float> hit1;
+        DBuf<uint32_t> queue, ctr;
+        void free_() {
+            state.free_();
+            hit0.free_();
+            ts.free_();
+            hit1.free_();
+            queue.free_();
+            ctr.free_();
+        }
+    };
+    WfBufs wf, bwf;  // the single-frame renders' pool; the batch graph's own (its pointers are baked in)
     uint32_t *wf_host = nullptr;  // pinned word the iteration count is read into
+    cudaEvent_t wf_ev[48] = {};   // per iteration of a 16-iteration window: before shade, between, after trace
     // the differentiable form: per frame slot (0 and 1: the frames, 2: the nominal frame)
     DBuf<float> adj_albedo[3], adj_sky[3], adj_emit[3];
     DBuf<int32_t> adj_tparam[3];
@@ -267,36 +280,76 @@ lw_status ensure_accum(lw_ctx *c, uint32_t w, uint32_t h) {
     return LW_OK;
 }
 
+// The wavefront's pool of n path slots, its queue and counters, cleared on `st` for a new render.
+lw_status wf_setup(lw_ctx *c, lw_ctx::WfBufs &b, uint32_t n, WfState &F, cudaStream_t st) {
+    CK(c, ensure(b.state, (size_t)kWfWords * n), "allocating the path slots");
+    CK(c, ensure(b.hit0, n), "allocating the hits");
+    CK(c, ensure(b.ts, (size_t)3 * n), "allocating the carried traversals");
+    CK(c, ensure(b.hit1, n), "allocating the hits");
+    CK(c, ensure(b.queue, n), "allocating the ray queue");
+    CK(c, ensure(b.ctr, 12), "allocating the queue counters");
+    if (!c->wf_host) CK(c, cudaMallocHost((void **)&c->wf_host, 4), "allocating a pinned word");
+    F = WfState{b.state.p, n, b.queue.p, b.hit0.p, b.hit1.p, b.ctr.p, b.ts.p};
+    // the slots' core words (flags 0: no item yet), the counters and the iteration, the hits
+    CK(c, cudaMemsetAsync(b.state.p + (size_t)4 * n, 0, (size_t)n * sizeof(float4), st), "clearing the slots");
+    CK(c, cudaMemsetAsync(b.ctr.p, 0, 12 * sizeof(uint32_t), st), "clearing the queue counters");
+    CK(c, cudaMemsetAsync(b.hit0.p, 0, (size_t)n * sizeof(float4), st), "clearing the hits");
+    return LW_OK;
+}
+
+// Path slots for a render of `samples` samples in `items` work items: one per 16 samples, a power
+// of two from 2^16 to 2^23, no more than the items (or the tuning's count).
+uint32_t wf_slots(const lw_ctx *c, uint64_t samples, uint64_t items) {
+    if (c->tuning.paths) return c->tuning.paths;
+    uint64_t want = samples / 16u;
+    uint32_t n = 1u << 16;
+    while (n < want && n < (1u << 23)) n <<= 1;
+    while (n > (1u << 10) && (n >> 1) >= items) n >>= 1;
+    return n;
+}
+
+void reset_stats(lw_ctx *c) {
+    double up = c->stats.upload_ms;
+    c->stats = lw_stats{};
+    c->stats.upload_ms = up;
+}
+
 // One launch's items through the wavefront iterations, until no slot has a ray left. The pool
 // holds one slot per 16 samples of the launch (a power of two from 2^16 to 2^23, and no more slots
 // than items): a larger pool keeps more rays in each iteration, so the iterations' fixed costs and
 // their last long traversals weigh less, at 328 bytes of device memory per slot.
 lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const WorkDesc &W) {
-    uint32_t n = c->tuning.paths;
-    if (n == 0) {
-        uint64_t want = (uint64_t)W.w * W.h * W.spp / 16u;
-        n = 1u << 16;
-        while (n < want && n < (1u << 23)) n <<= 1;
-        while (n > (1u << 10) && (n >> 1) >= W.n_items) n >>= 1;
-    }
+    const uint32_t n = wf_slots(c, (uint64_t)W.w * W.h * W.spp, W.n_items);
     const uint32_t budget = c->tuning.budget ? c->tuning.budget : 4u;
-    CK(c, ensure(c->wf_state, (size_t)kWfWords * n), "allocating the path slots");
-    CK(c, ensure(c->wf_hit0, n), "allocating the hits");
-    CK(c, ensure(c->wf_ts, (size_t)3 * n), "allocating the carried traversals");
-    CK(c, ensure(c->wf_hit1, n), "allocating the hits");
-    CK(c, ensure(c->wf_queue, n), "allocating the ray queue");
-    CK(c, ensure(c->wf_ctr, 8), "allocating the queue counters");
-    if (!c->wf_host) CK(c, cudaMallocHost((void **)&c->wf_host, 4), "allocating a pinned word");
-    WfState F{c->wf_state.p, n, c->wf_queue.p, c->wf_hit0.p, c->wf_hit1.p, c->wf_ctr.p, c->wf_ts.p};
-    CK(c, cudaMemsetAsync(c->wf_state.p + (size_t)4 * n, 0, (size_t)n * sizeof(float4), c->stream), "clearing the slots");
-    CK(c, cudaMemsetAsync(c->wf_ctr.p, 0, 8 * sizeof(uint32_t), c->stream), "clearing the queue counters");
-    CK(c, cudaMemsetAsync(c->wf_hit0.p, 0, (size_t)n * sizeof(float4), c->stream), "clearing the hits");
+    WfState F;
+    lw_status s = wf_setup(c, c->wf, n, F, c->stream);
+    if (s != LW_OK) return s;
+    if (!c->wf_ev[0])
+        for (auto &e : c->wf_ev) CK(c, cudaEventCreate(&e), "creating events");
+    // Iterations in windows of 16: the host reads the last queue length of each window and stops
+    // after the first window whose last iteration had nothing to trace.
     for (uint32_t t = 0;; t++) {
-        CK(c, launch_wf_iteration(S, P, W, F, c->shape_wf, t & 1u, budget, c->wf_tail, c->stream), "launching an iteration");
+        cudaEvent_t *e = c->wf_ev + 3 * (t & 15u);
+        CK(c, cudaEventRecord(e[0], c->stream), "recording an event");
+        CK(c, launch_wf_shade(S, P, W, F, c->stream), "launching the shading kernel");
+        CK(c, cudaEventRecord(e[1], c->stream), "recording an event");
+        CK(c, launch_wf_trace(S, P, F, c->shape_wf, budget, c->wf_tail, c->stream), "launching the tracing kernel");
+        CK(c, cudaEventRecord(e[2], c->stream), "recording an event");
+        CK(c, launch_wf_advance(F, c->stream), "launching the iteration step");
+        c->stats.shade_launches++;
+        c->stats.trace_launches++;
+        c->stats.launches += 3;
         if ((t & 15u) == 15u) {
-            CK(c, cudaMemcpyAsync(c->wf_host, c->wf_ctr.p + 4 * (t & 1u), 4, cudaMemcpyDeviceToHost, c->stream),
+            CK(c, cudaMemcpyAsync(c->wf_host, F.ctr + 4 * (t & 1u), 4, cudaMemcpyDeviceToHost, c->stream),
                "reading the queue length");
             CK(c, cudaStreamSynchronize(c->stream), "running the iterations");
+            for (int k = 0; k < 16; k++) {
+                float a = 0.f, b = 0.f;
+                cudaEventElapsedTime(&a, c->wf_ev[3 * k], c->wf_ev[3 * k + 1]);
+                cudaEventElapsedTime(&b, c->wf_ev[3 * k + 1], c->wf_ev[3 * k + 2]);
+                c->stats.shade_ms += a;
+                c->stats.trace_ms += b;
+            }
             if (*(volatile uint32_t *)c->wf_host == 0u) break;
         }
     }
@@ -327,7 +380,7 @@ lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32
         }
         CK(c, cudaEventRecord(c->ev_b, c->stream), "recording an event");
         CK(c, launch_reduce(W, c->acc.p, w, c->stream), "launching the reduction");
-        c->stats.launches++;
+        c->stats.launches += c->tuning.engine == LW_ENGINE_WAVEFRONT ? 1u : 2u;
         c->stats.samples += (uint64_t)w * h * n;
         done += n;
         if (progress || done < spp) {
@@ -342,6 +395,64 @@ lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32
             c->stats.kernel_ms = -1.0;  // read by lw_get_stats once the last launch is done
         }
     }
+    return LW_OK;
+}
+
+// The batched form on the wavefront engine as one CUDA graph: clear the work counter, the
+// accumulators and the path slots; then a loop node (a conditional WHILE node) whose body is one
+// iteration (shade every slot, trace the queue, advance) and which runs again while the last
+// iteration had rays to trace, all decided on the device; then the per-camera reduction.
+lw_status batch_graph_wavefront(lw_ctx *c, const BatchDesc &B, const DevParams &P0, uint64_t pixels, uint32_t slots) {
+    if (!c->cap) CK(c, cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking), "creating a capture stream");
+    const uint32_t budget = c->tuning.budget ? c->tuning.budget : 4u;
+    // The buffers first (cleared outside the graph too, which is harmless).
+    WfState F;
+    lw_status s = wf_setup(c, c->bwf, slots, F, c->stream);
+    if (s != LW_OK) return s;
+    CK(c, cudaStreamSynchronize(c->stream), "preparing the path slots");
+    DevScene S = dev_scene(c);
+    cudaGraph_t graph = nullptr;
+    CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "starting the graph capture");
+    cudaError_t e = cudaMemsetAsync(B.counter, 0, 4, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->batch_acc.p, 0, sizeof(Accum) * pixels, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(F.state + (size_t)4 * F.n, 0, (size_t)F.n * sizeof(float4), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(F.ctr, 0, 12 * sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(F.hit0, 0, (size_t)F.n * sizeof(float4), c->stream);
+    cudaGraphNode_t loop_node = nullptr;
+    if (e == cudaSuccess) {
+        cudaStreamCaptureStatus status;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t *deps = nullptr;
+        size_t ndeps = 0;
+        e = cudaStreamGetCaptureInfo(c->stream, &status, nullptr, &g, &deps, &ndeps);
+        cudaGraphConditionalHandle loop{};
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault);
+        cudaGraphNodeParams np{};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = loop;
+        np.conditional.type = cudaGraphCondTypeWhile;
+        np.conditional.size = 1;
+        if (e == cudaSuccess) e = cudaGraphAddNode(&loop_node, g, deps, ndeps, &np);
+        if (e == cudaSuccess) {
+            cudaGraph_t body = np.conditional.phGraph_out[0];
+            e = cudaStreamBeginCaptureToGraph(c->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            if (e == cudaSuccess) {
+                cudaError_t eb = launch_wf_shade_batch(S, P0, B, F, c->cap);
+                if (eb == cudaSuccess) eb = launch_wf_trace(S, P0, F, c->shape_wf, budget, c->wf_tail, c->cap);
+                if (eb == cudaSuccess) eb = launch_wf_advance_graph(F, loop, c->cap);
+                cudaGraph_t done = nullptr;
+                e = cudaStreamEndCapture(c->cap, &done);
+                if (eb != cudaSuccess) e = eb;
+            }
+        }
+        if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(c->stream, &loop_node, 1, cudaStreamSetCaptureDependencies);
+    }
+    if (e == cudaSuccess) e = launch_reduce_batch(B, c->stream);
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
+    if (e == cudaSuccess) e = e2;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&c->batch_graph, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(c, e, "building the batch graph");
     return LW_OK;
 }
 
@@ -416,13 +527,11 @@ void lw_ctx_destroy(lw_ctx *c) {
         c->adj_tparam[k].free_();
     }
     for (auto *b : {&c->adj_img, &c->adj_img2, &c->adj_g}) b->free_();
-    c->wf_state.free_();
-    c->wf_hit0.free_();
-    c->wf_ts.free_();
-    c->wf_hit1.free_();
-    c->wf_queue.free_();
-    c->wf_ctr.free_();
+    c->wf.free_();
+    c->bwf.free_();
     if (c->wf_host) cudaFreeHost(c->wf_host);
+    for (auto e : c->wf_ev)
+        if (e) cudaEventDestroy(e);
     for (auto *b : {&c->sky, &c->gamma, &c->out_rgb, &c->samples, &c->rays}) b->free_();
     c->acc.free_();
     c->hits.free_();
@@ -430,6 +539,7 @@ void lw_ctx_destroy(lw_ctx *c) {
     delete c->cancel_host;
     c->cancel_word.free_();
     if (c->aux) cudaStreamDestroy(c->aux);
+    if (c->cap) cudaStreamDestroy(c->cap);
     if (c->ev_a) cudaEventDestroy(c->ev_a);
     if (c->ev_b) cudaEventDestroy(c->ev_b);
     for (auto m : c->marks)
@@ -624,9 +734,7 @@ lw_status lw_render_device(lw_ctx *c, const lw_params *params, uint32_t sample_s
     if (spp == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "spp is 0");
     __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
     CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
-    c->stats.launches = 0;
-    c->stats.samples = 0;
-    c->stats.kernel_ms = 0;
+    reset_stats(c);
     return render_batches(c, params, sample_start, spp, nullptr, nullptr, spp);
 }
 
@@ -688,9 +796,7 @@ lw_status lw_render_hq(lw_ctx *c, const lw_params *params, const float *sky, uin
     if (s != LW_OK) return s;
     __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
     CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
-    c->stats.launches = 0;
-    c->stats.samples = 0;
-    c->stats.kernel_ms = 0;
+    reset_stats(c);
     s = render_batches(c, params, 0, spp, progress, user, spp);
     if (s != LW_OK) return s;
     return lw_read_accumulator(c, out_rgb);
@@ -767,9 +873,7 @@ lw_status lw_render_hq_reference_port(lw_ctx *c, const lw_params *params, const 
     CK(c, cudaMemsetAsync(acc.p, 0, sizeof(float4) * (size_t)w * h, c->stream), "clearing the accumulator");
     DevScene Sv = dev_scene(c);
     DevParams P = dev_params(params);
-    c->stats.launches = 0;
-    c->stats.samples = 0;
-    c->stats.kernel_ms = 0;
+    reset_stats(c);
     uint32_t done = 0, batch = 1;
     lw_status result = LW_OK;
     while (done < spp) {
@@ -887,6 +991,13 @@ lw_status lw_batch_prepare(lw_ctx *c, const lw_camera_job *jobs, uint32_t n) {
     CK(c, cudaStreamSynchronize(c->stream), "uploading jobs");
     BatchDesc B{c->batch_jobs.p, c->batch_item_begin.p, c->batch_slot_begin.p, n, (uint32_t)items, (uint32_t)slots,
                 c->tuning.budget, c->counter.p, c->batch_partials.p, c->cancel_word.p};
+    if (c->tuning.engine == LW_ENGINE_WAVEFRONT) {
+        lw_status ws = batch_graph_wavefront(c, B, dj[0].P, pixels, wf_slots(c, total_samples, items));
+        if (ws != LW_OK) return ws;
+        c->batch_host.assign(jobs, jobs + n);
+        c->batch_samples = total_samples;
+        return LW_OK;
+    }
     LaunchShape shape = batch_shape(c->device, (int)c->tuning.threads, c->tuning.budget != 0);
     // Clear, render, reduce: one CUDA graph, replayed by lw_batch_run.
     cudaGraph_t graph = nullptr;

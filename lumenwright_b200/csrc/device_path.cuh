@@ -360,4 +360,15 @@ LW_DI void kahan_add(float &s, float &c, float x) {
 
 LW_DI bool finite3(V3 v) { return isfinite(v.x) && isfinite(v.y) && isfinite(v.z); }
 
+// The index of the job whose range [begin, next begin) holds `x` (begins ascending, first 0).
+LW_DI uint32_t find_job(const uint32_t *begins, uint32_t n, uint32_t x) {
+    uint32_t lo = 0, hi = n;
+    while (hi - lo > 1) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (ldg(begins + mid) <= x) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 }  // namespace lw

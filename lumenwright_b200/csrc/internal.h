@@ -89,13 +89,17 @@ struct WfState {
     uint32_t *queue;  // slot ids of the rays to trace this iteration
     float4 *hit0;     // per slot: t, quad, texel, s of its last ray
     float *hit1;      // per slot: tt
-    uint32_t *ctr;    // per iteration parity: queue length, trace fetch counter, -, -
+    uint32_t *ctr;    // per iteration parity: queue length, trace fetch counter, -, -; [8]: iteration
     float4 *ts;       // 3 float4 per slot (word k at ts[k * n + i]): a carried-over traversal
 };
 LaunchShape wf_trace_shape(int device);
-cudaError_t launch_wf_iteration(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F,
-                                LaunchShape trace_shape, uint32_t parity, uint32_t budget, uint32_t tail,
-                                cudaStream_t st);
+cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, cudaStream_t st);
+cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const BatchDesc &B, const WfState &F,
+                                  cudaStream_t st);
+cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState &F, LaunchShape trace_shape,
+                            uint32_t budget, uint32_t tail, cudaStream_t st);
+cudaError_t launch_wf_advance(const WfState &F, cudaStream_t st);
+cudaError_t launch_wf_advance_graph(const WfState &F, cudaGraphConditionalHandle loop, cudaStream_t st);
 
 // adjoint.cu: the differentiable form.
 #define LW_ADJ_EMITTER_GROUPS 32

@@ -118,19 +118,49 @@ LW_DI uint32_t ticket(uint32_t *ctr) {
     return base + (uint32_t)__popc(am & ((1u << lane) - 1u));
 }
 
-// The next item of the launch, or W.n_items when none is left (or the render is cancelled: the
-// cancel word is read when an item number crosses a multiple of 4096, as the megakernel does).
-LW_DI uint32_t next_item(const WorkDesc &W) {
-    uint32_t item = ticket(W.counter);
-    if ((item & 4095u) == 0u && *W.cancel) atomicMax(W.counter, W.n_items);
-    return item;
-}
-
 }  // namespace
 
-__global__ void __launch_bounds__(128) k_wf_shade(const DevScene S, const DevParams P, const WorkDesc W, const WfState F,
-                                                  uint32_t parity) {
+// The slot's item: in the single-frame form one of W's, in the batched form one of B's cameras
+// (found by a binary search over the cameras' item ranges).
+struct ItemRef {
+    uint32_t job, j, pslot, px, py, sample, s_end;
+    bool valid;
+};
+
+template <bool BATCH>
+LW_DI ItemRef decode_item(const WorkDesc &W, const BatchDesc &B, uint32_t item) {
+    ItemRef r{};
+    uint32_t n_slots, tiles_x, w, h, x0 = 0, y0 = 0, sample_start, spp, sub, local = item;
+    if (BATCH) {
+        r.job = find_job(B.item_begin, B.n_jobs, item);
+        const DevJob &J = B.jobs[r.job];
+        local = item - J.item_begin;
+        n_slots = J.n_slots, tiles_x = J.tiles_x, w = J.w, h = J.h;
+        sample_start = J.sample_start, spp = J.spp, sub = J.sub;
+    } else {
+        n_slots = W.n_slots, tiles_x = W.tiles_x, w = W.w, h = W.h, x0 = W.x0, y0 = W.y0;
+        sample_start = W.sample_start, spp = W.spp, sub = W.sub;
+    }
+    r.j = local / n_slots;
+    r.pslot = local - r.j * n_slots;
+    uint32_t tile = r.pslot >> 5, in = r.pslot & 31u;
+    uint32_t rx = (tile % tiles_x) * 8u + (in & 7u);
+    uint32_t ry = (tile / tiles_x) * 4u + (in >> 3);
+    r.valid = rx < w && ry < h;
+    r.px = x0 + rx;
+    r.py = y0 + ry;
+    r.sample = sample_start + r.j * sub;
+    r.s_end = min(r.sample + sub, sample_start + spp);
+    return r;
+}
+
+// One shading step per slot. The iteration's parity (which queue counters are this iteration's)
+// is the device word ctr[8], advanced by k_wf_advance after each trace.
+template <bool BATCH>
+__global__ void __launch_bounds__(128) k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
+                                                  const BatchDesc B, const WfState F) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t parity = *(volatile uint32_t *)&F.ctr[8] & 1u;
     if (i == 0) {
         // The queue counters of the next iteration (the trace kernel of the previous one is done).
         F.ctr[4 * (parity ^ 1u)] = 0u;
@@ -140,6 +170,8 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene S, const DevPar
     float4 core = ld(F, W_CORE, i);
     uint32_t flags = fu(core.w);
     if (flags & F_DEAD) return;
+    float4 it2 = ld(F, W_ITEM2, i);
+    uint32_t job = BATCH ? fu(it2.z) : 0u;
     Path p;
     Act a = A_END;
     if (flags & F_ACTIVE) {
@@ -148,11 +180,17 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene S, const DevPar
         load_core(F, i, p, core);
         if (p.kind != K_EXTEND) load_nee(F, i, p);
         Hit h{h0.x, fu(h0.y), fu(h0.z), h0.w, F.hit1[i]};
-        a = shade(p, S, P, h);
+        if (BATCH) {
+            DevScene S = S0;
+            S.sky = B.jobs[job].sky;
+            a = shade(p, S, B.jobs[job].P, h);
+        } else {
+            a = shade(p, S0, P0, h);
+        }
     }
     if (a == A_END) {
         // The sample is over: the item's sums, then its next sample or the next item.
-        float4 it = ld(F, W_ITEM, i), it2 = ld(F, W_ITEM2, i), sa = ld(F, W_SUM, i), sb = ld(F, W_SUM2, i);
+        float4 it = ld(F, W_ITEM, i), sa = ld(F, W_SUM, i), sb = ld(F, W_SUM2, i);
         uint32_t px = fu(it.x), py = fu(it.y), sample = fu(it.z), s_end = fu(it.w);
         uint32_t j = fu(it2.x), pslot = fu(it2.y);
         float s0 = sa.x, s1 = sa.y, s2 = sa.z, c0 = sa.w, c1 = sb.x, c2 = sb.y;
@@ -165,36 +203,44 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene S, const DevPar
                 }
                 sample++;
                 if (sample < s_end) {
-                    begin_sample(p, P, px, py, sample);
+                    begin_sample(p, BATCH ? B.jobs[job].P : P0, px, py, sample);
                     a = A_TRACE;
                     break;
                 }
-                W.partials[(size_t)j * W.n_slots + pslot] = make_float4(s0 - c0, s1 - c1, s2 - c2, 0.0f);
+                float4 v = make_float4(s0 - c0, s1 - c1, s2 - c2, 0.0f);
+                if (BATCH) {
+                    const DevJob &J = B.jobs[job];
+                    B.partials[J.partial_off + (size_t)j * J.n_slots + pslot] = v;
+                } else {
+                    W.partials[(size_t)j * W.n_slots + pslot] = v;
+                }
                 flags &= ~F_ACTIVE;
             }
-            uint32_t item = next_item(W);
-            if (item >= W.n_items) {
+            const uint32_t n_items = BATCH ? B.n_items : W.n_items;
+            uint32_t item = ticket(BATCH ? B.counter : W.counter);
+            // The cancel word is read when an item number crosses a multiple of 4096.
+            if ((item & 4095u) == 0u && *(BATCH ? B.cancel : W.cancel)) atomicMax(BATCH ? B.counter : W.counter, n_items);
+            if (item >= n_items) {
                 flags |= F_DEAD;
                 break;
             }
-            j = item / W.n_slots;
-            pslot = item - j * W.n_slots;
-            uint32_t tile = pslot >> 5, in = pslot & 31u;
-            uint32_t rx = (tile % W.tiles_x) * 8u + (in & 7u);
-            uint32_t ry = (tile / W.tiles_x) * 4u + (in >> 3);
-            if (rx < W.w && ry < W.h) {
-                px = W.x0 + rx;
-                py = W.y0 + ry;
-                sample = W.sample_start + j * W.sub;
-                s_end = min(sample + W.sub, W.sample_start + W.spp);
+            ItemRef r = decode_item<BATCH>(W, B, item);
+            job = r.job;
+            j = r.j;
+            pslot = r.pslot;
+            if (r.valid) {
+                px = r.px;
+                py = r.py;
+                sample = r.sample;
+                s_end = r.s_end;
                 s0 = s1 = s2 = c0 = c1 = c2 = 0.0f;
-                begin_sample(p, P, px, py, sample);
+                begin_sample(p, BATCH ? B.jobs[job].P : P0, px, py, sample);
                 flags |= F_ACTIVE;
                 a = A_TRACE;
             }
         }
         st(F, W_ITEM, i, u4(px, py, sample, s_end));
-        st(F, W_ITEM2, i, u4(j, pslot, 0u, 0u));
+        st(F, W_ITEM2, i, u4(j, pslot, job, 0u));
         st(F, W_SUM, i, make_float4(s0, s1, s2, c0));
         st(F, W_SUM2, i, make_float4(c1, c2, 0.0f, 0.0f));
     }
@@ -207,6 +253,18 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene S, const DevPar
     }
 }
 
+// The end of an iteration: the next iteration's parity; in a graph, whether to run another one
+// (the loop stops after an iteration that had no ray to trace).
+__global__ void k_wf_advance(const WfState F) {
+    uint32_t t = F.ctr[8];
+    F.ctr[8] = t + 1u;
+}
+__global__ void k_wf_advance_graph(const WfState F, cudaGraphConditionalHandle loop) {
+    uint32_t t = F.ctr[8];
+    cudaGraphSetConditional(loop, F.ctr[4 * (t & 1u)] != 0u ? 1u : 0u);
+    F.ctr[8] = t + 1u;
+}
+
 #ifndef LW_WF_TRACE_MINB
 #define LW_WF_TRACE_MINB 8
 #endif
@@ -215,9 +273,10 @@ __global__ void __launch_bounds__(128) k_wf_shade(const DevScene S, const DevPar
 // has run dry, a ray still on its way after `tail` more rounds saves its traversal state and goes
 // to the next iteration's queue, so an iteration does not wait for its single longest ray.
 __global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevScene S, const DevParams P, const WfState F,
-                                                                      uint32_t parity, uint32_t budget, uint32_t tail) {
+                                                                      uint32_t budget, uint32_t tail) {
     const unsigned FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t parity = *(volatile uint32_t *)&F.ctr[8] & 1u;
     const uint32_t count = *(volatile uint32_t *)&F.ctr[4 * parity];
     uint32_t *fetch = &F.ctr[4 * parity + 1];
     TraceState ts;
@@ -297,13 +356,32 @@ LaunchShape wf_trace_shape(int device) {
     return LaunchShape{sms * per_sm, 128};
 }
 
-cudaError_t launch_wf_iteration(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F,
-                                LaunchShape trace_shape, uint32_t parity, uint32_t budget, uint32_t tail,
-                                cudaStream_t st) {
-    k_wf_shade<<<(F.n + 127) / 128, 128, 0, st>>>(S, P, W, F, parity);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    k_wf_trace<<<trace_shape.blocks, trace_shape.threads, 0, st>>>(S, P, F, parity, budget, tail);
+cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, cudaStream_t st) {
+    BatchDesc none{};
+    k_wf_shade<false><<<(F.n + 127) / 128, 128, 0, st>>>(S, P, W, none, F);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const BatchDesc &B, const WfState &F,
+                                  cudaStream_t st) {
+    WorkDesc none{};
+    k_wf_shade<true><<<(F.n + 127) / 128, 128, 0, st>>>(S, P0, none, B, F);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState &F, LaunchShape trace_shape,
+                            uint32_t budget, uint32_t tail, cudaStream_t st) {
+    k_wf_trace<<<trace_shape.blocks, trace_shape.threads, 0, st>>>(S, P, F, budget, tail);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wf_advance(const WfState &F, cudaStream_t st) {
+    k_wf_advance<<<1, 1, 0, st>>>(F);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_wf_advance_graph(const WfState &F, cudaGraphConditionalHandle loop, cudaStream_t st) {
+    k_wf_advance_graph<<<1, 1, 0, st>>>(F, loop);
     return cudaGetLastError();
 }
 

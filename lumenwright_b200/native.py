@@ -58,7 +58,9 @@ class SceneDesc(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("kernel_ms", C.c_double), ("upload_ms", C.c_double), ("launches", C.c_uint32),
-                ("blocks", C.c_uint32), ("threads", C.c_uint32), ("samples", C.c_uint64)]
+                ("blocks", C.c_uint32), ("threads", C.c_uint32), ("samples", C.c_uint64),
+                ("trace_ms", C.c_double), ("shade_ms", C.c_double), ("trace_launches", C.c_uint32),
+                ("shade_launches", C.c_uint32)]
 
 
 class Tuning(C.Structure):

@@ -49,8 +49,33 @@ def test_autotuner_picks_a_tuning(ctx, tmp_path):
     ctx.upload_hq_scene(hq)
     tuner = BT.Autotuner(ctx, cache_dir=str(tmp_path), trial_fraction=1.0)
     best, entry = tuner.tune(jobs)
-    assert best["threads"] in (64, 128, 256) and len(entry["trials"]) == 18
+    assert best["engine"] in (0, 1) and len(entry["trials"]) == len(BT.Autotuner.candidates())
     again, _ = tuner.tune(jobs)  # from the cache
     now = ctx.get_tuning()
     assert again == best and {k: now[k] for k in best} == best
-    ctx.set_tuning(128, 0, 0)
+    ctx.set_tuning(threads=128, budget=0, sub=0, engine=0, paths=0)
+
+
+def test_batch_engines_give_the_same_images(ctx):
+    # The batched wavefront (one graph whose loop node runs the shade/trace iterations on the
+    # device) and the batched megakernel take the same items: equal images, bit for bit.
+    from lumenwright_b200.native import ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT
+    hq, jobs = BT.c3_jobs(ctx, small_cameras())
+    ctx.upload_hq_scene(hq)
+    ctx.set_tuning(engine=ENGINE_MEGAKERNEL)
+    outs = ctx.batch_prepare(jobs)
+    ctx.batch_run()
+    ctx.batch_read()
+    want = [o.copy() for o in outs]
+    ctx.set_tuning(engine=ENGINE_WAVEFRONT)
+    got = ctx.batch_prepare(jobs)
+    ctx.batch_run()
+    ctx.batch_read()
+    for a, b in zip(got, want):
+        assert np.array_equal(a, b)
+    # replayed again: the loop starts over from the cleared slots
+    first = [o.copy() for o in got]
+    ctx.batch_run()
+    ctx.batch_read()
+    for a, b in zip(first, got):
+        assert np.array_equal(a, b)
