@@ -237,11 +237,12 @@ DevParams dev_params(const lw_params *p) {
 struct Plan {
     uint32_t sub, batch;
 };
-Plan plan(const lw_ctx *c, uint64_t n_slots, uint32_t spp) {
+Plan plan(const lw_ctx *c, uint64_t n_slots, uint32_t spp, uint32_t sub_override = 0) {
     uint64_t lanes = (uint64_t)c->shape_accum.blocks * c->shape_accum.threads;
     uint64_t total = n_slots * spp;
     uint64_t sub = total / (lanes * 16ull + 1ull);
     sub = sub < 1 ? 1 : (sub > 16 ? 16 : sub);
+    if (sub_override) sub = sub_override;
     if (c->tuning.sub) sub = c->tuning.sub;
     uint64_t max_items = c->partials_cap_bytes / sizeof(float4);
     uint64_t max_sub_per_launch = max_items / (n_slots ? n_slots : 1);
@@ -363,6 +364,13 @@ lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32
     const uint32_t w = params->frame[0], h = params->frame[1];
     WorkDesc probe = work(c, 0, 0, w, h, 0, 1, 1);
     Plan pl = plan(c, probe.n_slots, spp);
+    if (c->tuning.engine == LW_ENGINE_WAVEFRONT && c->tuning.sub == 0) {
+        // Items of a quarter of the samples per path slot at most, so the pool stays full until
+        // the last items (the slots take items one after another).
+        uint64_t samples = (uint64_t)w * h * spp;
+        uint64_t sub = samples / (4ull * wf_slots(c, samples, samples));
+        pl = plan(c, probe.n_slots, spp, (uint32_t)(sub < 1 ? 1 : (sub > 16 ? 16 : sub)));
+    }
     CK(c, ensure(c->partials, (size_t)probe.n_slots * ((pl.batch + pl.sub - 1) / pl.sub)), "allocating partial sums");
     DevScene S = dev_scene(c);
     DevParams P = dev_params(params);

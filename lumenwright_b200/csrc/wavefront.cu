@@ -156,8 +156,11 @@ LW_DI ItemRef decode_item(const WorkDesc &W, const BatchDesc &B, uint32_t item) 
 
 // One shading step per slot. The iteration's parity (which queue counters are this iteration's)
 // is the device word ctr[8], advanced by k_wf_advance after each trace.
+#ifndef LW_WF_SHADE_MINB
+#define LW_WF_SHADE_MINB 5
+#endif
 template <bool BATCH>
-__global__ void __launch_bounds__(128) k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
+__global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
                                                   const BatchDesc B, const WfState F) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t parity = *(volatile uint32_t *)&F.ctr[8] & 1u;

@@ -87,12 +87,13 @@ def test_wavefront_and_megakernel_give_the_same_image(ctx, c2, paths):
     # and the persistent megakernel take the same items in the same order of Kahan additions: the
     # images are equal bit for bit, with the automatic pool and with a small one that carries many
     # rays over.
+    # (The samples per item are set: by default each engine picks its own item size.)
     from lumenwright_b200.native import ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT
     p = c2.params
     ctx.upload_hq_scene(c2.scene)
-    ctx.set_tuning(engine=ENGINE_MEGAKERNEL)
+    ctx.set_tuning(engine=ENGINE_MEGAKERNEL, sub=3)
     want = ctx.render_hq(p, c2.sky, 12)
     ctx.set_tuning(engine=ENGINE_WAVEFRONT, paths=paths)
     got = ctx.render_hq(p, c2.sky, 12)
-    ctx.set_tuning(engine=ENGINE_WAVEFRONT, paths=0)
+    ctx.set_tuning(engine=ENGINE_WAVEFRONT, paths=0, sub=0)
     assert np.array_equal(got, want)
