@@ -113,6 +113,7 @@ typedef struct {
     /* the wavefront engine: CUDA-event time and launches of its tracing and shading kernels */
     double trace_ms, shade_ms;
     uint32_t trace_launches, shade_launches;
+    uint64_t rays;           /* rays traced (path, shadow and emitter rays) */
 } lw_stats;
 
 /* Launch tuning of the render (the autotuner's knobs).

@@ -354,6 +354,9 @@ lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const 
             if (*(volatile uint32_t *)c->wf_host == 0u) break;
         }
     }
+    uint64_t rays = 0;
+    CK(c, cudaMemcpy(&rays, F.ctr + 10, 8, cudaMemcpyDeviceToHost), "reading the ray count");
+    c->stats.rays += rays;
     return LW_OK;
 }
 

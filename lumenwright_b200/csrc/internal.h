@@ -89,7 +89,8 @@ struct WfState {
     uint32_t *queue;  // slot ids of the rays to trace this iteration
     float4 *hit0;     // per slot: t, quad, texel, s of its last ray
     float *hit1;      // per slot: tt
-    uint32_t *ctr;    // per iteration parity: queue length, trace fetch counter, -, -; [8]: iteration
+    uint32_t *ctr;    // per iteration parity: queue length, trace fetch counter, -, -; [8]: iteration;
+                      // [10..11]: rays traced (64-bit, 8-byte aligned)
     float4 *ts;       // 3 float4 per slot (word k at ts[k * n + i]): a carried-over traversal
 };
 LaunchShape wf_trace_shape(int device);

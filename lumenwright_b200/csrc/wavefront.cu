@@ -258,13 +258,17 @@ __global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevSce
 
 // The end of an iteration: the next iteration's parity; in a graph, whether to run another one
 // (the loop stops after an iteration that had no ray to trace).
+// ctr[10..11]: the rays traced so far (64-bit), for the statistics.
 __global__ void k_wf_advance(const WfState F) {
     uint32_t t = F.ctr[8];
+    *(unsigned long long *)&F.ctr[10] += F.ctr[4 * (t & 1u)];
     F.ctr[8] = t + 1u;
 }
 __global__ void k_wf_advance_graph(const WfState F, cudaGraphConditionalHandle loop) {
     uint32_t t = F.ctr[8];
-    cudaGraphSetConditional(loop, F.ctr[4 * (t & 1u)] != 0u ? 1u : 0u);
+    uint32_t n = F.ctr[4 * (t & 1u)];
+    *(unsigned long long *)&F.ctr[10] += n;
+    cudaGraphSetConditional(loop, n != 0u ? 1u : 0u);
     F.ctr[8] = t + 1u;
 }
 

@@ -60,7 +60,7 @@ class Stats(C.Structure):
     _fields_ = [("kernel_ms", C.c_double), ("upload_ms", C.c_double), ("launches", C.c_uint32),
                 ("blocks", C.c_uint32), ("threads", C.c_uint32), ("samples", C.c_uint64),
                 ("trace_ms", C.c_double), ("shade_ms", C.c_double), ("trace_launches", C.c_uint32),
-                ("shade_launches", C.c_uint32)]
+                ("shade_launches", C.c_uint32), ("rays", C.c_uint64)]
 
 
 class Tuning(C.Structure):
