@@ -261,6 +261,31 @@ lw_status lw_build_sky_cache(lw_ctx *ctx, const lw_params *params, uint32_t n, f
 lw_status lw_blend_chunky_sky(lw_ctx *ctx, const lw_params *params, const float *cache, uint64_t cache_len,
                               float *maps, const float sizes[4], float weight);
 
+/* ---- the display pass ---------------------------------------------------------------------------
+ * `post::tonemap` / `post::tonemap_mix` (crates/lumenwright/src/render/post.rs:152-217) on the
+ * device: exposure, the operator, the display gamma v^(1/2.2) and the 8-bit rounding, packed as
+ * RGBA8 with alpha 255 (byte 0 red). With mix = 0 it is tonemap(hdr, exposure, op); otherwise
+ * tonemap_mix(hdr, exposure, op, op_b, weight), the two curves mixed in display values (the
+ * reference's default for an hq frame: op = gamma, op_b = the game curve, weight = the day
+ * weight, crates/lumenwright/src/request.rs:938-947). */
+#define LW_TONEMAP_GAMMA 0u            /* Tonemap::Gamma */
+#define LW_TONEMAP_ACES 1u             /* Tonemap::Aces */
+#define LW_TONEMAP_FILMIC 2u           /* Tonemap::Filmic (Chunky's Hable preset FILMIC_WORLDS) */
+#define LW_TONEMAP_FILMIC_MID_GREY 3u  /* Tonemap::FilmicMidGrey (the game's curve) */
+typedef struct {
+    float exposure;
+    uint32_t op;
+    uint32_t mix;
+    uint32_t op_b;
+    float weight;
+} lw_tonemap;
+/* The display bytes of n linear RGB values (3n floats) into out_rgba (n words). */
+lw_status lw_tonemap_rgba(lw_ctx *ctx, const float *hdr, uint64_t n, const lw_tonemap *tm, uint32_t *out_rgba);
+/* The last render's mean radiance (the accumulator of lw_render_hq / lw_render_device) tone-mapped
+ * in the same pass that divides the sums, read back as frame[0] * frame[1] words; the linear means
+ * are read too when out_rgb is not NULL. Waits for the render. */
+lw_status lw_read_accumulator_rgba(lw_ctx *ctx, const lw_tonemap *tm, uint32_t *out_rgba, float *out_rgb);
+
 /* ---- the differentiable form ------------------------------------------------------------------
  * No counterpart in the reference: the forward/backward pair of an image loss's gradient with
  * respect to parameters theta of an hq frame on the uploaded scene. theta is

@@ -78,6 +78,7 @@ struct lw_ctx {
     uint64_t grid_len = 0, models_len = 0, quads_len = 0, atlas_len = 0, emitters_len = 0, egrid_len = 0;
     // frame
     DBuf<float> sky, gamma, out_rgb;
+    DBuf<uint32_t> out_rgba;
     uint64_t sky_len = 0;
     DBuf<Accum> acc;
     uint32_t acc_w = 0, acc_h = 0;
@@ -307,6 +308,49 @@ uint32_t wf_slots(const lw_ctx *c, uint64_t samples, uint64_t items) {
     while (n < want && n < (1u << 23)) n <<= 1;
     while (n > (1u << 10) && (n >> 1) >= items) n >>= 1;
     return n;
+}
+
+// The tone curves as post.rs computes them: Chunky's Hable preset FILMIC_WORLDS (post.rs:57-65),
+// its white scale in f32 (:74-88), and the game's curve: the preset brightened (:113-120) by the gain
+// that holds mid-grey 0.18 (:125-137).
+struct HableF {
+    float a, b, c, d, e, f, w;
+};
+float white_scale(const HableF &k) {
+    float num = k.w * (k.a * k.w + k.c * k.b) + k.d * k.e;
+    float den = k.w * (k.a * k.w + k.b) + k.d * k.f;
+    return 1.0f / (num / den - k.e / k.f);
+}
+ToneCurve tone_curve(const HableF &k) {
+    return ToneCurve{(double)k.a, (double)k.b, (double)(k.c * k.b), (double)(k.d * k.e), (double)(k.d * k.f),
+                     (double)(k.e / k.f), (double)white_scale(k)};
+}
+double mid_grey_gain(const HableF &k, double m) {
+    ToneCurve t = tone_curve(k);
+    double q = m / (double)white_scale(k) + t.ef;
+    double qa = t.a * (1.0 - q), qb = t.cb - q * t.b, qc = t.de - q * t.df;
+    double y = (-qb + std::sqrt(qb * qb - 4.0 * qa * qc)) / (2.0 * qa);
+    return y / (2.0 * m);
+}
+HableF brightened(const HableF &k, double g) {
+    HableF r = k;
+    r.a = (float)((double)k.a * g * g);
+    r.b = (float)((double)k.b * g);
+    r.w = (float)((double)k.w / g);
+    return r;
+}
+lw_status tonemap_desc(lw_ctx *c, const lw_tonemap *tm, TonemapDesc &t) {
+    if (!tm || tm->op > 3u || (tm->mix && tm->op_b > 3u)) return fail(c, LW_ERR_INVALID_ARGUMENT, "unknown tone map");
+    const HableF preset{0.15f, 0.5f, 0.1f, 0.2f, 0.02f, 0.3f, 11.2f};
+    t.exposure = tm->exposure;
+    t.op_a = tm->op;
+    t.op_b = tm->mix ? tm->op_b : tm->op;
+    t.mix = tm->mix ? 1u : 0u;
+    t.weight = tm->weight;
+    t.inv_gamma = 1.0f / 2.2f;
+    t.preset = tone_curve(preset);
+    t.game = tone_curve(brightened(preset, mid_grey_gain(preset, 0.18)));
+    return LW_OK;
 }
 
 void reset_stats(lw_ctx *c) {
@@ -544,6 +588,7 @@ void lw_ctx_destroy(lw_ctx *c) {
     for (auto e : c->wf_ev)
         if (e) cudaEventDestroy(e);
     for (auto *b : {&c->sky, &c->gamma, &c->out_rgb, &c->samples, &c->rays}) b->free_();
+    c->out_rgba.free_();
     c->acc.free_();
     c->hits.free_();
     c->xyz.free_();
@@ -1253,6 +1298,42 @@ lw_status lw_adjoint_fd(lw_ctx *c, const lw_adj_frame *plus, const lw_adj_frame 
     if (s != LW_OK) return s;
     CK(c, cudaMemcpy(diff_rgb, c->adj_img.p, n * 8, cudaMemcpyDeviceToHost), "reading the differences");
     CK(c, cudaMemcpy(mean_rgb, c->adj_img2.p, n * 8, cudaMemcpyDeviceToHost), "reading the means");
+    return LW_OK;
+}
+
+lw_status lw_tonemap_rgba(lw_ctx *c, const float *hdr, uint64_t n, const lw_tonemap *tm, uint32_t *out_rgba) {
+    if (!c || !hdr || !out_rgba) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    if (n == 0) return LW_OK;
+    if (n > 0xFFFFFFFFull / 3u) return fail(c, LW_ERR_INVALID_ARGUMENT, "%llu pixels", (unsigned long long)n);
+    cudaSetDevice(c->device);
+    TonemapDesc t;
+    lw_status s = tonemap_desc(c, tm, t);
+    if (s != LW_OK) return s;
+    CK(c, ensure(c->out_rgb, 3 * n), "allocating the pixels");
+    CK(c, ensure(c->out_rgba, n), "allocating the pixels");
+    CK(c, cudaMemcpyAsync(c->out_rgb.p, hdr, 12 * n, cudaMemcpyHostToDevice, c->stream), "uploading the pixels");
+    CK(c, launch_tonemap(c->out_rgb.p, (uint32_t)n, t, c->out_rgba.p, c->stream), "launching the tone map");
+    CK(c, cudaMemcpyAsync(out_rgba, c->out_rgba.p, 4 * n, cudaMemcpyDeviceToHost, c->stream), "reading the pixels");
+    CK(c, cudaStreamSynchronize(c->stream), "reading the pixels");
+    return LW_OK;
+}
+
+lw_status lw_read_accumulator_rgba(lw_ctx *c, const lw_tonemap *tm, uint32_t *out_rgba, float *out_rgb) {
+    if (!c || !out_rgba) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    cudaSetDevice(c->device);
+    TonemapDesc t;
+    lw_status s = tonemap_desc(c, tm, t);
+    if (s != LW_OK) return s;
+    size_t n = (size_t)c->acc_w * c->acc_h;
+    if (n == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "no accumulator");
+    CK(c, ensure(c->out_rgba, n), "allocating the pixels");
+    if (out_rgb) CK(c, ensure(c->out_rgb, 3 * n), "allocating the output");
+    CK(c, launch_finalize_tonemap(c->acc.p, (uint32_t)n, t, c->out_rgba.p, out_rgb ? c->out_rgb.p : nullptr, c->stream),
+       "launching the display pass");
+    CK(c, cudaMemcpyAsync(out_rgba, c->out_rgba.p, 4 * n, cudaMemcpyDeviceToHost, c->stream), "reading the pixels");
+    if (out_rgb)
+        CK(c, cudaMemcpyAsync(out_rgb, c->out_rgb.p, 12 * n, cudaMemcpyDeviceToHost, c->stream), "reading the image");
+    CK(c, cudaStreamSynchronize(c->stream), "reading the pixels");
     return LW_OK;
 }
 

@@ -102,6 +102,21 @@ cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState
 cudaError_t launch_wf_advance(const WfState &F, cudaStream_t st);
 cudaError_t launch_wf_advance_graph(const WfState &F, cudaGraphConditionalHandle loop, cudaStream_t st);
 
+// post.cu: the display pass (tone mapping to RGBA8).
+struct ToneCurve {  // a Hable curve as HableCurve::h reads it: f32 products widened, and 1 / h(W)
+    double a, b, cb, de, df, ef, white;
+};
+struct TonemapDesc {
+    float exposure;
+    uint32_t op_a, op_b, mix;  // operators (0 gamma, 1 ACES, 2 Hable preset, 3 game curve); mix: tonemap_mix
+    float weight;              // the mix weight of op_a
+    float inv_gamma;           // 1 / 2.2 in f32
+    ToneCurve preset, game;
+};
+cudaError_t launch_finalize_tonemap(const Accum *acc, uint32_t n, const TonemapDesc &t, uint32_t *rgba, float *hdr,
+                                    cudaStream_t st);
+cudaError_t launch_tonemap(const float *hdr, uint32_t n, const TonemapDesc &t, uint32_t *rgba, cudaStream_t st);
+
 // adjoint.cu: the differentiable form.
 #define LW_ADJ_EMITTER_GROUPS 32
 struct AdjFrame {

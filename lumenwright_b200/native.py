@@ -30,8 +30,11 @@ EXPORTS = (
     "lw_read_accumulator", "lw_render_samples", "lw_trace_rays", "lw_voxel_lookup", "lw_build_sky_cache",
     "lw_blend_chunky_sky", "lw_render_hq_reference_port", "lw_render_accumulate_noalloc", "lw_batch_prepare",
     "lw_batch_run", "lw_batch_read", "lw_render_batch", "lw_adjoint_forward", "lw_adjoint_backward", "lw_adjoint_fd",
-    "lw_gamma_table",
+    "lw_gamma_table", "lw_tonemap_rgba", "lw_read_accumulator_rgba",
 )
+
+# lw_tonemap operators (post.rs `Tonemap`)
+TONEMAP_GAMMA, TONEMAP_ACES, TONEMAP_FILMIC, TONEMAP_FILMIC_MID_GREY = 0, 1, 2, 3
 
 EMITTER_GROUPS = 32  # LW_EMITTER_GROUPS
 
@@ -83,6 +86,12 @@ class AdjFrame(C.Structure):
     _fields_ = [("params", C.c_void_p), ("sky", C.c_void_p), ("sky_len", C.c_uint64), ("albedo", C.c_void_p),
                 ("n_params", C.c_uint32), ("texel_param", C.c_void_p), ("texel_param_len", C.c_uint64),
                 ("emitter_scale", C.c_void_p)]
+
+
+class ToneMap(C.Structure):
+    """`lw_tonemap`."""
+    _fields_ = [("exposure", C.c_float), ("op", C.c_uint32), ("mix", C.c_uint32), ("op_b", C.c_uint32),
+                ("weight", C.c_float)]
 
 
 class Gradient(C.Structure):
@@ -145,6 +154,8 @@ def load(path: str = LIB_PATH):
     L.lw_adjoint_backward.argtypes = [P, C.POINTER(AdjFrame), C.c_uint32, P, C.POINTER(Gradient)]
     L.lw_adjoint_fd.argtypes = [P, C.POINTER(AdjFrame), C.POINTER(AdjFrame), C.POINTER(AdjFrame), C.c_uint32, P, P]
     L.lw_gamma_table.argtypes = [P]
+    L.lw_tonemap_rgba.argtypes = [P, P, C.c_uint64, C.POINTER(ToneMap), P]
+    L.lw_read_accumulator_rgba.argtypes = [P, C.POINTER(ToneMap), P, P]
     for name in EXPORTS:
         if name not in ("lw_ctx_destroy", "lw_last_error", "lw_stream", "lw_cancel"):
             getattr(L, name).restype = C.c_int
@@ -327,6 +338,25 @@ class Context:
 
     def batch_read(self):
         self._check(self.L.lw_batch_read(self.h))
+
+    def tonemap_rgba(self, hdr, exposure=1.0, op=TONEMAP_GAMMA, mix=0, op_b=TONEMAP_GAMMA, weight=1.0):
+        """post::tonemap / tonemap_mix on the device: (n, 3) linear values to n RGBA8 words."""
+        hdr = np.ascontiguousarray(hdr, np.float32).reshape(-1, 3)
+        out = np.zeros(hdr.shape[0], np.uint32)
+        tm = ToneMap(exposure, op, mix, op_b, weight)
+        self._check(self.L.lw_tonemap_rgba(self.h, hdr.ctypes.data, hdr.shape[0], C.byref(tm), out.ctypes.data))
+        return out
+
+    def read_accumulator_rgba(self, w, h, exposure=1.0, op=TONEMAP_GAMMA, mix=0, op_b=TONEMAP_GAMMA, weight=1.0,
+                              with_hdr=False):
+        """The last render's image as RGBA8 words (h, w), tone-mapped on the device in the pass that
+        divides the sums; with ``with_hdr`` also the linear means (h, w, 3)."""
+        out = np.zeros((h, w), np.uint32)
+        hdr = np.zeros((h, w, 3), np.float32) if with_hdr else None
+        tm = ToneMap(exposure, op, mix, op_b, weight)
+        self._check(self.L.lw_read_accumulator_rgba(self.h, C.byref(tm), out.ctypes.data,
+                                                    hdr.ctypes.data if with_hdr else None))
+        return (out, hdr) if with_hdr else out
 
     def read_accumulator(self, w, h):
         out = np.zeros((h, w, 3), np.float32)

@@ -163,6 +163,14 @@ void lwo32_count_work(const lwo_scene *s, uint32_t x0, uint32_t y0, uint32_t w, 
 uint64_t lwo_bounds_errors(void);
 void lwo_reset_bounds_errors(void);
 
+/* ---- the display pass (post.c) ------------------------------------------------------- */
+/* post::tonemap (mix = 0) or post::tonemap_mix, n pixels of 3 floats to RGBA8 words. */
+void lwo_tonemap(const float *hdr, uint64_t n, float exposure, uint32_t op, uint32_t mix, uint32_t op_b, float weight,
+                 uint32_t *out);
+void lwo_game_tone_curve(float out[7]);
+double lwo_mid_grey_gain(void);
+double lwo_game_before_gamma(double x);
+
 /* ---- FP64 build ---------------------------------------------------------------------- */
 void lwo64_render_sample(const lwo_scene *s, const lwo_camera64 *cam, uint32_t px, uint32_t py,
                          uint32_t sample, double out[3]);

@@ -132,6 +132,12 @@ def _declare(L):
     L.lwo_bounds_errors.restype = C.c_uint64
     L.lwo64_render_sample.argtypes = [sp, P(Camera64), C.c_uint32, C.c_uint32, C.c_uint32, D3]
     L.lwo64_render_mean.argtypes = [sp, P(Camera64)] + [C.c_uint32] * 5 + [C.c_void_p, C.c_int]
+    L.lwo_tonemap.argtypes = [C.c_void_p, C.c_uint64, C.c_float, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
+                              C.c_void_p]
+    L.lwo_game_tone_curve.argtypes = [C.c_void_p]
+    L.lwo_mid_grey_gain.restype = C.c_double
+    L.lwo_game_before_gamma.restype = C.c_double
+    L.lwo_game_before_gamma.argtypes = [C.c_double]
     L.lwo64_render_mean_theta.argtypes = [sp, P(Camera64), P(Theta)] + [C.c_uint32] * 5 + [C.c_void_p, C.c_int]
     L.lwo64_render_fd_theta.argtypes = [sp, P(Camera64), P(Theta), P(Theta)] + [C.c_uint32] * 5 + \
         [C.c_void_p, C.c_void_p, C.c_int]
@@ -284,6 +290,20 @@ class OracleScene:
         c = Counters()
         lib().lwo32_count_work(self.ref, x0, y0, w, h, spp, C.byref(c))
         return c.as_dict()
+
+
+def tonemap(hdr, exposure=1.0, op=0, mix=0, op_b=0, weight=1.0):
+    """post::tonemap / tonemap_mix: (n, 3) linear values to n RGBA8 words (uint32)."""
+    hdr = np.ascontiguousarray(hdr, np.float32).reshape(-1, 3)
+    out = np.zeros(hdr.shape[0], np.uint32)
+    lib().lwo_tonemap(hdr.ctypes.data, hdr.shape[0], exposure, op, mix, op_b, weight, out.ctypes.data)
+    return out
+
+
+def game_tone_curve():
+    out = np.zeros(7, np.float32)
+    lib().lwo_game_tone_curve(out.ctypes.data)
+    return out
 
 
 def pcg_hash(v):
