@@ -76,6 +76,12 @@ LW_COLD V3 map_lookup(const DevScene &S, uint32_t base, float w, float h, V3 d) 
     return top * (1.0f - ty) + bottom * ty;
 }
 
+// sky_lens (lens = true) or sky_light, with one inlined copy of each lookup.
+LW_DI V3 sky_of(const DevScene &S, const DevParams &P, V3 d, bool lens) {
+    if (P.sky_map.x < 1.0f) return sky_radiance(S, P, d);
+    uint32_t base = lens ? 0u : to_u32(P.sky_map.x * P.sky_map.y) * 3u;
+    return map_lookup(S, base, lens ? P.sky_map.x : P.sky_map.z, lens ? P.sky_map.y : P.sky_map.w, d);
+}
 LW_DI V3 sky_lens(const DevScene &S, const DevParams &P, V3 d) {  // :225-231
     if (P.sky_map.x < 1.0f) return sky_radiance(S, P, d);
     return map_lookup(S, 0u, P.sky_map.x, P.sky_map.y, d);

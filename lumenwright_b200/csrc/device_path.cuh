@@ -66,46 +66,54 @@ LW_DI Act on_extend(Path &p, const DevScene &S, const DevParams &P, Hit h) {
         }
     }
     const V3 sigma = f4v(P.water_color);
+    // Water (the plane outside the grid columns, or a water surface) refracts or reflects the ray;
+    // both cases meet at one call of water_interface.
+    V3 wpos, wn;
+    bool wfront, water = false;
     float tp;
+    uint32_t flags = 0u;
+    V3 pos = v3(0.0f, 0.0f, 0.0f), albedo = pos, n = pos;
+    float alpha = 0.0f, qemit = 0.0f;
     if (water_plane(P, p.o, p.d, tp) && (!found || tp < h.t)) {
         if (p.in_water) p.beta = vmul(p.beta, transmittance(sigma, tp));
-        bool front = p.d.y < 0.0f;
-        V3 n = v3(0.0f, front ? 1.0f : -1.0f, 0.0f);
-        V3 nd, no;
-        p.in_water = water_interface(P, p.o + p.d * tp, p.d, n, front, p.in_water, eps, p.rng, nd, no);
-        p.d = nd;
-        p.o = no;
-        p.specular = true;
-        p.tmin = 0.0f;
-        return A_CONTINUE;
-    }
-    if (!found) {
-        if (!p.in_water && !under_water_plane(P, p.o, p.d)) {
-            if (p.bounces == 0) p.radiance = p.radiance + vmul(p.beta, sky_lens(S, P, p.d));
-            else p.radiance = p.radiance + vmul(p.beta, sky_light(S, P, p.d));
-            if (p.specular && p.bounces == 0) p.radiance = p.radiance + vmul(p.beta, sun_texture(S, P, p.d));
+        wfront = p.d.y < 0.0f;
+        wn = v3(0.0f, wfront ? 1.0f : -1.0f, 0.0f);
+        wpos = p.o + p.d * tp;
+        water = true;
+    } else {
+        if (!found) {
+            if (!p.in_water && !under_water_plane(P, p.o, p.d)) {
+                p.radiance = p.radiance + vmul(p.beta, sky_of(S, P, p.d, p.bounces == 0));
+                if (p.specular && p.bounces == 0) p.radiance = p.radiance + vmul(p.beta, sun_texture(S, P, p.d));
+            }
+            return A_END;
         }
-        return A_END;
+        if (p.in_water) p.beta = vmul(p.beta, transmittance(sigma, h.t));
+        const DevQuad *q = S.quads + h.quad;
+        float4 qn = ldg(&q->n_nn);
+        flags = __float_as_uint(ldg(&q->p0_flags).w);
+        uint32_t tint = __float_as_uint(ldg(&q->eu_tint).w);
+        qemit = ldg(&q->ev_em).w;
+        pos = p.o + p.d * h.t;
+        alpha = __fdiv_rn((float)(h.texel >> 24), 255.0f);
+        albedo = vmul(linear_rgb(S.gamma, h.texel), linear_rgb(S.gamma, tint));
+        // shading_normal (integrator.rs:308-315): normal() = ev x eu = -(eu x ev), exactly.
+        n = normalize(-f4v(qn));
+        bool front = true;
+        if (!(dot(n, p.d) < 0.0f)) {
+            n = -n;
+            front = false;
+        }
+        if (flags & FLAG_WATER) {
+            wpos = pos;
+            wn = n;
+            wfront = front;
+            water = true;
+        }
     }
-    if (p.in_water) p.beta = vmul(p.beta, transmittance(sigma, h.t));
-    const DevQuad *q = S.quads + h.quad;
-    float4 qn = ldg(&q->n_nn);
-    uint32_t flags = __float_as_uint(ldg(&q->p0_flags).w);
-    uint32_t tint = __float_as_uint(ldg(&q->eu_tint).w);
-    float qemit = ldg(&q->ev_em).w;
-    V3 pos = p.o + p.d * h.t;
-    float alpha = __fdiv_rn((float)(h.texel >> 24), 255.0f);
-    V3 albedo = vmul(linear_rgb(S.gamma, h.texel), linear_rgb(S.gamma, tint));
-    // shading_normal (integrator.rs:308-315): normal() = ev x eu = -(eu x ev), exactly.
-    V3 n = normalize(-f4v(qn));
-    bool front = true;
-    if (!(dot(n, p.d) < 0.0f)) {
-        n = -n;
-        front = false;
-    }
-    if (flags & FLAG_WATER) {
+    if (water) {
         V3 nd, no;
-        p.in_water = water_interface(P, pos, p.d, n, front, p.in_water, eps, p.rng, nd, no);
+        p.in_water = water_interface(P, wpos, p.d, wn, wfront, p.in_water, eps, p.rng, nd, no);
         p.d = nd;
         p.o = no;
         p.specular = true;

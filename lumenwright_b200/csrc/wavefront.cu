@@ -206,8 +206,7 @@ __global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevSce
                 }
                 sample++;
                 if (sample < s_end) {
-                    begin_sample(p, BATCH ? B.jobs[job].P : P0, px, py, sample);
-                    a = A_TRACE;
+                    a = A_TRACE;  // the item's next sample
                     break;
                 }
                 float4 v = make_float4(s0 - c0, s1 - c1, s2 - c2, 0.0f);
@@ -237,11 +236,11 @@ __global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevSce
                 sample = r.sample;
                 s_end = r.s_end;
                 s0 = s1 = s2 = c0 = c1 = c2 = 0.0f;
-                begin_sample(p, BATCH ? B.jobs[job].P : P0, px, py, sample);
                 flags |= F_ACTIVE;
                 a = A_TRACE;
             }
         }
+        if (a == A_TRACE) begin_sample(p, BATCH ? B.jobs[job].P : P0, px, py, sample);  // one call site
         st(F, W_ITEM, i, u4(px, py, sample, s_end));
         st(F, W_ITEM2, i, u4(j, pslot, job, 0u));
         st(F, W_SUM, i, make_float4(s0, s1, s2, c0));
