@@ -167,6 +167,51 @@ lw_status lw_elapsed_ms(lw_ctx *ctx, uint32_t from, uint32_t to, double *ms);
  * stays resident across renders until the next upload. */
 lw_status lw_scene_upload(lw_ctx *ctx, const lw_scene_desc *scene);
 
+/* ---- the grid build on the device -----------------------------------------------------------
+ * `voxel::build_hq` (crates/lumenwright/src/scene/voxel.rs:111-491, with `emitter_list`, :542-607)
+ * for a block volume, producing the same buffers word for word as the host build, resident as the
+ * context's scene (as after lw_scene_upload). Two calls around the caller's model generation:
+ *   1. lw_scene_build_keys: the volume's distinct model-instance keys (a block state `s` gives
+ *      key s << 8, a fluid state s << 8 | its face mask, `Scene::fluid_face_mask`,
+ *      crates/lumenwright/src/scene/mod.rs:586-609; an invisible state none) in the order the
+ *      build interns them (bricks in brick order, voxels in (y, z, x) order inside a brick);
+ *   2. lw_scene_build_grid, with the caller's models and quads for those keys (models[0] air,
+ *      models[i] the instance of keys[i - 1], quads as the build lays them out, model_emits[i] 1 for
+ *      an emitting instance) and the atlas: instance ids, buried / uniform / stored bricks, the
+ *      grid, the emitters and the emitter grid, then the B200 re-layout. */
+#define LW_STATE_OCCLUDES 1u
+#define LW_STATE_INVISIBLE 2u
+#define LW_STATE_FLUID 4u
+typedef struct {
+    const uint16_t *blocks;     /* voxel states, index (y * size[2] + z) * size[0] + x */
+    uint32_t size[3];           /* x, y, z in voxels, multiples of 16 */
+    const uint8_t *state_flags; /* per state: LW_STATE_* bits */
+    uint32_t n_states;          /* at most 65536 */
+} lw_world_desc;
+typedef struct {
+    const lw_model *models;
+    uint64_t models_len;
+    const lw_quad *quads;
+    uint64_t quads_len;
+    const uint8_t *model_emits;
+    const uint32_t *atlas;
+    uint64_t atlas_len;
+    uint32_t atlas_size[2];
+} lw_instances_desc;
+typedef struct {
+    uint32_t dims[3];      /* the grid in bricks */
+    uint32_t offsets[5];   /* top, bricks, ov_top, ov_cells, ov_quads */
+    uint64_t grid_len, emitter_grid_len;
+    uint32_t bricks, uniform_bricks, buried_bricks, emitters;
+    double keys_ms, grid_ms; /* wall time of the two calls */
+} lw_build_info;
+lw_status lw_scene_build_keys(lw_ctx *ctx, const lw_world_desc *world, uint32_t *keys, uint32_t cap, uint32_t *n_keys);
+lw_status lw_scene_build_grid(lw_ctx *ctx, const lw_world_desc *world, const lw_instances_desc *inst, lw_build_info *info);
+/* Reads the context's scene back: the grid, the emitters and the emitter grid (each skipped when
+ * NULL; each capacity in elements must hold the scene's length). */
+lw_status lw_scene_read(lw_ctx *ctx, uint32_t *grid, uint64_t grid_cap, lw_emitter *emitters, uint64_t emitters_cap,
+                        uint32_t *emitter_grid, uint64_t emitter_grid_cap);
+
 /* ---- rendering -----------------------------------------------------------------------------
  * `Backend::render_hq` (crates/lumenwright/src/render/mod.rs:98-102) on the uploaded scene:
  * `params` is the frame's `Params`, `sky` the frame's sky buffer (`HqFrame.sky`), `spp` the

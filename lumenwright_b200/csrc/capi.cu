@@ -1,6 +1,7 @@
 // The C ABI (include/lumenwright_b200.h): contexts, scene upload and validation, the render
 // loop that replaces CudaBackend::render_hq (crates/lumenwright/src/render/cuda.rs:77-184), and
 // the parity entry points.
+#include <algorithm>
 #include <atomic>
 #include <chrono>
 #include <cmath>
@@ -127,6 +128,13 @@ struct lw_ctx {
     WfBufs wf, bwf;  // the single-frame renders' pool; the batch graph's own (its pointers are baked in)
     uint32_t *wf_host = nullptr;  // pinned word the iteration count is read into
     cudaEvent_t wf_ev[48] = {};   // per iteration of a 16-iteration window: before shade, between, after trace
+    // the grid build on the device
+    DBuf<uint16_t> bv_blocks, bv_ids;
+    DBuf<uint8_t> bv_flags, bv_emits;
+    DBuf<uint32_t> bv_keys, bv_first, bv_key_id, bv_slot, bv_emit_off;
+    DBuf<uint4> bv_cls, bv_sites;
+    std::vector<uint32_t> bv_order;  // the keys of the last lw_scene_build_keys, in interning order
+    uint32_t bv_size[3] = {}, bv_states = 0;
     // the differentiable form: per frame slot (0 and 1: the frames, 2: the nominal frame)
     DBuf<float> adj_albedo[3], adj_sky[3], adj_emit[3];
     DBuf<int32_t> adj_tparam[3];
@@ -352,6 +360,8 @@ lw_status tonemap_desc(lw_ctx *c, const lw_tonemap *tm, TonemapDesc &t) {
     t.game = tone_curve(brightened(preset, mid_grey_gain(preset, 0.18)));
     return LW_OK;
 }
+
+lw_status install_scene(lw_ctx *c, const lw_scene_desc *d, uint32_t n_bricks, uint32_t n_ov);
 
 void reset_stats(lw_ctx *c) {
     double up = c->stats.upload_ms;
@@ -584,6 +594,13 @@ void lw_ctx_destroy(lw_ctx *c) {
     for (auto *b : {&c->adj_img, &c->adj_img2, &c->adj_g}) b->free_();
     c->wf.free_();
     c->bwf.free_();
+    c->bv_blocks.free_();
+    c->bv_ids.free_();
+    c->bv_flags.free_();
+    c->bv_emits.free_();
+    for (auto *b : {&c->bv_keys, &c->bv_first, &c->bv_key_id, &c->bv_slot, &c->bv_emit_off}) b->free_();
+    c->bv_cls.free_();
+    c->bv_sites.free_();
     if (c->wf_host) cudaFreeHost(c->wf_host);
     for (auto e : c->wf_ev)
         if (e) cudaEventDestroy(e);
@@ -726,6 +743,21 @@ lw_status lw_scene_upload(lw_ctx *c, const lw_scene_desc *d) {
         return fail(c, LW_ERR_BUFFER_LENGTH, "atlas %ux%u needs more than %llu texels", d->atlas_size[0], d->atlas_size[1], (unsigned long long)d->atlas_len);
 
     CK(c, upload(c, c->grid, d->grid, d->grid_len, 4), "uploading the grid");
+    lw_status s = install_scene(c, d, n_bricks, n_ov);
+    if (s != LW_OK) return s;
+    c->stats.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return LW_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// The scene's buffers other than the grid (already in c->grid) to the device, the B200 re-layout,
+// and the context's scene description.
+lw_status install_scene(lw_ctx *c, const lw_scene_desc *d, uint32_t n_bricks, uint32_t n_ov) {
+    const uint64_t nb = (uint64_t)d->dims[0] * d->dims[1] * d->dims[2];
+    const uint32_t *o = d->offsets;
     CK(c, upload(c, c->models, d->models, d->models_len, 16), "uploading the models");
     CK(c, upload(c, c->atlas, d->atlas, d->atlas_len, 4), "uploading the atlas");
     CK(c, upload(c, c->emitters, d->emitters, d->emitters_len, 32), "uploading the emitters");
@@ -758,9 +790,12 @@ lw_status lw_scene_upload(lw_ctx *c, const lw_scene_desc *d) {
     c->emitters_len = d->emitters_len;
     c->egrid_len = d->emitter_grid_len;
     c->has_scene = true;
-    c->stats.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return LW_OK;
 }
+
+}  // namespace
+
+extern "C" {
 
 lw_status lw_sky_upload(lw_ctx *c, const float *sky, uint64_t sky_len) {
     if (!c) return LW_ERR_INVALID_ARGUMENT;
@@ -1334,6 +1369,256 @@ lw_status lw_read_accumulator_rgba(lw_ctx *c, const lw_tonemap *tm, uint32_t *ou
     if (out_rgb)
         CK(c, cudaMemcpyAsync(out_rgb, c->out_rgb.p, 12 * n, cudaMemcpyDeviceToHost, c->stream), "reading the image");
     CK(c, cudaStreamSynchronize(c->stream), "reading the pixels");
+    return LW_OK;
+}
+
+static lw_status world_check(lw_ctx *c, const lw_world_desc *w) {
+    if (!w || !w->blocks || !w->state_flags) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    for (int a = 0; a < 3; a++)
+        if (w->size[a] == 0 || w->size[a] % 16u || w->size[a] > (1u << 16))
+            return fail(c, LW_ERR_INVALID_ARGUMENT, "volume size %u (a multiple of 16, at most 65536)", w->size[a]);
+    if ((uint64_t)w->size[0] * w->size[1] * w->size[2] > 0xFFFFFFFFull)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "volume of more than 2^32 voxels");
+    if (w->n_states == 0 || w->n_states > 65536u) return fail(c, LW_ERR_INVALID_ARGUMENT, "%u states", w->n_states);
+    return LW_OK;
+}
+
+static BuildVol build_vol(lw_ctx *c, const lw_world_desc *w) {
+    return BuildVol{c->bv_blocks.p, {w->size[0], w->size[1], w->size[2]}, c->bv_flags.p, w->n_states, c->error.p};
+}
+
+lw_status lw_scene_build_keys(lw_ctx *c, const lw_world_desc *w, uint32_t *keys, uint32_t cap, uint32_t *n_keys) {
+    if (!c || !n_keys) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    lw_status s = world_check(c, w);
+    if (s != LW_OK) return s;
+    cudaSetDevice(c->device);
+    auto t0 = std::chrono::steady_clock::now();
+    const uint64_t n = (uint64_t)w->size[0] * w->size[1] * w->size[2];
+    const uint64_t nk = (uint64_t)w->n_states * 256u;
+    CK(c, upload(c, c->bv_blocks, w->blocks, n, 2), "uploading the blocks");
+    CK(c, upload(c, c->bv_flags, w->state_flags, w->n_states, 1), "uploading the state flags");
+    CK(c, ensure(c->bv_keys, n), "allocating the keys");
+    CK(c, ensure(c->bv_first, nk), "allocating the key table");
+    CK(c, cudaMemsetAsync(c->bv_first.p, 0xFF, nk * 4, c->stream), "clearing the key table");
+    CK(c, cudaMemsetAsync(c->error.p, 0, 4, c->stream), "clearing the error word");
+    CK(c, launch_keys_first(build_vol(c, w), c->bv_keys.p, c->bv_first.p, c->stream), "launching the key pass");
+    std::vector<uint32_t> first(nk);
+    uint32_t err = 0;
+    CK(c, cudaMemcpyAsync(first.data(), c->bv_first.p, nk * 4, cudaMemcpyDeviceToHost, c->stream), "reading the key table");
+    CK(c, cudaMemcpyAsync(&err, c->error.p, 4, cudaMemcpyDeviceToHost, c->stream), "reading the error word");
+    CK(c, cudaStreamSynchronize(c->stream), "finding the keys");
+    if (err) return fail(c, LW_ERR_BUFFER_LENGTH, "a voxel names a state beyond the %u states", w->n_states);
+    std::vector<std::pair<uint32_t, uint32_t>> present;  // (first position, key)
+    for (uint64_t k = 1; k < nk; k++)
+        if (first[k] != 0xFFFFFFFFu) present.push_back({first[k], (uint32_t)k});
+    std::sort(present.begin(), present.end());
+    if (present.size() > 65535u) return fail(c, LW_ERR_INVALID_ARGUMENT, "more than 65535 distinct block model instances");
+    c->bv_order.clear();
+    for (auto &p : present) c->bv_order.push_back(p.second);
+    std::memcpy(c->bv_size, w->size, sizeof c->bv_size);
+    c->bv_states = w->n_states;
+    *n_keys = (uint32_t)c->bv_order.size();
+    if (keys) {
+        if (cap < *n_keys) return fail(c, LW_ERR_BUFFER_LENGTH, "%u keys, room for %u", *n_keys, cap);
+        std::memcpy(keys, c->bv_order.data(), 4 * (size_t)*n_keys);
+    }
+    c->stats.upload_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return LW_OK;
+}
+
+lw_status lw_scene_build_grid(lw_ctx *c, const lw_world_desc *w, const lw_instances_desc *in, lw_build_info *info) {
+    if (!c || !in || !in->models || !in->quads || !in->model_emits || !in->atlas)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    lw_status s = world_check(c, w);
+    if (s != LW_OK) return s;
+    if (std::memcmp(c->bv_size, w->size, sizeof c->bv_size) != 0 || c->bv_states != w->n_states)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "call lw_scene_build_keys for this volume first");
+    if (in->models_len != c->bv_order.size() + 1)
+        return fail(c, LW_ERR_BUFFER_LENGTH, "%llu models for %zu keys (and air)", (unsigned long long)in->models_len,
+                    c->bv_order.size());
+    cudaSetDevice(c->device);
+    auto t0 = std::chrono::steady_clock::now();
+    c->has_scene = false;
+    const uint32_t dims[3] = {w->size[0] / 16u, w->size[1] / 16u, w->size[2] / 16u};
+    const uint32_t nb = dims[0] * dims[1] * dims[2];
+    const uint64_t n = (uint64_t)w->size[0] * w->size[1] * w->size[2];
+    const uint64_t nk = (uint64_t)w->n_states * 256u;
+    // instance ids per key, emitting instances
+    std::vector<uint32_t> key_id(nk, 0u);
+    for (size_t i = 0; i < c->bv_order.size(); i++) key_id[c->bv_order[i]] = (uint32_t)i + 1u;
+    CK(c, upload(c, c->bv_key_id, key_id.data(), nk, 4), "uploading the instance ids");
+    CK(c, upload(c, c->bv_emits, in->model_emits, in->models_len, 1), "uploading the emitting instances");
+    CK(c, ensure(c->bv_ids, n), "allocating the ids");
+    CK(c, ensure(c->bv_cls, nb), "allocating the brick classes");
+    BuildVol v = build_vol(c, w);
+    CK(c, launch_bricks_scan(v, c->bv_keys.p, c->bv_key_id.p, c->bv_emits.p, c->bv_ids.p, c->bv_cls.p, nb, c->stream),
+       "launching the brick pass");
+    std::vector<uint4> cls(nb);
+    CK(c, cudaMemcpyAsync(cls.data(), c->bv_cls.p, (size_t)nb * 16, cudaMemcpyDeviceToHost, c->stream), "reading the bricks");
+    CK(c, cudaStreamSynchronize(c->stream), "classifying the bricks");
+    // voxel.rs:345-392: buried (all occluding, every face neighbour inside and all occluding),
+    // uniform, or stored; emitter sites of every brick in brick order.
+    auto all_occ = [&](int64_t bx, int64_t by, int64_t bz) -> bool {
+        if (bx < 0 || by < 0 || bz < 0 || bx >= dims[0] || by >= dims[1] || bz >= dims[2]) return false;
+        return (cls[(by * dims[2] + bz) * dims[0] + bx].x & 2u) != 0u;
+    };
+    std::vector<uint32_t> top(nb, 0xFFFFFFFFu), slot(nb, 0xFFFFFFFFu), emit_off(nb, 0u);
+    uint32_t n_bricks = 0, n_uniform = 0, n_buried = 0, n_emit = 0;
+    for (uint32_t b = 0; b < nb; b++) {
+        emit_off[b] = n_emit;
+        n_emit += cls[b].w;
+        if (!(cls[b].x & 1u)) continue;
+        int64_t bx = b % dims[0], bz = (b / dims[0]) % dims[2], by = b / (dims[0] * dims[2]);
+        bool buried = (cls[b].x & 2u) && all_occ(bx, by - 1, bz) && all_occ(bx, by + 1, bz) && all_occ(bx, by, bz - 1) &&
+                      all_occ(bx, by, bz + 1) && all_occ(bx - 1, by, bz) && all_occ(bx + 1, by, bz);
+        if (buried) {
+            top[b] = UNIFORM | (cls[b].z ? cls[b].z : 1u);
+            n_buried++;
+        } else if (cls[b].x & 4u) {
+            top[b] = UNIFORM | cls[b].y;
+            n_uniform++;
+        } else {
+            top[b] = n_bricks;
+            slot[b] = n_bricks++;
+        }
+    }
+    // The grid: top | bricks | ov_top (no overlay) | a final 0 word.
+    const uint64_t grid_len = (uint64_t)nb + (uint64_t)n_bricks * 2048u + nb + 1u;
+    if (grid_len > 0xFFFFFFFFull) return fail(c, LW_ERR_INVALID_ARGUMENT, "grid of %llu words", (unsigned long long)grid_len);
+    CK(c, ensure(c->grid, grid_len), "allocating the grid");
+    CK(c, cudaMemcpyAsync(c->grid.p, top.data(), (size_t)nb * 4, cudaMemcpyHostToDevice, c->stream), "uploading the top level");
+    CK(c, cudaMemsetAsync(c->grid.p + nb + (size_t)n_bricks * 2048u, 0xFF, (size_t)nb * 4, c->stream), "writing ov_top");
+    CK(c, cudaMemsetAsync(c->grid.p + grid_len - 1, 0, 4, c->stream), "writing the last word");
+    CK(c, upload(c, c->bv_slot, slot.data(), nb, 4), "uploading the brick slots");
+    CK(c, upload(c, c->bv_emit_off, emit_off.data(), nb, 4), "uploading the emitter offsets");
+    CK(c, ensure(c->bv_sites, n_emit ? n_emit : 1), "allocating the emitter sites");
+    CK(c, launch_bricks_pack(v, c->bv_ids.p, c->bv_emits.p, c->bv_slot.p, c->bv_emit_off.p, c->grid.p + nb, c->bv_sites.p, nb,
+                             c->stream), "launching the packing pass");
+    std::vector<uint4> sites(n_emit);
+    if (n_emit)
+        CK(c, cudaMemcpyAsync(sites.data(), c->bv_sites.p, (size_t)n_emit * 16, cudaMemcpyDeviceToHost, c->stream),
+           "reading the emitter sites");
+    CK(c, cudaStreamSynchronize(c->stream), "packing the bricks");
+    // emitter_list (voxel.rs:542-607): one emitter per site; the grid of 10-block cells, each
+    // listing the emitters within one cell of it (27 neighbours), emitters in site order.
+    const int64_t CELL = 10;
+    std::vector<lw_emitter> em(n_emit ? n_emit : 1);
+    std::vector<uint32_t> eg;
+    if (n_emit == 0) {
+        std::memset(em.data(), 0, sizeof(lw_emitter));
+        eg.assign(8, 0u);
+        eg[0] = (uint32_t)CELL;
+    } else {
+        int64_t lo[3] = {INT64_MAX, INT64_MAX, INT64_MAX}, hi[3] = {INT64_MIN, INT64_MIN, INT64_MIN};
+        std::vector<int64_t> g(3 * (size_t)n_emit);
+        for (uint32_t i = 0; i < n_emit; i++) {
+            const uint32_t cc[3] = {sites[i].x, sites[i].y, sites[i].z};
+            lw_emitter &e = em[i];
+            std::memset(&e, 0, sizeof e);
+            for (int a = 0; a < 3; a++) e.pos[a] = (float)cc[a];
+            uint32_t off = in->models[sites[i].w].quad_offset;
+            std::memcpy(&e.pos[3], &off, 4);
+            e.faces[0] = in->models[sites[i].w].quad_count;
+            for (int a = 0; a < 3; a++) {
+                int64_t q = (int64_t)cc[a] / CELL;  // corners are non-negative: floor division
+                g[3 * (size_t)i + a] = q;
+                lo[a] = std::min(lo[a], q);
+                hi[a] = std::max(hi[a], q);
+            }
+        }
+        int64_t offset[3], size[3];
+        for (int a = 0; a < 3; a++) {
+            offset[a] = lo[a] - 1;
+            size[a] = hi[a] - lo[a] + 3;
+        }
+        const uint64_t ncells = (uint64_t)size[0] * size[1] * size[2];
+        std::vector<uint32_t> counts(ncells, 0u);
+        auto cell = [&](uint32_t i, int dx, int dy, int dz) -> uint64_t {
+            int64_t l0 = g[3 * (size_t)i] + dx - offset[0], l1 = g[3 * (size_t)i + 1] + dy - offset[1],
+                    l2 = g[3 * (size_t)i + 2] + dz - offset[2];
+            return (uint64_t)((l1 * size[2] + l2) * size[0] + l0);
+        };
+        for (uint32_t i = 0; i < n_emit; i++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dz = -1; dz <= 1; dz++)
+                    for (int dx = -1; dx <= 1; dx++) counts[cell(i, dx, dy, dz)]++;
+        std::vector<uint32_t> start(ncells, 0u), fill(ncells, 0u);
+        uint64_t acc = 0;
+        for (uint64_t k = 0; k < ncells; k++) {
+            start[k] = (uint32_t)acc;
+            acc += counts[k];
+        }
+        eg.assign(8 + 2 * ncells + acc, 0u);
+        eg[0] = (uint32_t)CELL;
+        for (int a = 0; a < 3; a++) {
+            eg[1 + a] = (uint32_t)size[a];
+            eg[4 + a] = (uint32_t)(int32_t)offset[a];
+        }
+        for (uint64_t k = 0; k < ncells; k++) {
+            eg[8 + 2 * k] = start[k];
+            eg[9 + 2 * k] = counts[k];
+        }
+        // per cell, emitters in site order: sites are visited in order
+        for (uint32_t i = 0; i < n_emit; i++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dz = -1; dz <= 1; dz++)
+                    for (int dx = -1; dx <= 1; dx++) {
+                        uint64_t k = cell(i, dx, dy, dz);
+                        eg[8 + 2 * ncells + start[k] + fill[k]++] = i;
+                    }
+    }
+    lw_scene_desc d{};
+    d.grid = nullptr;
+    d.grid_len = grid_len;
+    d.models = in->models;
+    d.models_len = in->models_len;
+    d.quads = in->quads;
+    d.quads_len = in->quads_len;
+    d.atlas = in->atlas;
+    d.atlas_len = in->atlas_len;
+    d.emitters = em.data();
+    d.emitters_len = em.size();
+    d.emitter_grid = eg.data();
+    d.emitter_grid_len = eg.size();
+    std::memcpy(d.dims, dims, sizeof dims);
+    const uint32_t off_ov_top = nb + n_bricks * 2048u;
+    const uint32_t offs[5] = {0u, nb, off_ov_top, off_ov_top + nb, off_ov_top + nb};
+    std::memcpy(d.offsets, offs, sizeof offs);
+    d.atlas_size[0] = in->atlas_size[0];
+    d.atlas_size[1] = in->atlas_size[1];
+    if ((uint64_t)in->atlas_size[0] * in->atlas_size[1] > in->atlas_len || !in->atlas_size[0] || !in->atlas_size[1])
+        return fail(c, LW_ERR_BUFFER_LENGTH, "atlas size");
+    for (uint64_t i = 0; i < in->models_len; i++)
+        if ((uint64_t)in->models[i].quad_offset + in->models[i].quad_count > in->quads_len)
+            return fail(c, LW_ERR_BUFFER_LENGTH, "model %llu's quads outside the quads", (unsigned long long)i);
+    s = install_scene(c, &d, n_bricks, 0u);
+    if (s != LW_OK) return s;
+    if (info) {
+        std::memcpy(info->dims, dims, sizeof dims);
+        std::memcpy(info->offsets, offs, sizeof offs);
+        info->grid_len = grid_len;
+        info->emitter_grid_len = eg.size();
+        info->bricks = n_bricks;
+        info->uniform_bricks = n_uniform;
+        info->buried_bricks = n_buried;
+        info->emitters = n_emit;
+        info->keys_ms = c->stats.upload_ms;
+        info->grid_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return LW_OK;
+}
+
+lw_status lw_scene_read(lw_ctx *c, uint32_t *grid, uint64_t grid_cap, lw_emitter *emitters, uint64_t emitters_cap,
+                        uint32_t *egrid, uint64_t egrid_cap) {
+    if (!c) return LW_ERR_INVALID_ARGUMENT;
+    if (!c->has_scene) return fail(c, LW_ERR_NO_SCENE, "no scene");
+    cudaSetDevice(c->device);
+    if ((grid && grid_cap < c->grid_len) || (emitters && emitters_cap < c->emitters_len) || (egrid && egrid_cap < c->egrid_len))
+        return fail(c, LW_ERR_BUFFER_LENGTH, "the scene holds %llu grid words, %llu emitters, %llu emitter-grid words",
+                    (unsigned long long)c->grid_len, (unsigned long long)c->emitters_len, (unsigned long long)c->egrid_len);
+    if (grid) CK(c, cudaMemcpy(grid, c->grid.p, c->grid_len * 4, cudaMemcpyDeviceToHost), "reading the grid");
+    if (emitters) CK(c, cudaMemcpy(emitters, c->emitters.p, c->emitters_len * 32, cudaMemcpyDeviceToHost), "reading the emitters");
+    if (egrid) CK(c, cudaMemcpy(egrid, c->egrid.p, c->egrid_len * 4, cudaMemcpyDeviceToHost), "reading the emitter grid");
     return LW_OK;
 }
 

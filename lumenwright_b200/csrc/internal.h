@@ -102,6 +102,20 @@ cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState
 cudaError_t launch_wf_advance(const WfState &F, cudaStream_t st);
 cudaError_t launch_wf_advance_graph(const WfState &F, cudaGraphConditionalHandle loop, cudaStream_t st);
 
+// build.cu: the hq grid build on the device.
+struct BuildVol {
+    const uint16_t *blocks;  // voxel states, (y * size_z + z) * size_x + x
+    uint32_t size[3];        // x, y, z in voxels
+    const uint8_t *flags;    // per state: 1 occludes, 2 invisible, 4 fluid
+    uint32_t n_states;
+    uint32_t *error;         // bit 0: a voxel names a state out of range
+};
+cudaError_t launch_keys_first(const BuildVol &v, uint32_t *keys, uint32_t *first, cudaStream_t st);
+cudaError_t launch_bricks_scan(const BuildVol &v, const uint32_t *keys, const uint32_t *key_id, const uint8_t *model_emits,
+                               uint16_t *ids, uint4 *cls, uint32_t nb, cudaStream_t st);
+cudaError_t launch_bricks_pack(const BuildVol &v, const uint16_t *ids, const uint8_t *model_emits, const uint32_t *slot,
+                               const uint32_t *emit_off, uint32_t *brick_words, uint4 *sites, uint32_t nb, cudaStream_t st);
+
 // post.cu: the display pass (tone mapping to RGBA8).
 struct ToneCurve {  // a Hable curve as HableCurve::h reads it: f32 products widened, and 1 / h(W)
     double a, b, cb, de, df, ef, white;

@@ -30,7 +30,8 @@ EXPORTS = (
     "lw_read_accumulator", "lw_render_samples", "lw_trace_rays", "lw_voxel_lookup", "lw_build_sky_cache",
     "lw_blend_chunky_sky", "lw_render_hq_reference_port", "lw_render_accumulate_noalloc", "lw_batch_prepare",
     "lw_batch_run", "lw_batch_read", "lw_render_batch", "lw_adjoint_forward", "lw_adjoint_backward", "lw_adjoint_fd",
-    "lw_gamma_table", "lw_tonemap_rgba", "lw_read_accumulator_rgba",
+    "lw_gamma_table", "lw_tonemap_rgba", "lw_read_accumulator_rgba", "lw_scene_build_keys", "lw_scene_build_grid",
+    "lw_scene_read",
 )
 
 # lw_tonemap operators (post.rs `Tonemap`)
@@ -86,6 +87,25 @@ class AdjFrame(C.Structure):
     _fields_ = [("params", C.c_void_p), ("sky", C.c_void_p), ("sky_len", C.c_uint64), ("albedo", C.c_void_p),
                 ("n_params", C.c_uint32), ("texel_param", C.c_void_p), ("texel_param_len", C.c_uint64),
                 ("emitter_scale", C.c_void_p)]
+
+
+class WorldDesc(C.Structure):
+    """`lw_world_desc`."""
+    _fields_ = [("blocks", C.c_void_p), ("size", C.c_uint32 * 3), ("state_flags", C.c_void_p), ("n_states", C.c_uint32)]
+
+
+class InstancesDesc(C.Structure):
+    """`lw_instances_desc`."""
+    _fields_ = [("models", C.c_void_p), ("models_len", C.c_uint64), ("quads", C.c_void_p), ("quads_len", C.c_uint64),
+                ("model_emits", C.c_void_p), ("atlas", C.c_void_p), ("atlas_len", C.c_uint64),
+                ("atlas_size", C.c_uint32 * 2)]
+
+
+class BuildInfo(C.Structure):
+    """`lw_build_info`."""
+    _fields_ = [("dims", C.c_uint32 * 3), ("offsets", C.c_uint32 * 5), ("grid_len", C.c_uint64),
+                ("emitter_grid_len", C.c_uint64), ("bricks", C.c_uint32), ("uniform_bricks", C.c_uint32),
+                ("buried_bricks", C.c_uint32), ("emitters", C.c_uint32), ("keys_ms", C.c_double), ("grid_ms", C.c_double)]
 
 
 class ToneMap(C.Structure):
@@ -155,6 +175,9 @@ def load(path: str = LIB_PATH):
     L.lw_adjoint_fd.argtypes = [P, C.POINTER(AdjFrame), C.POINTER(AdjFrame), C.POINTER(AdjFrame), C.c_uint32, P, P]
     L.lw_gamma_table.argtypes = [P]
     L.lw_tonemap_rgba.argtypes = [P, P, C.c_uint64, C.POINTER(ToneMap), P]
+    L.lw_scene_build_keys.argtypes = [P, C.POINTER(WorldDesc), P, C.c_uint32, C.POINTER(C.c_uint32)]
+    L.lw_scene_build_grid.argtypes = [P, C.POINTER(WorldDesc), C.POINTER(InstancesDesc), C.POINTER(BuildInfo)]
+    L.lw_scene_read.argtypes = [P, P, C.c_uint64, P, C.c_uint64, P, C.c_uint64]
     L.lw_read_accumulator_rgba.argtypes = [P, C.POINTER(ToneMap), P, P]
     for name in EXPORTS:
         if name not in ("lw_ctx_destroy", "lw_last_error", "lw_stream", "lw_cancel"):
@@ -445,6 +468,46 @@ class Context:
         self._check(self.L.lw_adjoint_fd(self.h, C.byref(fp), C.byref(fm), C.byref(f0), spp, diff.ctypes.data,
                                          mean.ctypes.data))
         return diff, mean
+
+    # ---- the grid build on the device -------------------------------------------------------
+    def _world(self, blocks, state_flags):
+        blocks = np.ascontiguousarray(blocks, np.uint16)
+        flags = np.ascontiguousarray(state_flags, np.uint8)
+        Y, Z, X = blocks.shape
+        return WorldDesc(blocks.ctypes.data, (C.c_uint32 * 3)(X, Y, Z), flags.ctypes.data, flags.size), (blocks, flags)
+
+    def scene_build_keys(self, blocks, state_flags):
+        """Phase 1 of the device grid build: the model-instance keys of ``blocks`` ((y, z, x) states)
+        in the order the build interns them."""
+        w, keep = self._world(blocks, state_flags)
+        n = C.c_uint32()
+        self._check(self.L.lw_scene_build_keys(self.h, C.byref(w), None, 0, C.byref(n)))
+        out = np.zeros(max(1, n.value), np.uint32)
+        self._check(self.L.lw_scene_build_keys(self.h, C.byref(w), out.ctypes.data, out.size, C.byref(n)))
+        return out[:n.value]
+
+    def scene_build_grid(self, blocks, state_flags, models, quads, model_emits, atlas, atlas_size):
+        """Phase 2: the grid, emitters and emitter grid on the device, installed as the scene."""
+        w, keep = self._world(blocks, state_flags)
+        models = np.ascontiguousarray(models, MODEL_DTYPE)
+        quads = np.ascontiguousarray(quads, QUAD_DTYPE)
+        emits = np.ascontiguousarray(model_emits, np.uint8)
+        atlas = np.ascontiguousarray(atlas, np.uint32)
+        d = InstancesDesc(models.ctypes.data, models.size, quads.ctypes.data, quads.size, emits.ctypes.data,
+                          atlas.ctypes.data, atlas.size, (C.c_uint32 * 2)(*atlas_size))
+        info = BuildInfo()
+        self._check(self.L.lw_scene_build_grid(self.h, C.byref(w), C.byref(d), C.byref(info)))
+        return info
+
+    def scene_read(self, grid_len, emitters_len, emitter_grid_len):
+        """The context's scene buffers: (grid, emitters, emitter grid)."""
+        from .layout import EMITTER_DTYPE
+        grid = np.zeros(grid_len, np.uint32)
+        em = np.zeros(emitters_len, EMITTER_DTYPE)
+        eg = np.zeros(emitter_grid_len, np.uint32)
+        self._check(self.L.lw_scene_read(self.h, grid.ctypes.data, grid.size, em.ctypes.data, em.size, eg.ctypes.data,
+                                         eg.size))
+        return grid, em, eg
 
     def voxel_lookup(self, xyz):
         xyz = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)
