@@ -348,7 +348,7 @@ def main():
     ctx.mark(0)
     launches = 0
     trace_ms = shade_ms = kernel_ms = 0.0
-    trace_launches = 0
+    trace_launches = rays = 0
     with ClockSampler(local) as clocks:
         for i in range(args.steps):
             device_step(args.warmup + i)
@@ -358,6 +358,7 @@ def main():
             trace_ms += st["trace_ms"]
             shade_ms += st["shade_ms"]
             trace_launches += st["trace_launches"]
+            rays += st["rays"]
         ctx.mark(1)
         total_ms = ctx.elapsed(0, 1)
     if dist:
@@ -399,6 +400,11 @@ def main():
         my_samples = samples_per_step * args.steps
         trace_bytes = alg["trace_bytes_per_sample"] * my_samples
         achieved = trace_bytes / (trace_ms / 1e3) / 1e9 if trace_ms > 0 else None
+        # DRAM traffic per launch: the ncu capture's bytes per traced ray times this run's rays per
+        # tracing launch.
+        with open(os.path.join(ROOT, "profiles", "k_wf_trace_traffic_c2.json")) as f:
+            per_ray = json.load(f)["dram_bytes_per_ray"]
+        traffic = per_ray * rays / max(1, trace_launches)
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -414,7 +420,9 @@ def main():
             "kernels": {"trace_ms": trace_ms, "shade_ms": shade_ms, "other_ms": kernel_ms - trace_ms - shade_ms,
                         "trace_launches": trace_launches},
             "roofline": {"bound": "hbm", "kernel": "k_wf_trace", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak if achieved else None, "traffic": None, "peak_kind": peak_kind,
+                         "frac": achieved / peak if achieved else None, "traffic": traffic, "peak_kind": peak_kind,
+                         "traffic_unit": "bytes per launch (ncu DRAM bytes per ray x rays per launch)",
+                         "rays_per_launch": rays / max(1, trace_launches),
                          "algorithmic_bytes_per_launch": trace_bytes / max(1, trace_launches),
                          "avg_launch_ms": trace_ms / max(1, trace_launches),
                          "trace_bytes_per_sample": alg["trace_bytes_per_sample"]},

@@ -296,16 +296,19 @@ lw_status wf_setup(lw_ctx *c, lw_ctx::WfBufs &b, uint32_t n, WfState &F, cudaStr
     CK(c, ensure(b.hit0, n), "allocating the hits");
     CK(c, ensure(b.ts, (size_t)3 * n), "allocating the carried traversals");
     CK(c, ensure(b.hit1, n), "allocating the hits");
-    CK(c, ensure(b.queue, n), "allocating the ray queue");
-    CK(c, ensure(b.ctr, 12), "allocating the queue counters");
+    CK(c, ensure(b.queue, (size_t)3 * n), "allocating the ray queues");
+    CK(c, ensure(b.ctr, 16), "allocating the queue counters");
     if (!c->wf_host) CK(c, cudaMallocHost((void **)&c->wf_host, 4), "allocating a pinned word");
     F = WfState{b.state.p, n, b.queue.p, b.hit0.p, b.hit1.p, b.ctr.p, b.ts.p};
     // the slots' core words (flags 0: no item yet), the counters and the iteration, the hits
     CK(c, cudaMemsetAsync(b.state.p + (size_t)4 * n, 0, (size_t)n * sizeof(float4), st), "clearing the slots");
-    CK(c, cudaMemsetAsync(b.ctr.p, 0, 12 * sizeof(uint32_t), st), "clearing the queue counters");
+    CK(c, cudaMemsetAsync(b.ctr.p, 0, 16 * sizeof(uint32_t), st), "clearing the queue counters");
     CK(c, cudaMemsetAsync(b.hit0.p, 0, (size_t)n * sizeof(float4), st), "clearing the hits");
     return LW_OK;
 }
+
+// Blocks of the shading kernel: one thread per slot.
+uint32_t wf_shade_blocks(const lw_ctx *, uint32_t n) { return (n + 127u) / 128u; }
 
 // Path slots for a render of `samples` samples in `items` work items: one per 16 samples, a power
 // of two from 2^16 to 2^23, no more than the items (or the tuning's count).
@@ -386,7 +389,7 @@ lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const 
     for (uint32_t t = 0;; t++) {
         cudaEvent_t *e = c->wf_ev + 3 * (t & 15u);
         CK(c, cudaEventRecord(e[0], c->stream), "recording an event");
-        CK(c, launch_wf_shade(S, P, W, F, c->stream), "launching the shading kernel");
+        CK(c, launch_wf_shade(S, P, W, F, wf_shade_blocks(c, n), c->stream), "launching the shading kernel");
         CK(c, cudaEventRecord(e[1], c->stream), "recording an event");
         CK(c, launch_wf_trace(S, P, F, c->shape_wf, budget, c->wf_tail, c->stream), "launching the tracing kernel");
         CK(c, cudaEventRecord(e[2], c->stream), "recording an event");
@@ -395,7 +398,7 @@ lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const 
         c->stats.trace_launches++;
         c->stats.launches += 3;
         if ((t & 15u) == 15u) {
-            CK(c, cudaMemcpyAsync(c->wf_host, F.ctr + 4 * (t & 1u), 4, cudaMemcpyDeviceToHost, c->stream),
+            CK(c, cudaMemcpyAsync(c->wf_host, F.ctr + 4 * (t % 3u), 4, cudaMemcpyDeviceToHost, c->stream),
                "reading the queue length");
             CK(c, cudaStreamSynchronize(c->stream), "running the iterations");
             for (int k = 0; k < 16; k++) {
@@ -409,7 +412,7 @@ lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const 
         }
     }
     uint64_t rays = 0;
-    CK(c, cudaMemcpy(&rays, F.ctr + 10, 8, cudaMemcpyDeviceToHost), "reading the ray count");
+    CK(c, cudaMemcpy(&rays, F.ctr + 14, 8, cudaMemcpyDeviceToHost), "reading the ray count");
     c->stats.rays += rays;
     return LW_OK;
 }
@@ -481,7 +484,7 @@ lw_status batch_graph_wavefront(lw_ctx *c, const BatchDesc &B, const DevParams &
     cudaError_t e = cudaMemsetAsync(B.counter, 0, 4, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->batch_acc.p, 0, sizeof(Accum) * pixels, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(F.state + (size_t)4 * F.n, 0, (size_t)F.n * sizeof(float4), c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(F.ctr, 0, 12 * sizeof(uint32_t), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(F.ctr, 0, 16 * sizeof(uint32_t), c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(F.hit0, 0, (size_t)F.n * sizeof(float4), c->stream);
     cudaGraphNode_t loop_node = nullptr;
     if (e == cudaSuccess) {
@@ -502,7 +505,7 @@ lw_status batch_graph_wavefront(lw_ctx *c, const BatchDesc &B, const DevParams &
             cudaGraph_t body = np.conditional.phGraph_out[0];
             e = cudaStreamBeginCaptureToGraph(c->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
             if (e == cudaSuccess) {
-                cudaError_t eb = launch_wf_shade_batch(S, P0, B, F, c->cap);
+                cudaError_t eb = launch_wf_shade_batch(S, P0, B, F, wf_shade_blocks(c, F.n), c->cap);
                 if (eb == cudaSuccess) eb = launch_wf_trace(S, P0, F, c->shape_wf, budget, c->wf_tail, c->cap);
                 if (eb == cudaSuccess) eb = launch_wf_advance_graph(F, loop, c->cap);
                 cudaGraph_t done = nullptr;

@@ -86,17 +86,18 @@ constexpr int kWfWords = 16;
 struct WfState {
     float4 *state;    // kWfWords float4 per slot, word k of slot i at state[k * n + i]
     uint32_t n;       // slots
-    uint32_t *queue;  // slot ids of the rays to trace this iteration
+    uint32_t *queue;  // 3 sets of n slot ids: the rays of iterations t % 3
     float4 *hit0;     // per slot: t, quad, texel, s of its last ray
     float *hit1;      // per slot: tt
-    uint32_t *ctr;    // per iteration parity: queue length, trace fetch counter, -, -; [8]: iteration;
-                      // [10..11]: rays traced (64-bit, 8-byte aligned)
+    uint32_t *ctr;    // per queue set s: [4s] its length, [4s + 1] the trace fetch counter; [12]: the
+                      // iteration; [14..15]: rays traced (64-bit, 8-byte aligned)
     float4 *ts;       // 3 float4 per slot (word k at ts[k * n + i]): a carried-over traversal
 };
 LaunchShape wf_trace_shape(int device);
-cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, cudaStream_t st);
+cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, uint32_t blocks,
+                            cudaStream_t st);
 cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const BatchDesc &B, const WfState &F,
-                                  cudaStream_t st);
+                                  uint32_t blocks, cudaStream_t st);
 cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState &F, LaunchShape trace_shape,
                             uint32_t budget, uint32_t tail, cudaStream_t st);
 cudaError_t launch_wf_advance(const WfState &F, cudaStream_t st);

@@ -154,22 +154,10 @@ LW_DI ItemRef decode_item(const WorkDesc &W, const BatchDesc &B, uint32_t item) 
     return r;
 }
 
-// One shading step per slot. The iteration's parity (which queue counters are this iteration's)
-// is the device word ctr[8], advanced by k_wf_advance after each trace.
-#ifndef LW_WF_SHADE_MINB
-#define LW_WF_SHADE_MINB 5
-#endif
+// One shading step of slot i; its next ray goes to queue set `cur`.
 template <bool BATCH>
-__global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
-                                                  const BatchDesc B, const WfState F) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t parity = *(volatile uint32_t *)&F.ctr[8] & 1u;
-    if (i == 0) {
-        // The queue counters of the next iteration (the trace kernel of the previous one is done).
-        F.ctr[4 * (parity ^ 1u)] = 0u;
-        F.ctr[4 * (parity ^ 1u) + 1] = 0u;
-    }
-    if (i >= F.n) return;
+LW_DI void shade_slot(uint32_t i, const DevScene &S0, const DevParams &P0, const WorkDesc &W, const BatchDesc &B,
+                      const WfState &F, uint32_t cur) {
     float4 core = ld(F, W_CORE, i);
     uint32_t flags = fu(core.w);
     if (flags & F_DEAD) return;
@@ -247,7 +235,7 @@ __global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevSce
         st(F, W_SUM2, i, make_float4(c1, c2, 0.0f, 0.0f));
     }
     if (a == A_TRACE) {
-        F.queue[ticket(&F.ctr[4 * parity])] = i;
+        F.queue[(size_t)cur * F.n + ticket(&F.ctr[4 * cur])] = i;
         store_core(F, i, p, flags);
         if (p.kind != K_EXTEND) store_nee(F, i, p);
     } else {
@@ -255,20 +243,47 @@ __global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevSce
     }
 }
 
-// The end of an iteration: the next iteration's parity; in a graph, whether to run another one
-// (the loop stops after an iteration that had no ray to trace).
-// ctr[10..11]: the rays traced so far (64-bit), for the statistics.
+// One shading step for every slot that had a ray in the previous iteration. Iteration t's rays are queue set t % 3, filled by the shading of iteration t and by
+// the rays the tracing of iteration t - 1 carried over; the shading of iteration t reads set
+// (t - 1) % 3 and clears set (t + 1) % 3 for the next iteration. The iteration is the device word
+// ctr[12], advanced by k_wf_advance after each trace.
+#ifndef LW_WF_SHADE_MINB
+#define LW_WF_SHADE_MINB 5
+#endif
+template <bool BATCH>
+__global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
+                                                  const BatchDesc B, const WfState F) {
+    const uint32_t t = *(volatile uint32_t *)&F.ctr[12];
+    const uint32_t cur = t % 3u, prev = (t + 2u) % 3u, next = (t + 1u) % 3u;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        F.ctr[4 * next] = 0u;
+        F.ctr[4 * next + 1] = 0u;
+    }
+    // While most slots have a ray, thread k shades slot k (coalesced loads of the slot words; slots
+    // without a ray return at once); once the previous iteration traced fewer than an eighth of
+    // the slots, as the pool drains, only the slots in its queue are visited.
+    const uint32_t queued = *(volatile uint32_t *)&F.ctr[4 * prev];
+    const bool dense = t == 0u || (uint64_t)queued * 8u > F.n;
+    const uint32_t n = dense ? F.n : queued;
+    const uint32_t *list = F.queue + (size_t)prev * F.n;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;  // the grid covers every slot
+    if (k < n) shade_slot<BATCH>(dense ? k : list[k], S0, P0, W, B, F, cur);
+}
+
+// The end of an iteration: the next iteration's number; in a graph, whether to run another one (the
+// loop stops after an iteration that had no ray to trace). ctr[14..15]: the rays traced so far
+// (64-bit), for the statistics.
 __global__ void k_wf_advance(const WfState F) {
-    uint32_t t = F.ctr[8];
-    *(unsigned long long *)&F.ctr[10] += F.ctr[4 * (t & 1u)];
-    F.ctr[8] = t + 1u;
+    uint32_t t = F.ctr[12];
+    *(unsigned long long *)&F.ctr[14] += F.ctr[4 * (t % 3u)];
+    F.ctr[12] = t + 1u;
 }
 __global__ void k_wf_advance_graph(const WfState F, cudaGraphConditionalHandle loop) {
-    uint32_t t = F.ctr[8];
-    uint32_t n = F.ctr[4 * (t & 1u)];
-    *(unsigned long long *)&F.ctr[10] += n;
+    uint32_t t = F.ctr[12];
+    uint32_t n = F.ctr[4 * (t % 3u)];
+    *(unsigned long long *)&F.ctr[14] += n;
     cudaGraphSetConditional(loop, n != 0u ? 1u : 0u);
-    F.ctr[8] = t + 1u;
+    F.ctr[12] = t + 1u;
 }
 
 #ifndef LW_WF_TRACE_MINB
@@ -282,9 +297,11 @@ __global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevSce
                                                                       uint32_t budget, uint32_t tail) {
     const unsigned FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t parity = *(volatile uint32_t *)&F.ctr[8] & 1u;
-    const uint32_t count = *(volatile uint32_t *)&F.ctr[4 * parity];
-    uint32_t *fetch = &F.ctr[4 * parity + 1];
+    const uint32_t t = *(volatile uint32_t *)&F.ctr[12];
+    const uint32_t cur = t % 3u, next = (t + 1u) % 3u;
+    const uint32_t count = *(volatile uint32_t *)&F.ctr[4 * cur];
+    uint32_t *fetch = &F.ctr[4 * cur + 1];
+    const uint32_t *list = F.queue + (size_t)cur * F.n;
     TraceState ts;
     V3 o = v3(0.0f, 0.0f, 0.0f), d = o;
     float tmin = 0.0f;
@@ -303,7 +320,7 @@ __global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevSce
                 if (q >= count) {
                     done = true;
                 } else {
-                    slot = F.queue[q];
+                    slot = list[q];
                     float4 a = ld(F, W_O, slot), b = ld(F, W_D, slot);
                     o = f4v(a);
                     tmin = a.w;
@@ -346,7 +363,7 @@ __global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevSce
                 F.ts[F.n + slot] = make_float4(ts.s.n1, ts.s.n2, ts.s.t, ts.inv.x);
                 F.ts[2 * (size_t)F.n + slot] = make_float4(ts.inv.y, ts.inv.z, ts.t_end, __uint_as_float(ts.it));
                 F.hit0[slot] = make_float4(0.0f, __uint_as_float(RESUME_MARK), 0.0f, 0.0f);
-                F.queue[ticket(&F.ctr[4 * (parity ^ 1u)])] = slot;
+                F.queue[(size_t)next * F.n + ticket(&F.ctr[4 * next])] = slot;
                 have = false;
                 done = true;
             }
@@ -362,16 +379,17 @@ LaunchShape wf_trace_shape(int device) {
     return LaunchShape{sms * per_sm, 128};
 }
 
-cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, cudaStream_t st) {
+cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, uint32_t blocks,
+                            cudaStream_t st) {
     BatchDesc none{};
-    k_wf_shade<false><<<(F.n + 127) / 128, 128, 0, st>>>(S, P, W, none, F);
+    k_wf_shade<false><<<blocks, 128, 0, st>>>(S, P, W, none, F);
     return cudaGetLastError();
 }
 
 cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const BatchDesc &B, const WfState &F,
-                                  cudaStream_t st) {
+                                  uint32_t blocks, cudaStream_t st) {
     WorkDesc none{};
-    k_wf_shade<true><<<(F.n + 127) / 128, 128, 0, st>>>(S, P0, none, B, F);
+    k_wf_shade<true><<<blocks, 128, 0, st>>>(S, P0, none, B, F);
     return cudaGetLastError();
 }
 
