@@ -367,7 +367,10 @@ typedef struct {
 /* The mean radiance per pixel of samples [0, spp) under theta, FP64, frame[0] * frame[1] * 3. */
 lw_status lw_adjoint_forward(lw_ctx *ctx, const lw_adj_frame *frame, uint32_t spp, double *out_rgb);
 /* The gradient of a loss whose derivative with respect to the forward image is `d_rgb`
- * (frame[0] * frame[1] * 3 doubles), over the same samples; overwrites `out`. */
+ * (frame[0] * frame[1] * 3 doubles), over the same samples; overwrites `out`. Called after
+ * lw_adjoint_forward with the same inputs (params, sky, theta, spp: compared by a digest of their
+ * bytes), it reads each sample's radiance the forward pass kept on the device (up to 4 GiB of
+ * them) instead of replaying every path a first time. */
 lw_status lw_adjoint_backward(lw_ctx *ctx, const lw_adj_frame *frame, uint32_t spp, const double *d_rgb,
                               lw_gradient *out);
 /* Paired finite differences: every sample under `plus` and under `minus` (same size, same

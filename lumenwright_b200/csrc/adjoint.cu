@@ -528,13 +528,15 @@ LW_DI bool cell_of(const DevParams &P, uint32_t spp, uint32_t chunk, Cell &c) {
 
 // The per-pixel mean radiance of samples [0, spp) with theta (non-finite samples left out of the
 // sum, every sample counted).
-__global__ void k_adj_forward(const DevScene S, const Theta T, uint32_t spp, uint32_t chunk, double *img) {
+// With `Ls`, each sample's radiance is kept there ([pixel * spp + sample]) for the backward pass.
+__global__ void k_adj_forward(const DevScene S, const Theta T, uint32_t spp, uint32_t chunk, double *img, DV *Ls) {
     Cell c;
     if (!cell_of(T.F.P, spp, chunk, c)) return;
     const AdjGrad none{};
     double a0 = 0, a1 = 0, a2 = 0;
     for (uint32_t s = c.s0; s < c.s1; s++) {
         DV r = path<M_FWD>(S, T, c.px, c.py, s, DV{}, V3{}, none);
+        if (Ls) Ls[(size_t)c.pix * spp + s] = r;
         if (finite_dv(r)) {
             a0 += r.x;
             a1 += r.y;
@@ -546,15 +548,16 @@ __global__ void k_adj_forward(const DevScene S, const Theta T, uint32_t spp, uin
     atomicAdd(img + 3 * c.pix + 2, a2 / spp);
 }
 
-// Replay 1 then replay 2 per sample; d_img = dLoss/dI per pixel.
+// Replay 1 (or the forward pass's kept radiance `Ls`) then replay 2 per sample; d_img = dLoss/dI
+// per pixel.
 __global__ void k_adj_backward(const DevScene S, const Theta T, uint32_t spp, uint32_t chunk, const double *d_img,
-                               const AdjGrad go) {
+                               const AdjGrad go, const DV *Ls) {
     Cell c;
     if (!cell_of(T.F.P, spp, chunk, c)) return;
     V3 w = v3((float)(d_img[3 * c.pix] / spp), (float)(d_img[3 * c.pix + 1] / spp), (float)(d_img[3 * c.pix + 2] / spp));
     if (w.x == 0.0f && w.y == 0.0f && w.z == 0.0f) return;
     for (uint32_t s = c.s0; s < c.s1; s++) {
-        DV L = path<M_FWD>(S, T, c.px, c.py, s, DV{}, V3{}, go);
+        DV L = Ls ? Ls[(size_t)c.pix * spp + s] : path<M_FWD>(S, T, c.px, c.py, s, DV{}, V3{}, go);
         if (!finite_dv(L)) continue;
         (void)path<M_GRAD>(S, T, c.px, c.py, s, L, w, go);
     }
@@ -598,16 +601,18 @@ unsigned adj_blocks(const DevParams &P, uint32_t spp) {
 }
 }  // namespace
 
-cudaError_t launch_adj_forward(const DevScene &S, const AdjFrame &F, uint32_t spp, double *img, cudaStream_t st) {
+cudaError_t launch_adj_forward(const DevScene &S, const AdjFrame &F, uint32_t spp, double *img, double *Ls,
+                               cudaStream_t st) {
     adj::Theta t{F, F.albedo, F.P.sun_dir};
-    adj::k_adj_forward<<<adj_blocks(F.P, spp), kAdjThreads, 0, st>>>(S, t, spp, kAdjChunk, img);
+    adj::k_adj_forward<<<adj_blocks(F.P, spp), kAdjThreads, 0, st>>>(S, t, spp, kAdjChunk, img, (adj::DV *)Ls);
     return cudaGetLastError();
 }
 
 cudaError_t launch_adj_backward(const DevScene &S, const AdjFrame &F, uint32_t spp, const double *d_img,
-                                const AdjGrad &G, cudaStream_t st) {
+                                const AdjGrad &G, const double *Ls, cudaStream_t st) {
     adj::Theta t{F, F.albedo, F.P.sun_dir};
-    adj::k_adj_backward<<<adj_blocks(F.P, spp), kAdjThreads, 0, st>>>(S, t, spp, kAdjChunk, d_img, G);
+    adj::k_adj_backward<<<adj_blocks(F.P, spp), kAdjThreads, 0, st>>>(S, t, spp, kAdjChunk, d_img, G,
+                                                                      (const adj::DV *)Ls);
     return cudaGetLastError();
 }
 

@@ -138,7 +138,8 @@ struct lw_ctx {
     // the differentiable form: per frame slot (0 and 1: the frames, 2: the nominal frame)
     DBuf<float> adj_albedo[3], adj_sky[3], adj_emit[3];
     DBuf<int32_t> adj_tparam[3];
-    DBuf<double> adj_img, adj_img2, adj_g;
+    DBuf<double> adj_img, adj_img2, adj_g, adj_L;
+    uint64_t adj_L_key = 0;  // the inputs the kept per-sample radiance belongs to (0: none)
 };
 
 namespace {
@@ -594,7 +595,7 @@ void lw_ctx_destroy(lw_ctx *c) {
         c->adj_emit[k].free_();
         c->adj_tparam[k].free_();
     }
-    for (auto *b : {&c->adj_img, &c->adj_img2, &c->adj_g}) b->free_();
+    for (auto *b : {&c->adj_img, &c->adj_img2, &c->adj_g, &c->adj_L}) b->free_();
     c->wf.free_();
     c->bwf.free_();
     c->bv_blocks.free_();
@@ -1232,6 +1233,30 @@ lw_status adj_upload(lw_ctx *c, const lw_adj_frame *f, int k, AdjFrame &out, uin
     return LW_OK;
 }
 
+// A 64-bit digest of a frame of the differentiable form and its spp (the key of the kept
+// per-sample radiance): every input byte through a multiply-xorshift mix.
+uint64_t mix_bytes(uint64_t h, const void *p, uint64_t n) {
+    const unsigned char *b = (const unsigned char *)p;
+    uint64_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        std::memcpy(&w, b + i, 8);
+        h = (h ^ w) * 0x9E3779B97F4A7C15ull;
+        h ^= h >> 29;
+    }
+    for (; i < n; i++) h = ((h ^ b[i]) * 0x100000001B3ull) ^ (h >> 31);
+    return h ^ n;
+}
+uint64_t adj_key(const lw_adj_frame *f, uint32_t spp) {
+    uint64_t h = 0x243F6A8885A308D3ull ^ spp;
+    h = mix_bytes(h, f->params, sizeof(lw_params));
+    h = mix_bytes(h, f->sky, f->sky_len * 4);
+    h = mix_bytes(h, f->albedo, (uint64_t)f->n_params * 12);
+    h = mix_bytes(h, f->texel_param, f->texel_param_len * 4);
+    h = mix_bytes(h, f->emitter_scale, LW_EMITTER_GROUPS * 4);
+    return h ? h : 1u;
+}
+
 lw_status adj_begin(lw_ctx *c) {
     if (!c) return LW_ERR_INVALID_ARGUMENT;
     if (!c->has_scene) return fail(c, LW_ERR_NO_SCENE, "no scene uploaded");
@@ -1266,11 +1291,17 @@ lw_status lw_adjoint_forward(lw_ctx *c, const lw_adj_frame *frame, uint32_t spp,
     size_t n = (size_t)F.P.frame.x * F.P.frame.y * 3;
     CK(c, ensure(c->adj_img, n), "allocating the image");
     CK(c, cudaMemsetAsync(c->adj_img.p, 0, n * 8, c->stream), "clearing the image");
-    struct A { DevScene S; AdjFrame F; uint32_t spp; double *img; } a{dev_scene(c), F, spp, c->adj_img.p};
+    // Each sample's radiance is kept for a backward pass over the same inputs (up to 4 GiB).
+    const uint64_t kept = (uint64_t)n / 3 * spp * 3;
+    double *Ls = nullptr;
+    c->adj_L_key = 0;
+    if (kept * 8 <= (uint64_t(4) << 30) && ensure(c->adj_L, kept) == cudaSuccess) Ls = c->adj_L.p;
+    struct A { DevScene S; AdjFrame F; uint32_t spp; double *img, *Ls; } a{dev_scene(c), F, spp, c->adj_img.p, Ls};
     s = adj_timed(c, [](lw_ctx *cc, void *p) {
         A &x = *(A *)p;
-        return launch_adj_forward(x.S, x.F, x.spp, x.img, cc->stream);
+        return launch_adj_forward(x.S, x.F, x.spp, x.img, x.Ls, cc->stream);
     }, &a, (uint64_t)n / 3 * spp);
+    if (s == LW_OK && Ls) c->adj_L_key = adj_key(frame, spp);
     if (s != LW_OK) return s;
     CK(c, cudaMemcpy(out_rgb, c->adj_img.p, n * 8, cudaMemcpyDeviceToHost), "reading the image");
     return LW_OK;
@@ -1295,11 +1326,14 @@ lw_status lw_adjoint_backward(lw_ctx *c, const lw_adj_frame *frame, uint32_t spp
     G.emit = G.albedo + (size_t)np * 3;
     G.cache = G.emit + LW_EMITTER_GROUPS;
     G.sun = G.cache + frame->sky_len;
-    struct A { DevScene S; AdjFrame F; uint32_t spp; const double *d; AdjGrad G; } a{dev_scene(c), F, spp, c->adj_img.p, G};
+    // The forward pass's per-sample radiance, when it was over these very inputs, replaces replay 1.
+    const double *Ls = c->adj_L_key && c->adj_L_key == adj_key(frame, spp) ? c->adj_L.p : nullptr;
+    struct A { DevScene S; AdjFrame F; uint32_t spp; const double *d; AdjGrad G; const double *Ls; } a{
+        dev_scene(c), F, spp, c->adj_img.p, G, Ls};
     s = adj_timed(c, [](lw_ctx *cc, void *p) {
         A &x = *(A *)p;
-        return launch_adj_backward(x.S, x.F, x.spp, x.d, x.G, cc->stream);
-    }, &a, (uint64_t)n / 3 * spp * 2);
+        return launch_adj_backward(x.S, x.F, x.spp, x.d, x.G, x.Ls, cc->stream);
+    }, &a, (uint64_t)n / 3 * spp * (Ls ? 1u : 2u));
     if (s != LW_OK) return s;
     if (np) CK(c, cudaMemcpy(out->albedo, G.albedo, (size_t)np * 3 * 8, cudaMemcpyDeviceToHost), "reading the gradient");
     CK(c, cudaMemcpy(out->emitter_scale, G.emit, LW_EMITTER_GROUPS * 8, cudaMemcpyDeviceToHost), "reading the gradient");

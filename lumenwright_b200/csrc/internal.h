@@ -147,9 +147,12 @@ struct AdjGrad {
     double *cache;   // one per sky float
     double *sun;     // [3]: d / d sun_dir.xyz
 };
-cudaError_t launch_adj_forward(const DevScene &S, const AdjFrame &F, uint32_t spp, double *img, cudaStream_t st);
+// Ls: per-sample radiance, 3 doubles per sample at [pixel * spp + sample] (kept by the forward
+// pass, read by the backward pass in place of its first replay), or null.
+cudaError_t launch_adj_forward(const DevScene &S, const AdjFrame &F, uint32_t spp, double *img, double *Ls,
+                               cudaStream_t st);
 cudaError_t launch_adj_backward(const DevScene &S, const AdjFrame &F, uint32_t spp, const double *d_img,
-                                const AdjGrad &G, cudaStream_t st);
+                                const AdjGrad &G, const double *Ls, cudaStream_t st);
 cudaError_t launch_adj_fd(const DevScene &S, const AdjFrame &plus, const AdjFrame &minus, const float *albedo0,
                           float4 sun0, uint32_t spp, double *diff, double *mean, cudaStream_t st);
 
