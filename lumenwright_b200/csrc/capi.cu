@@ -110,7 +110,10 @@ struct lw_ctx {
     uint64_t batch_samples = 0;
     size_t partials_cap_bytes = size_t(4) << 30;
     // the wavefront engine: path slots (grown to the largest pool used), queue fetch settings
-    uint32_t wf_tail = 4;
+#ifndef LW_WF_TAIL
+#define LW_WF_TAIL 8
+#endif
+    uint32_t wf_tail = LW_WF_TAIL;
     LaunchShape shape_wf{};
     struct WfBufs {
         DBuf<float4> state, hit0, ts;

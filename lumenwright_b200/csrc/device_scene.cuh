@@ -283,131 +283,174 @@ LW_DI bool trace_begin(TraceState &ts, const DevParams &P, V3 o, V3 d, float tma
     return true;
 }
 
+// The brick a traversal is in: its top and overlay entries and its occupancy mask, loaded once
+// when the ray enters the brick and kept in registers.
+struct BrickCache {
+    uint32_t b, entry, ov;
+    uint2 occ;
+};
+LW_DI BrickCache no_brick() { return BrickCache{0xFFFFFFFFu, EMPTY, EMPTY, make_uint2(0u, 0u)}; }
+
+// The per-ray constants of the traversal loop.
+struct RayDda {
+    int s0, s1, s2;     // signs of the direction
+    int gs0, gs1, gs2;  // the grid's size in voxels
+};
+LW_DI RayDda ray_dda(const DevParams &P, V3 d) {
+    return RayDda{sgn(d.x), sgn(d.y), sgn(d.z), (int)P.grid_dims.x * 16, (int)P.grid_dims.y * 16, (int)P.grid_dims.z * 16};
+}
+
+// One iteration of trace's loop (trace.rs:176-241) up to the quad tests. Returns -1 when the ray
+// leaves the range or the grid (or the visit limit is reached), 0 when it stepped past an empty
+// brick or voxel, 1 when the cell has quads to test: its model in `model`, its brick's overlay
+// entry in bc.ov; the DDA then stays in that cell.
+//  * A voxel in an empty 4^3 sub-block of a brick without overlay is not read (its model is 0, it
+//    tests no quad); with LW_SUBBLOCK_SKIP the rest of that sub-block is crossed in one step
+//    (skip_empty_sub_block).
+//  * Every visit (brick skip, empty voxel, voxel with quads) counts towards MAX_STEPS as one
+//    iteration of the reference's loop does.
+LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, const RayDda &R, BrickCache &bc,
+                uint32_t &model) {
+    const uint32_t dx = P.grid_dims.x, dz = P.grid_dims.z;
+    Dda &s = ts.s;
+    if (ts.it >= MAX_STEPS) return -1;
+    ts.it++;
+    uint32_t bx = (uint32_t)(s.c0 >> 4), by = (uint32_t)(s.c1 >> 4), bz = (uint32_t)(s.c2 >> 4);
+    uint32_t b = (by * dz + bz) * dx + bx;
+    if (b != bc.b) {
+        bc.b = b;
+        uint2 e = ldg(S.top + b);
+        bc.entry = e.x;
+        bc.ov = e.y;
+        if (bc.entry != EMPTY && !(bc.entry & UNIFORM)) bc.occ = ldg(S.occ + bc.entry);
+    }
+    const V3 inv = ts.inv;
+    if (bc.entry == EMPTY && bc.ov == EMPTY) {
+        // Skip the whole brick: jump to its exit face (trace.rs:184-226).
+        int bc0 = (int)bx, bc1 = (int)by, bc2 = (int)bz;
+        float t_out = kINF;
+        int axis = 0;
+        if (R.s0 != 0) {
+            float tt = ((float)(R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
+            if (tt < t_out) { t_out = tt; axis = 0; }
+        }
+        if (R.s1 != 0) {
+            float tt = ((float)(R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
+            if (tt < t_out) { t_out = tt; axis = 1; }
+        }
+        if (R.s2 != 0) {
+            float tt = ((float)(R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
+            if (tt < t_out) { t_out = tt; axis = 2; }
+        }
+        if (t_out > ts.t_end) return -1;
+        V3 pos = o + d * t_out;
+        s.c0 = axis == 0 ? (R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
+        s.c1 = axis == 1 ? (R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
+        s.c2 = axis == 2 ? (R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
+        int ca = axis == 0 ? s.c0 : (axis == 1 ? s.c1 : s.c2);
+        int ga = axis == 0 ? R.gs0 : (axis == 1 ? R.gs1 : R.gs2);
+        if (ca < 0 || ca >= ga) return -1;
+        s.n0 = next_boundary(o.x, inv.x, s.c0, R.s0);
+        s.n1 = next_boundary(o.y, inv.y, s.c1, R.s1);
+        s.n2 = next_boundary(o.z, inv.z, s.c2, R.s2);
+        s.t = t_out;
+        return 0;
+    }
+    // Block model in this voxel (trace.rs:233-241).
+    model = 0u;
+    if (bc.entry != EMPTY) {
+        if (bc.entry & UNIFORM) {
+            model = bc.entry & ~UNIFORM;
+        } else {
+            int lx = s.c0 & 15, ly = s.c1 & 15, lz = s.c2 & 15;
+            uint32_t sb = (uint32_t)(((ly >> 2) * 4 + (lz >> 2)) * 4 + (lx >> 2));
+            uint32_t word = sb < 32u ? bc.occ.x : bc.occ.y;
+            if ((word >> (sb & 31u)) & 1u) {
+                model = brick_voxel(S, bc.entry, lx, ly, lz);
+            } else if (LW_SUBBLOCK_SKIP && bc.ov == EMPTY) {
+                // An empty 4^3 sub-block: go to where the DDA would leave it.
+                return skip_empty_sub_block(s, o, inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end, ts.it) < 0 ? -1 : 0;
+            }
+        }
+    }
+    if (model != 0u || bc.ov != EMPTY) return 1;
+    return dda_advance(s, o, inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end) ? 0 : -1;
+}
+
+// The quads of the cell the DDA is in (trace.rs:228-264): true with the closest hit in `out`.
+LW_DI bool test_cell(const DevScene &S, const DevParams &P, const TraceState &ts, V3 o, V3 d, float tmin, uint32_t model,
+                     uint32_t ov, Hit &out) {
+    const Dda &s = ts.s;
+    float t_cell_exit = fmin_r(s.n0, fmin_r(s.n1, s.n2));
+    float t_lo = fmax_r(s.t - 1e-4f, tmin);
+    float t_hi = t_cell_exit + 1e-4f;
+    Hit cand = no_hit();
+    cand.t = fmin_r(t_hi, ts.t_end + 1e-3f);
+    if (model != 0u) {
+        uint4 m = ldg(S.models + model);
+        V3 lo = o - v3((float)s.c0, (float)s.c1, (float)s.c2);
+        for (uint32_t i = 0; i < m.y; i++) test_quad(S, P, m.x + i, lo, d, t_lo, cand);
+    }
+    if (ov != EMPTY) {
+        uint32_t local = (uint32_t)((((s.c1 & 15) * 16 + (s.c2 & 15)) * 16) + (s.c0 & 15));
+        size_t base = (size_t)P.off.w + (size_t)ov * OV_CELL_WORDS + local * 2u;
+        uint32_t off = ldg(S.grid + base);
+        uint32_t count = ldg(S.grid + base + 1);
+        for (uint32_t i = 0; i < count; i++) {
+            uint32_t qi = ldg(S.grid + (size_t)P.off2.x + off + i);
+            test_quad(S, P, qi, o, d, t_lo, cand);
+        }
+    }
+    if (cand.quad == NO_QUAD) return false;
+    out = cand;
+    return true;
+}
+
 // The traversal loop of trace (trace.rs:176-289), run for at most `budget` voxel visits (0: no
 // limit). Returns 1 with the hit, -1 when the ray leaves without one, 0 when the budget ran out
 // first; trace_run then continues from `ts` exactly where it stopped.
 //
-// The DDA is the reference's step for step; what differs is where the words come from and how
-// the lanes of a warp are kept together:
-//  * the brick's top and overlay entries and its occupancy mask are loaded once when the ray
-//    enters the brick and kept in registers; a voxel in an empty 4^3 sub-block of a brick without
-//    overlay is not read (its model is 0, it tests no quad) and the rest of that sub-block is
-//    crossed in one step (skip_empty_sub_block);
-//  * the loop is split in two (a "while-while" traversal): an inner loop steps through empty
-//    bricks and empty voxels until the ray reaches a voxel with a model or overlay quads, then
-//    the quads of that voxel are tested, so the lanes of a warp reach the quad tests together.
-// Every visit (brick skip, empty voxel, voxel with quads) counts towards MAX_STEPS as one
-// iteration of the reference's loop does.
+// The DDA is the reference's step for step; what differs is where the words come from (visit) and
+// how the lanes of a warp are kept together: the loop is split in two (a "while-while" traversal),
+// an inner loop that steps through empty bricks and empty voxels until the ray reaches a cell with
+// quads, then the quads of that cell, so the lanes of a warp reach the quad tests together.
 LW_DI int trace_run(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, float tmin, uint32_t budget,
                     Hit &out) {
-    const uint32_t dx = P.grid_dims.x, dy = P.grid_dims.y, dz = P.grid_dims.z;
-    const int gs0 = (int)dx * 16, gs1 = (int)dy * 16, gs2 = (int)dz * 16;
-    const int s0 = sgn(d.x), s1 = sgn(d.y), s2 = sgn(d.z);
-    const V3 inv = ts.inv;
-    const float t_end = ts.t_end;
-    const float best_t = t_end + 1e-3f;
-    Dda &s = ts.s;
-    uint32_t cur_b = 0xFFFFFFFFu, entry = EMPTY, ov = EMPTY;
-    uint2 occ = make_uint2(0u, 0u);
+    const RayDda R = ray_dda(P, d);
+    BrickCache bc = no_brick();
     uint32_t n = 0;
     for (;;) {
-        // Inner loop: empty space, up to the next voxel with a model or overlay quads.
         uint32_t model = 0;
         for (;;) {
-            if (ts.it >= MAX_STEPS) return -1;
             if (budget != 0u && n >= budget) return 0;
             n++;
-            ts.it++;
-            uint32_t bx = (uint32_t)(s.c0 >> 4), by = (uint32_t)(s.c1 >> 4), bz = (uint32_t)(s.c2 >> 4);
-            uint32_t b = (by * dz + bz) * dx + bx;
-            if (b != cur_b) {
-                cur_b = b;
-                uint2 e = ldg(S.top + b);
-                entry = e.x;
-                ov = e.y;
-                if (entry != EMPTY && !(entry & UNIFORM)) occ = ldg(S.occ + entry);
-            }
-            if (entry == EMPTY && ov == EMPTY) {
-                // Skip the whole brick: jump to its exit face (trace.rs:184-226).
-                int bc0 = (int)bx, bc1 = (int)by, bc2 = (int)bz;
-                float t_out = kINF;
-                int axis = 0;
-                if (s0 != 0) {
-                    float tt = ((float)(s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
-                    if (tt < t_out) { t_out = tt; axis = 0; }
-                }
-                if (s1 != 0) {
-                    float tt = ((float)(s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
-                    if (tt < t_out) { t_out = tt; axis = 1; }
-                }
-                if (s2 != 0) {
-                    float tt = ((float)(s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
-                    if (tt < t_out) { t_out = tt; axis = 2; }
-                }
-                if (t_out > t_end) return -1;
-                V3 pos = o + d * t_out;
-                s.c0 = axis == 0 ? (s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
-                s.c1 = axis == 1 ? (s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
-                s.c2 = axis == 2 ? (s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
-                int ca = axis == 0 ? s.c0 : (axis == 1 ? s.c1 : s.c2);
-                int ga = axis == 0 ? gs0 : (axis == 1 ? gs1 : gs2);
-                if (ca < 0 || ca >= ga) return -1;
-                s.n0 = next_boundary(o.x, inv.x, s.c0, s0);
-                s.n1 = next_boundary(o.y, inv.y, s.c1, s1);
-                s.n2 = next_boundary(o.z, inv.z, s.c2, s2);
-                s.t = t_out;
-                continue;
-            }
-            // Block model in this voxel (trace.rs:233-241).
-            if (entry == EMPTY) {
-                model = 0;
-            } else if (entry & UNIFORM) {
-                model = entry & ~UNIFORM;
-            } else {
-                int lx = s.c0 & 15, ly = s.c1 & 15, lz = s.c2 & 15;
-                uint32_t sb = (uint32_t)(((ly >> 2) * 4 + (lz >> 2)) * 4 + (lx >> 2));
-                uint32_t word = sb < 32u ? occ.x : occ.y;
-                if ((word >> (sb & 31u)) & 1u) {
-                    model = brick_voxel(S, entry, lx, ly, lz);
-                } else if (LW_SUBBLOCK_SKIP && ov == EMPTY) {
-                    // An empty 4^3 sub-block: go to where the DDA would leave it.
-                    if (skip_empty_sub_block(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end, ts.it) < 0) return -1;
-                    continue;
-                } else {
-                    model = 0;
-                }
-            }
-            if (model != 0u || ov != EMPTY) break;
-            if (!dda_advance(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end)) return -1;
+            int r = visit(S, P, ts, o, d, R, bc, model);
+            if (r < 0) return -1;
+            if (r > 0) break;
         }
-
-        // The voxel's quads (trace.rs:228-264).
-        float t_cell_exit = fmin_r(s.n0, fmin_r(s.n1, s.n2));
-        float t_lo = fmax_r(s.t - 1e-4f, tmin);
-        float t_hi = t_cell_exit + 1e-4f;
-        Hit cand = no_hit();
-        cand.t = fmin_r(t_hi, best_t);
-        if (model != 0u) {
-            uint4 m = ldg(S.models + model);
-            V3 lo = o - v3((float)s.c0, (float)s.c1, (float)s.c2);
-            for (uint32_t i = 0; i < m.y; i++) test_quad(S, P, m.x + i, lo, d, t_lo, cand);
-        }
-        if (ov != EMPTY) {
-            uint32_t local = (uint32_t)((((s.c1 & 15) * 16 + (s.c2 & 15)) * 16) + (s.c0 & 15));
-            size_t base = (size_t)P.off.w + (size_t)ov * OV_CELL_WORDS + local * 2u;
-            uint32_t off = ldg(S.grid + base);
-            uint32_t count = ldg(S.grid + base + 1);
-            for (uint32_t i = 0; i < count; i++) {
-                uint32_t qi = ldg(S.grid + (size_t)P.off2.x + off + i);
-                test_quad(S, P, qi, o, d, t_lo, cand);
-            }
-        }
-        if (cand.quad != NO_QUAD) {
-            out = cand;
-            return 1;
-        }
-        if (!dda_advance(s, o, inv, s0, s1, s2, gs0, gs1, gs2, t_end)) return -1;
+        if (test_cell(S, P, ts, o, d, tmin, model, bc.ov, out)) return 1;
+        if (!dda_advance(ts.s, o, ts.inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end)) return -1;
     }
+}
+
+// One round of a traversal for the lanes of a warp that trace rays together: at most `budget`
+// (>= 1) visits through empty space, up to the first cell with quads, then that cell's quad tests.
+// Each lane meets at most one cell with quads per round, so the warp runs one phase of quad tests
+// per round with every lane that reached such a cell. Returns as trace_run does; after 0 the next
+// round continues from `ts`. The visits and quad tests are trace_run's, in the same order.
+LW_DI int trace_round(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, float tmin, uint32_t budget,
+                      Hit &out) {
+    const RayDda R = ray_dda(P, d);
+    BrickCache bc = no_brick();
+    uint32_t model = 0;
+    int r = 0;
+    for (uint32_t n = 0; n < budget; n++) {
+        r = visit(S, P, ts, o, d, R, bc, model);
+        if (r != 0) break;
+    }
+    if (r <= 0) return r;
+    if (test_cell(S, P, ts, o, d, tmin, model, bc.ov, out)) return 1;
+    return dda_advance(ts.s, o, ts.inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end) ? 0 : -1;
 }
 
 // trace (trace.rs:137-290): the closest hit along o + t d, t in (tmin, tmax), in one go.

@@ -161,7 +161,9 @@ LW_DI void shade_slot(uint32_t i, const DevScene &S0, const DevParams &P0, const
     float4 core = ld(F, W_CORE, i);
     uint32_t flags = fu(core.w);
     if (flags & F_DEAD) return;
-    float4 it2 = ld(F, W_ITEM2, i);
+    // The item words: in the batched form the camera is needed at every step, otherwise only when
+    // a sample ends.
+    float4 it2 = BATCH ? ld(F, W_ITEM2, i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     uint32_t job = BATCH ? fu(it2.z) : 0u;
     Path p;
     Act a = A_END;
@@ -181,6 +183,7 @@ LW_DI void shade_slot(uint32_t i, const DevScene &S0, const DevParams &P0, const
     }
     if (a == A_END) {
         // The sample is over: the item's sums, then its next sample or the next item.
+        if (!BATCH) it2 = ld(F, W_ITEM2, i);
         float4 it = ld(F, W_ITEM, i), sa = ld(F, W_SUM, i), sb = ld(F, W_SUM2, i);
         uint32_t px = fu(it.x), py = fu(it.y), sample = fu(it.z), s_end = fu(it.w);
         uint32_t j = fu(it2.x), pslot = fu(it2.y);
@@ -289,8 +292,10 @@ __global__ void k_wf_advance_graph(const WfState F, cudaGraphConditionalHandle l
 #ifndef LW_WF_TRACE_MINB
 #define LW_WF_TRACE_MINB 8
 #endif
-// Traces the queued rays of this iteration: each lane takes a ray, advances it by at most `budget`
-// voxel visits per round, and takes the next queued ray as soon as its ray ends. Once the queue
+// Traces the queued rays of this iteration: each lane takes a ray and advances it in rounds
+// (trace_round: at most `budget` visits through empty space, then the quad tests of at most one
+// cell, so the lanes of a warp run one phase of quad tests per round together), and takes the
+// next queued ray as soon as its ray ends. Once the queue
 // has run dry, a ray still on its way after `tail` more rounds saves its traversal state and goes
 // to the next iteration's queue, so an iteration does not wait for its single longest ray.
 __global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevScene S, const DevParams P, const WfState F,
@@ -352,7 +357,7 @@ __global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevSce
         if (__any_sync(FULL, done)) rounds++;  // the queue is dry: count the tail rounds
         if (have) {
             Hit h = no_hit();
-            int r = trace_run(S, P, ts, o, d, tmin, budget, h);
+            int r = trace_round(S, P, ts, o, d, tmin, budget, h);
             if (r != 0) {
                 if (r != 1) h = no_hit();
                 F.hit0[slot] = make_float4(h.t, __uint_as_float(h.quad), __uint_as_float(h.texel), h.s);
@@ -395,6 +400,7 @@ cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const 
 
 cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState &F, LaunchShape trace_shape,
                             uint32_t budget, uint32_t tail, cudaStream_t st) {
+    if (budget == 0u) budget = 4u;  // a round makes at least one visit
     k_wf_trace<<<trace_shape.blocks, trace_shape.threads, 0, st>>>(S, P, F, budget, tail);
     return cudaGetLastError();
 }
