@@ -96,30 +96,31 @@ LW_DI V3 linear_rgb(const float *gamma, uint32_t c) {
     return v3(gamma[c & 0xFFu], gamma[(c >> 8) & 0xFFu], gamma[(c >> 16) & 0xFFu]);
 }
 
-// test_quad (trace.rs:81-109) with intersect_quad (:37-58) and quad_texel (:62-69). The normal
-// eu x ev and n . n come precomputed; a front-only quad met from behind is rejected before the
-// division instead of after it: `normal() . d` is exactly `-(n . d)`, and intersect_quad has no
-// side effects, so the outcome is the reference's.
-LW_DI void test_quad(const DevScene &S, const DevParams &P, uint32_t qi, V3 o, V3 d, float tmin, Hit &best) {
+// intersect_quad (trace.rs:37-58) with quad_texel (:62-69) and the alpha test of test_quad
+// (:81-109): whether quad qi is met at a t in (tmin, t_limit), inside its bounds, on a texel that
+// is not cut out; the hit in `h`. The normal eu x ev and n . n come precomputed; a front-only quad
+// met from behind is rejected before the division instead of after it: `normal() . d` is exactly
+// `-(n . d)`, and intersect_quad has no side effects, so the outcome is the reference's.
+LW_DI bool quad_candidate(const DevScene &S, const DevParams &P, uint32_t qi, V3 o, V3 d, float tmin, float t_limit,
+                          Hit &h) {
     const DevQuad *q = S.quads + qi;
-    float reach = (best.quad != NO_QUAD && qi > best.quad) ? best.t + COPLANAR : best.t;
     float4 a = ldg(&q->n_nn);
     V3 n = f4v(a);
     float denom = dot(n, d);
-    if (fabs_r(denom) < 1e-12f) return;
+    if (fabs_r(denom) < 1e-12f) return false;
     float4 b = ldg(&q->p0_flags);
     uint32_t flags = __float_as_uint(b.w);
-    if ((flags & FLAG_FRONT_ONLY) && -denom >= 0.0f) return;
+    if ((flags & FLAG_FRONT_ONLY) && -denom >= 0.0f) return false;
     V3 p0 = f4v(b);
     float t = __fdiv_rn(dot(n, p0 - o), denom);
-    if (!(t > tmin && t < reach)) return;
+    if (!(t > tmin && t < t_limit)) return false;
     V3 eu = f4v(ldg(&q->eu_tint));
     V3 ev = f4v(ldg(&q->ev_em));
     V3 p = (o + d * t) - p0;
     float nn = a.w;
     float s = __fdiv_rn(dot(cross(p, ev), n), nn);
     float tt = __fdiv_rn(dot(cross(eu, p), n), nn);
-    if (s < 0.0f || s > 1.0f || tt < 0.0f || tt > 1.0f) return;
+    if (s < 0.0f || s > 1.0f || tt < 0.0f || tt > 1.0f) return false;
     float4 uv = ldg(&q->uv);
     float4 uvt = ldg(&q->uvt);
     float sc = fmin_r(fmax_r(s, 0.0005f), 0.9995f);
@@ -129,8 +130,21 @@ LW_DI void test_quad(const DevScene &S, const DevParams &P, uint32_t qi, V3 o, V
     uint32_t tx = texel(S, P, u, v);
     uint32_t alpha = tx >> 24;
     uint32_t mode = flags & FLAG_ALPHA_MASK;
-    if ((mode == ALPHA_CUTOUT && alpha < 128u) || (mode == ALPHA_TRANSLUCENT && alpha == 0u)) return;
-    best = Hit{t, qi, tx, s, tt};
+    if ((mode == ALPHA_CUTOUT && alpha < 128u) || (mode == ALPHA_TRANSLUCENT && alpha == 0u)) return false;
+    h = Hit{t, qi, tx, s, tt};
+    return true;
+}
+
+// The acceptance rule of test_quad (trace.rs:81-109): a quad is taken when it is met before the
+// best hit so far, or (a later quad, coplanar with it) less than COPLANAR behind it.
+LW_DI float reach_of(const Hit &best, uint32_t qi) {
+    return (best.quad != NO_QUAD && qi > best.quad) ? best.t + COPLANAR : best.t;
+}
+
+// test_quad (trace.rs:81-109).
+LW_DI void test_quad(const DevScene &S, const DevParams &P, uint32_t qi, V3 o, V3 d, float tmin, Hit &best) {
+    const float reach = reach_of(best, qi);
+    quad_candidate(S, P, qi, o, d, tmin, reach, best);  // writes `best` only when the quad is taken
 }
 
 // SceneView::voxel (scene.rs:271-284) on the re-laid grid.
@@ -433,24 +447,114 @@ LW_DI int trace_run(const DevScene &S, const DevParams &P, TraceState &ts, V3 o,
     }
 }
 
-// One round of a traversal for the lanes of a warp that trace rays together: at most `budget`
-// (>= 1) visits through empty space, up to the first cell with quads, then that cell's quad tests.
-// Each lane meets at most one cell with quads per round, so the warp runs one phase of quad tests
-// per round with every lane that reached such a cell. Returns as trace_run does; after 0 the next
+// The quad tests of the cells the lanes of a warp reached in a round, spread over the warp. Every
+// lane calls it (a lane without a cell passes pending = false). The quads of the pending lanes'
+// models form one list in lane order; entry k runs quad_candidate on lane k % 32 (in chunks of
+// 32), with its owner's ray fetched by shuffles, and writes its candidate hit to `sq` (32 entries
+// for this warp). Each owner then takes its own quads' candidates in quad order under trace's
+// acceptance rule (reach_of), exactly as the sequential loop of test_cell would, and tests its
+// cell's overlay quads, if any, after them. Returns true with the closest hit in `out`.
+LW_DI bool warp_test_cells(const DevScene &S, const DevParams &P, const TraceState &ts, V3 o, V3 d, float tmin,
+                           bool pending, uint32_t model, uint32_t ov, Hit &out, float4 *sq) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const Dda &s = ts.s;
+    float t_lo = 0.0f;
+    uint32_t qbase = 0u, cnt = 0u;
+    V3 lo = v3(0.0f, 0.0f, 0.0f);
+    Hit best = no_hit();
+    if (pending) {
+        float t_cell_exit = fmin_r(s.n0, fmin_r(s.n1, s.n2));
+        t_lo = fmax_r(s.t - 1e-4f, tmin);
+        best.t = fmin_r(t_cell_exit + 1e-4f, ts.t_end + 1e-3f);
+        if (model != 0u) {
+            uint4 m = ldg(S.models + model);
+            qbase = m.x;
+            cnt = m.y;
+        }
+        lo = o - v3((float)s.c0, (float)s.c1, (float)s.c2);
+    }
+    // Exclusive scan of the lanes' quad counts.
+    uint32_t incl = cnt;
+    for (uint32_t off = 1; off < 32u; off <<= 1) {
+        uint32_t v = __shfl_up_sync(FULL, incl, off);
+        if (lane >= off) incl += v;
+    }
+    const uint32_t pre = incl - cnt;
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    for (uint32_t base = 0; base < total; base += 32u) {
+        const uint32_t k = base + lane;
+        // The entry's owner: the highest lane whose list starts at or before k (a lane with no
+        // quads starts where the next one does, so the owner of an entry k < total has quads).
+        uint32_t L = 0;
+        for (uint32_t step = 16; step != 0u; step >>= 1) {
+            uint32_t p = __shfl_sync(FULL, pre, L + step);
+            if (p <= k) L += step;
+        }
+        const V3 olo = v3(__shfl_sync(FULL, lo.x, L), __shfl_sync(FULL, lo.y, L), __shfl_sync(FULL, lo.z, L));
+        const V3 od = v3(__shfl_sync(FULL, d.x, L), __shfl_sync(FULL, d.y, L), __shfl_sync(FULL, d.z, L));
+        const float otlo = __shfl_sync(FULL, t_lo, L);
+        const uint32_t oq = __shfl_sync(FULL, qbase, L) + (k - __shfl_sync(FULL, pre, L));
+        Hit h;
+        // No upper bound on t here: the owner applies the exact reach when it takes the entry.
+        const bool valid = k < total && quad_candidate(S, P, oq, olo, od, otlo, kINF, h);
+        if (valid) sq[lane] = make_float4(h.t, h.s, h.tt, __uint_as_float(h.texel));
+        const unsigned vm = __ballot_sync(FULL, valid);
+        __syncwarp();
+        // This lane's entries in the chunk, in order; only valid candidates can be taken.
+        if (cnt != 0u && pre < base + 32u && pre + cnt > base) {
+            const uint32_t a = pre > base ? pre - base : 0u;
+            const uint32_t b = min(pre + cnt - base, 32u);
+            unsigned mine = vm & (b >= 32u ? FULL : ((1u << b) - 1u)) & ~((1u << a) - 1u);
+            while (mine) {
+                const uint32_t j = (uint32_t)(__ffs(mine) - 1);
+                mine &= mine - 1u;
+                const float4 c = sq[j];
+                const uint32_t qi = qbase + (base + j - pre);
+                if (c.x < reach_of(best, qi)) best = Hit{c.x, qi, __float_as_uint(c.w), c.y, c.z};
+            }
+        }
+        __syncwarp();
+    }
+    if (pending && ov != EMPTY) {
+        uint32_t local = (uint32_t)((((s.c1 & 15) * 16 + (s.c2 & 15)) * 16) + (s.c0 & 15));
+        size_t b = (size_t)P.off.w + (size_t)ov * OV_CELL_WORDS + local * 2u;
+        uint32_t off = ldg(S.grid + b);
+        uint32_t count = ldg(S.grid + b + 1);
+        for (uint32_t i = 0; i < count; i++) {
+            uint32_t qi = ldg(S.grid + (size_t)P.off2.x + off + i);
+            test_quad(S, P, qi, o, d, t_lo, best);
+        }
+    }
+    if (!pending || best.quad == NO_QUAD) return false;
+    out = best;
+    return true;
+}
+
+// One round of a traversal for the lanes of a warp that trace rays together; every lane calls it
+// (a lane without a ray passes have = false and gets 0). Each lane makes at most `budget` (>= 1)
+// visits through empty space, up to the first cell with quads; then one warp_test_cells tests the
+// cells the lanes reached, so a warp runs one phase of quad tests per round, spread over its 32
+// lanes. Returns as trace_run does (1 hit, -1 no hit, 0 the round ended first); after 0 the next
 // round continues from `ts`. The visits and quad tests are trace_run's, in the same order.
-LW_DI int trace_round(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, float tmin, uint32_t budget,
-                      Hit &out) {
+LW_DI int trace_round_warp(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, float tmin,
+                           uint32_t budget, bool have, Hit &out, float4 *sq) {
     const RayDda R = ray_dda(P, d);
     BrickCache bc = no_brick();
     uint32_t model = 0;
     int r = 0;
-    for (uint32_t n = 0; n < budget; n++) {
-        r = visit(S, P, ts, o, d, R, bc, model);
-        if (r != 0) break;
+    if (have) {
+        for (uint32_t n = 0; n < budget; n++) {
+            r = visit(S, P, ts, o, d, R, bc, model);
+            if (r != 0) break;
+        }
     }
-    if (r <= 0) return r;
-    if (test_cell(S, P, ts, o, d, tmin, model, bc.ov, out)) return 1;
-    return dda_advance(ts.s, o, ts.inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end) ? 0 : -1;
+    const bool pending = have && r > 0;
+    if (__any_sync(0xFFFFFFFFu, pending)) {
+        const bool hit = warp_test_cells(S, P, ts, o, d, tmin, pending, model, bc.ov, out, sq);
+        if (pending) r = hit ? 1 : (dda_advance(ts.s, o, ts.inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end) ? 0 : -1);
+    }
+    return have ? r : 0;
 }
 
 // trace (trace.rs:137-290): the closest hit along o + t d, t in (tmin, tmax), in one go.

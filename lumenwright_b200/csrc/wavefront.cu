@@ -15,6 +15,11 @@
 namespace lw {
 namespace {
 
+// Queue entries a warp takes from the fetch counter at a time (one atomic per 32 rays, not per
+// round); at least 32, the most a warp can need at once.
+constexpr uint32_t kFetchChunk = 32u;
+constexpr int kTraceThreads = 128;  // threads per block of the tracing kernel
+
 enum : uint32_t { F_ACTIVE = 1u, F_DEAD = 2u };
 // hit0.y of a slot whose ray is still being traversed (carried over to the next iteration).
 constexpr uint32_t RESUME_MARK = 0xFFFFFFFEu;
@@ -51,8 +56,7 @@ LW_DI float4 u4(uint32_t a, uint32_t b, uint32_t c, uint32_t d) {
 }
 LW_DI uint32_t fu(float x) { return __float_as_uint(x); }
 
-LW_DI void load_core(const WfState &F, uint32_t i, Path &p, float4 core) {
-    float4 a = ld(F, W_O, i), b = ld(F, W_D, i), c = ld(F, W_RAD, i), d = ld(F, W_BETA, i);
+LW_DI void unpack_core(Path &p, float4 a, float4 b, float4 c, float4 d, float4 core) {
     p.o = f4v(a);
     p.tmin = a.w;
     p.d = f4v(b);
@@ -170,9 +174,11 @@ LW_DI void shade_slot(uint32_t i, const DevScene &S0, const DevParams &P0, const
     if (flags & F_ACTIVE) {
         float4 h0 = F.hit0[i];
         if (fu(h0.y) == RESUME_MARK) return;  // its ray is still on its way: nothing to shade yet
-        load_core(F, i, p, core);
+        float4 wo = ld(F, W_O, i), wd = ld(F, W_D, i), wr = ld(F, W_RAD, i), wb = ld(F, W_BETA, i);
+        float h1 = F.hit1[i];
+        unpack_core(p, wo, wd, wr, wb, core);
         if (p.kind != K_EXTEND) load_nee(F, i, p);
-        Hit h{h0.x, fu(h0.y), fu(h0.z), h0.w, F.hit1[i]};
+        Hit h{h0.x, fu(h0.y), fu(h0.z), h0.w, h1};
         if (BATCH) {
             DevScene S = S0;
             S.sky = B.jobs[job].sky;
@@ -298,7 +304,7 @@ __global__ void k_wf_advance_graph(const WfState F, cudaGraphConditionalHandle l
 // next queued ray as soon as its ray ends. Once the queue
 // has run dry, a ray still on its way after `tail` more rounds saves its traversal state and goes
 // to the next iteration's queue, so an iteration does not wait for its single longest ray.
-__global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevScene S, const DevParams P, const WfState F,
+__global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(const DevScene S, const DevParams P, const WfState F,
                                                                       uint32_t budget, uint32_t tail) {
     const unsigned FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
@@ -312,16 +318,29 @@ __global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevSce
     float tmin = 0.0f;
     uint32_t slot = 0, rounds = 0;
     bool have = false, done = false;
+    __shared__ float4 s_quads[kTraceThreads / 32][32];  // warp_test_cells' candidates, per warp
+    uint32_t chunk_next = 0, chunk_end = 0;  // warp-uniform: queue entries this warp has taken
     for (;;) {
         bool need = !have && !done;
         unsigned m = __ballot_sync(FULL, need);
         if (m) {
-            int leader = __ffs(m) - 1;
-            uint32_t base = 0;
-            if ((int)lane == leader) base = atomicAdd(fetch, (uint32_t)__popc(m));
-            base = __shfl_sync(FULL, base, leader);
+            const uint32_t rank = (uint32_t)__popc(m & ((1u << lane) - 1u));
+            // The needing lanes take the warp's next entries in lane order: what is left of its
+            // chunk first, then a new chunk (entries are handed out in increasing order, so once
+            // one is past the queue's end every later one is too).
+            const uint32_t want = (uint32_t)__popc(m), avail = chunk_end - chunk_next;
+            uint32_t q = chunk_next + rank;
+            if (avail < want) {
+                uint32_t base = 0;
+                if (lane == 0u) base = atomicAdd(fetch, kFetchChunk);
+                base = __shfl_sync(FULL, base, 0);
+                if (rank >= avail) q = base + (rank - avail);
+                chunk_next = base + (want - avail);
+                chunk_end = base + kFetchChunk;
+            } else {
+                chunk_next += want;
+            }
             if (need) {
-                uint32_t q = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
                 if (q >= count) {
                     done = true;
                 } else {
@@ -355,9 +374,9 @@ __global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevSce
         }
         if (__all_sync(FULL, done && !have)) break;
         if (__any_sync(FULL, done)) rounds++;  // the queue is dry: count the tail rounds
+        Hit h = no_hit();
+        const int r = trace_round_warp(S, P, ts, o, d, tmin, budget, have, h, s_quads[threadIdx.x >> 5]);
         if (have) {
-            Hit h = no_hit();
-            int r = trace_round(S, P, ts, o, d, tmin, budget, h);
             if (r != 0) {
                 if (r != 1) h = no_hit();
                 F.hit0[slot] = make_float4(h.t, __uint_as_float(h.quad), __uint_as_float(h.texel), h.s);
@@ -379,9 +398,9 @@ __global__ void __launch_bounds__(128, LW_WF_TRACE_MINB) k_wf_trace(const DevSce
 LaunchShape wf_trace_shape(int device) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_wf_trace, 128, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_wf_trace, kTraceThreads, 0);
     if (per_sm < 1) per_sm = 1;
-    return LaunchShape{sms * per_sm, 128};
+    return LaunchShape{sms * per_sm, kTraceThreads};
 }
 
 cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, uint32_t blocks,
