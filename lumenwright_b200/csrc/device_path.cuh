@@ -209,54 +209,46 @@ LW_DI Act on_emit(Path &p, const DevScene &S, const DevParams &P, const Hit &h, 
     return A_FACE_DONE;
 }
 
-// Runs the state machine from `act` until the lane needs a trace or its path ends.
+// Runs the state machine from `act` until the lane needs a trace or its path ends. The steps are
+// written in the order a lane meets them (the sun's light, the emitters, Russian roulette and the
+// next direction), each at most once per pass, so the lanes of a warp that are at different steps
+// run each step's code together as they fall through it; only the loop over emitters and faces
+// goes back.
 LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 val) {
     const float eps = P.misc_f.y;
     for (;;) {
-        switch (act) {
-        case A_TRACE:
-        case A_END:
-            return act;
-        case A_CONTINUE:
-            if (p.events >= MAX_EVENTS) return A_END;
-            p.kind = K_EXTEND;
-            p.tmax = kINF;
-            return A_TRACE;
-        case A_SUN_DONE:
+        if (act == A_SUN_DONE) {
             p.radiance = p.radiance + vmul(vmul(p.beta, f4v(P.sun_color)), p.tr) * p.cos_l;
             act = A_EMIT_START;
-            break;
-        case A_EMIT_START: {
+        }
+        if (act == A_EMIT_START) {
             // sample_emitters (integrator.rs:441-469).
             if (p.emode == 0u) {
                 act = A_FINISH_SURFACE;
-                break;
-            }
-            if (p.count == 0u) {
+            } else if (p.count == 0u) {
                 val = v3(0.0f, 0.0f, 0.0f);
                 act = A_EMIT_FINISH;
-                break;
-            }
-            const uint32_t *g = S.emitter_grid;
-            uint32_t start = p.list;
-            p.list = EMITTER_GRID_HEADER + ldg(g + 1) * ldg(g + 2) * ldg(g + 3) * 2u + start;
-            uint32_t strategy = strategy_of(P);
-            if (strategy == EMITTER_SAMPLING_ONE || strategy == EMITTER_SAMPLING_ONE_BLOCK) {
-                p.emode = E_SINGLE;
-                p.k = pick(p.count, rng_next(p.rng));
-                act = A_BEGIN_EMITTER;
-            } else if (strategy == EMITTER_SAMPLING_ALL) {
-                p.emode = E_ALL;
-                p.esum = v3(0.0f, 0.0f, 0.0f);
-                p.k = 0;
-                act = A_BEGIN_EMITTER;
             } else {
-                val = v3(0.0f, 0.0f, 0.0f);
-                act = A_EMIT_FINISH;
+                const uint32_t *g = S.emitter_grid;
+                uint32_t start = p.list;
+                p.list = EMITTER_GRID_HEADER + ldg(g + 1) * ldg(g + 2) * ldg(g + 3) * 2u + start;
+                uint32_t strategy = strategy_of(P);
+                if (strategy == EMITTER_SAMPLING_ONE || strategy == EMITTER_SAMPLING_ONE_BLOCK) {
+                    p.emode = E_SINGLE;
+                    p.k = pick(p.count, rng_next(p.rng));
+                    act = A_BEGIN_EMITTER;
+                } else if (strategy == EMITTER_SAMPLING_ALL) {
+                    p.emode = E_ALL;
+                    p.esum = v3(0.0f, 0.0f, 0.0f);
+                    p.k = 0;
+                    act = A_BEGIN_EMITTER;
+                } else {
+                    val = v3(0.0f, 0.0f, 0.0f);
+                    act = A_EMIT_FINISH;
+                }
             }
-            break;
         }
-        case A_BEGIN_EMITTER: {
+        if (act == A_BEGIN_EMITTER) {
             // sample_emitter (integrator.rs:419-433) for emitter list[k].
             uint32_t i = ldg(S.emitter_grid + p.list + p.k);
             float4 e0 = ldg(S.emitters + 2u * i);
@@ -267,20 +259,19 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
             if (p.faces == 0u) {
                 val = v3(0.0f, 0.0f, 0.0f);
                 act = A_EMITTER_DONE;
-                break;
-            }
-            if (P.emitter.x == EMITTER_SAMPLING_ONE) {
-                p.fmode = E_SINGLE;
-                p.f = pick(p.faces, rng_next(p.rng));
             } else {
-                p.fmode = E_ALL;
-                p.fsum = v3(0.0f, 0.0f, 0.0f);
-                p.f = 0;
+                if (P.emitter.x == EMITTER_SAMPLING_ONE) {
+                    p.fmode = E_SINGLE;
+                    p.f = pick(p.faces, rng_next(p.rng));
+                } else {
+                    p.fmode = E_ALL;
+                    p.fsum = v3(0.0f, 0.0f, 0.0f);
+                    p.f = 0;
+                }
+                act = A_START_FACE;
             }
-            act = A_START_FACE;
-            break;
         }
-        case A_START_FACE: {
+        if (act == A_START_FACE) {
             // sample_emitter_face (integrator.rs:381-401), up to its visibility trace.
             const DevQuad *q = S.quads + p.first + p.f;
             float s = rng_next(p.rng);
@@ -290,17 +281,17 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
             if (dot(to, p.n) <= 0.0f) {
                 val = v3(0.0f, 0.0f, 0.0f);
                 act = A_FACE_DONE;
-                break;
+            } else {
+                p.dist = vlength(to);
+                p.o = p.origin;
+                p.d = vdiv(to, p.dist);
+                p.tmin = eps;
+                p.tmax = p.dist + 2.0f * eps;
+                p.kind = K_EMIT;
+                return A_TRACE;
             }
-            p.dist = vlength(to);
-            p.o = p.origin;
-            p.d = vdiv(to, p.dist);
-            p.tmin = eps;
-            p.tmax = p.dist + 2.0f * eps;
-            p.kind = K_EMIT;
-            return A_TRACE;
         }
-        case A_FACE_DONE:
+        if (act == A_FACE_DONE) {
             if (p.fmode == E_SINGLE) {
                 act = A_EMITTER_DONE;
             } else {
@@ -313,8 +304,8 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
                     act = A_EMITTER_DONE;
                 }
             }
-            break;
-        case A_EMITTER_DONE:
+        }
+        if (act == A_EMITTER_DONE) {
             if (p.emode == E_SINGLE) {
                 val = val * kPI;
                 act = A_EMIT_FINISH;
@@ -328,12 +319,13 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
                     act = A_EMIT_FINISH;
                 }
             }
-            break;
-        case A_EMIT_FINISH:
+        }
+        if (act == A_START_FACE || act == A_BEGIN_EMITTER) continue;  // the next face or emitter
+        if (act == A_EMIT_FINISH) {
             p.radiance = p.radiance + vmul(p.beta, val);
             act = A_FINISH_SURFACE;
-            break;
-        case A_FINISH_SURFACE:
+        }
+        if (act == A_FINISH_SURFACE) {
             // integrator.rs:695-705.
             if (p.bounces >= 3u) {
                 float q_rr = clamp_r(max_elem(p.beta), 0.05f, 0.95f);
@@ -345,11 +337,16 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
             p.tmin = 0.0f;
             p.specular = false;
             act = A_CONTINUE;
-            break;
         }
+        if (act == A_CONTINUE) {
+            if (p.events >= MAX_EVENTS) return A_END;
+            p.kind = K_EXTEND;
+            p.tmax = kINF;
+            return A_TRACE;
+        }
+        return act;  // A_TRACE or A_END
     }
 }
-
 LW_DI Act shade(Path &p, const DevScene &S, const DevParams &P, const Hit &h) {
     V3 val = v3(0.0f, 0.0f, 0.0f);
     Act a;
