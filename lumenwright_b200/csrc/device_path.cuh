@@ -213,42 +213,45 @@ LW_DI Act on_emit(Path &p, const DevScene &S, const DevParams &P, const Hit &h, 
 // written in the order a lane meets them (the sun's light, the emitters, Russian roulette and the
 // next direction), each at most once per pass, so the lanes of a warp that are at different steps
 // run each step's code together as they fall through it; only the loop over emitters and faces
-// goes back.
+// goes back. A lane that is done (a ray to trace, or the path's end) falls through the remaining
+// steps rather than leaving early: one exit keeps the steps' code and registers shared.
 LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 val) {
     const float eps = P.misc_f.y;
-    for (;;) {
-        if (act == A_SUN_DONE) {
-            p.radiance = p.radiance + vmul(vmul(p.beta, f4v(P.sun_color)), p.tr) * p.cos_l;
-            act = A_EMIT_START;
-        }
-        if (act == A_EMIT_START) {
-            // sample_emitters (integrator.rs:441-469).
-            if (p.emode == 0u) {
-                act = A_FINISH_SURFACE;
-            } else if (p.count == 0u) {
+    bool done = act == A_TRACE || act == A_END;
+    Act out = act;
+    if (!done && act == A_SUN_DONE) {
+        p.radiance = p.radiance + vmul(vmul(p.beta, f4v(P.sun_color)), p.tr) * p.cos_l;
+        act = A_EMIT_START;
+    }
+    if (!done && act == A_EMIT_START) {
+        // sample_emitters (integrator.rs:441-469).
+        if (p.emode == 0u) {
+            act = A_FINISH_SURFACE;
+        } else if (p.count == 0u) {
+            val = v3(0.0f, 0.0f, 0.0f);
+            act = A_EMIT_FINISH;
+        } else {
+            const uint32_t *g = S.emitter_grid;
+            uint32_t start = p.list;
+            p.list = EMITTER_GRID_HEADER + ldg(g + 1) * ldg(g + 2) * ldg(g + 3) * 2u + start;
+            uint32_t strategy = strategy_of(P);
+            if (strategy == EMITTER_SAMPLING_ONE || strategy == EMITTER_SAMPLING_ONE_BLOCK) {
+                p.emode = E_SINGLE;
+                p.k = pick(p.count, rng_next(p.rng));
+                act = A_BEGIN_EMITTER;
+            } else if (strategy == EMITTER_SAMPLING_ALL) {
+                p.emode = E_ALL;
+                p.esum = v3(0.0f, 0.0f, 0.0f);
+                p.k = 0;
+                act = A_BEGIN_EMITTER;
+            } else {
                 val = v3(0.0f, 0.0f, 0.0f);
                 act = A_EMIT_FINISH;
-            } else {
-                const uint32_t *g = S.emitter_grid;
-                uint32_t start = p.list;
-                p.list = EMITTER_GRID_HEADER + ldg(g + 1) * ldg(g + 2) * ldg(g + 3) * 2u + start;
-                uint32_t strategy = strategy_of(P);
-                if (strategy == EMITTER_SAMPLING_ONE || strategy == EMITTER_SAMPLING_ONE_BLOCK) {
-                    p.emode = E_SINGLE;
-                    p.k = pick(p.count, rng_next(p.rng));
-                    act = A_BEGIN_EMITTER;
-                } else if (strategy == EMITTER_SAMPLING_ALL) {
-                    p.emode = E_ALL;
-                    p.esum = v3(0.0f, 0.0f, 0.0f);
-                    p.k = 0;
-                    act = A_BEGIN_EMITTER;
-                } else {
-                    val = v3(0.0f, 0.0f, 0.0f);
-                    act = A_EMIT_FINISH;
-                }
             }
         }
-        if (act == A_BEGIN_EMITTER) {
+    }
+    for (;;) {
+            if (!done && act == A_BEGIN_EMITTER) {
             // sample_emitter (integrator.rs:419-433) for emitter list[k].
             uint32_t i = ldg(S.emitter_grid + p.list + p.k);
             float4 e0 = ldg(S.emitters + 2u * i);
@@ -271,7 +274,7 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
                 act = A_START_FACE;
             }
         }
-        if (act == A_START_FACE) {
+            if (!done && act == A_START_FACE) {
             // sample_emitter_face (integrator.rs:381-401), up to its visibility trace.
             const DevQuad *q = S.quads + p.first + p.f;
             float s = rng_next(p.rng);
@@ -288,10 +291,11 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
                 p.tmin = eps;
                 p.tmax = p.dist + 2.0f * eps;
                 p.kind = K_EMIT;
-                return A_TRACE;
+                out = A_TRACE;
+                done = true;
             }
         }
-        if (act == A_FACE_DONE) {
+            if (!done && act == A_FACE_DONE) {
             if (p.fmode == E_SINGLE) {
                 act = A_EMITTER_DONE;
             } else {
@@ -305,7 +309,7 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
                 }
             }
         }
-        if (act == A_EMITTER_DONE) {
+            if (!done && act == A_EMITTER_DONE) {
             if (p.emode == E_SINGLE) {
                 val = val * kPI;
                 act = A_EMIT_FINISH;
@@ -320,39 +324,55 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
                 }
             }
         }
-        if (act == A_START_FACE || act == A_BEGIN_EMITTER) continue;  // the next face or emitter
-        if (act == A_EMIT_FINISH) {
-            p.radiance = p.radiance + vmul(p.beta, val);
-            act = A_FINISH_SURFACE;
+        const bool again = !done && (act == A_START_FACE || act == A_BEGIN_EMITTER);  // the next face or emitter
+        if (!again) break;
+    }
+    if (!done && act == A_EMIT_FINISH) {
+        p.radiance = p.radiance + vmul(p.beta, val);
+        act = A_FINISH_SURFACE;
+    }
+    if (!done && act == A_FINISH_SURFACE) {
+        // integrator.rs:695-705.
+        bool ends = false;
+        if (p.bounces >= 3u) {
+            float q_rr = clamp_r(max_elem(p.beta), 0.05f, 0.95f);
+            if (rng_next(p.rng) > q_rr) ends = true;
+            else p.beta = vdiv(p.beta, q_rr);
         }
-        if (act == A_FINISH_SURFACE) {
-            // integrator.rs:695-705.
-            if (p.bounces >= 3u) {
-                float q_rr = clamp_r(max_elem(p.beta), 0.05f, 0.95f);
-                if (rng_next(p.rng) > q_rr) return A_END;
-                p.beta = vdiv(p.beta, q_rr);
-            }
+        if (ends) {
+            out = A_END;
+            done = true;
+        } else {
             p.d = cosine_hemisphere(p.n, p.rng);
             p.o = p.origin;
             p.tmin = 0.0f;
             p.specular = false;
             act = A_CONTINUE;
         }
-        if (act == A_CONTINUE) {
-            if (p.events >= MAX_EVENTS) return A_END;
+    }
+    if (!done && act == A_CONTINUE) {
+        if (p.events >= MAX_EVENTS) {
+            out = A_END;
+        } else {
             p.kind = K_EXTEND;
             p.tmax = kINF;
-            return A_TRACE;
+            out = A_TRACE;
         }
-        return act;  // A_TRACE or A_END
+        done = true;
     }
+    return out;
 }
+
+// The result of the lane's last ray, by its kind (on_extend, on_shadow, on_emit).
+LW_DI Act on_result(Path &p, const DevScene &S, const DevParams &P, const Hit &h, V3 &val) {
+    if (p.kind == K_EXTEND) return on_extend(p, S, P, h);
+    if (p.kind == K_SHADOW) return on_shadow(p, S, P, h);
+    return on_emit(p, S, P, h, val);
+}
+
 LW_DI Act shade(Path &p, const DevScene &S, const DevParams &P, const Hit &h) {
     V3 val = v3(0.0f, 0.0f, 0.0f);
-    Act a;
-    if (p.kind == K_EXTEND) a = on_extend(p, S, P, h);
-    else if (p.kind == K_SHADOW) a = on_shadow(p, S, P, h);
-    else a = on_emit(p, S, P, h, val);
+    Act a = on_result(p, S, P, h, val);
     return advance(p, S, P, a, val);
 }
 

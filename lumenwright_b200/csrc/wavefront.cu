@@ -158,35 +158,42 @@ LW_DI ItemRef decode_item(const WorkDesc &W, const BatchDesc &B, uint32_t item) 
     return r;
 }
 
-// One shading step of slot i; its next ray goes to queue set `cur`.
+// One shading step of slot i (none when valid is false); its next ray goes to queue set `cur`.
+// Slots with nothing to shade (dead, or their ray still being traced) leave after the state
+// machine rather than before it, so the kernel has one exit.
 template <bool BATCH>
-LW_DI void shade_slot(uint32_t i, const DevScene &S0, const DevParams &P0, const WorkDesc &W, const BatchDesc &B,
-                      const WfState &F, uint32_t cur) {
-    float4 core = ld(F, W_CORE, i);
+LW_DI void shade_slot(bool valid, uint32_t i, const DevScene &S0, const DevParams &P0, const WorkDesc &W,
+                      const BatchDesc &B, const WfState &F, uint32_t cur) {
+    float4 core = valid ? ld(F, W_CORE, i) : u4(0u, 0u, 0u, F_DEAD);
     uint32_t flags = fu(core.w);
-    if (flags & F_DEAD) return;
+    bool live = !(flags & F_DEAD);
     // The item words: in the batched form the camera is needed at every step, otherwise only when
     // a sample ends.
-    float4 it2 = BATCH ? ld(F, W_ITEM2, i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 it2 = BATCH && live ? ld(F, W_ITEM2, i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     uint32_t job = BATCH ? fu(it2.z) : 0u;
+    DevScene S = S0;
+    if (BATCH) S.sky = B.jobs[job].sky;
+    const DevParams &P = BATCH ? B.jobs[job].P : P0;
     Path p;
     Act a = A_END;
-    if (flags & F_ACTIVE) {
+    bool part = false;
+    V3 val = v3(0.0f, 0.0f, 0.0f);
+    if (live && (flags & F_ACTIVE)) {
         float4 h0 = F.hit0[i];
-        if (fu(h0.y) == RESUME_MARK) return;  // its ray is still on its way: nothing to shade yet
-        float4 wo = ld(F, W_O, i), wd = ld(F, W_D, i), wr = ld(F, W_RAD, i), wb = ld(F, W_BETA, i);
-        float h1 = F.hit1[i];
-        unpack_core(p, wo, wd, wr, wb, core);
-        if (p.kind != K_EXTEND) load_nee(F, i, p);
-        Hit h{h0.x, fu(h0.y), fu(h0.z), h0.w, h1};
-        if (BATCH) {
-            DevScene S = S0;
-            S.sky = B.jobs[job].sky;
-            a = shade(p, S, B.jobs[job].P, h);
+        if (fu(h0.y) == RESUME_MARK) {
+            live = false;  // its ray is still on its way: nothing to shade yet
         } else {
-            a = shade(p, S0, P0, h);
+            float4 wo = ld(F, W_O, i), wd = ld(F, W_D, i), wr = ld(F, W_RAD, i), wb = ld(F, W_BETA, i);
+            float h1 = F.hit1[i];
+            unpack_core(p, wo, wd, wr, wb, core);
+            if (p.kind != K_EXTEND) load_nee(F, i, p);
+            Hit h{h0.x, fu(h0.y), fu(h0.z), h0.w, h1};
+            a = on_result(p, S, P, h, val);
+            part = true;
         }
     }
+    if (part) a = advance(p, S, P, a, val);
+    if (!live) return;
     if (a == A_END) {
         // The sample is over: the item's sums, then its next sample or the next item.
         if (!BATCH) it2 = ld(F, W_ITEM2, i);
@@ -257,7 +264,7 @@ LW_DI void shade_slot(uint32_t i, const DevScene &S0, const DevParams &P0, const
 // (t - 1) % 3 and clears set (t + 1) % 3 for the next iteration. The iteration is the device word
 // ctr[12], advanced by k_wf_advance after each trace.
 #ifndef LW_WF_SHADE_MINB
-#define LW_WF_SHADE_MINB 5
+#define LW_WF_SHADE_MINB 6
 #endif
 template <bool BATCH>
 __global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
@@ -276,7 +283,7 @@ __global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevSce
     const uint32_t n = dense ? F.n : queued;
     const uint32_t *list = F.queue + (size_t)prev * F.n;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;  // the grid covers every slot
-    if (k < n) shade_slot<BATCH>(dense ? k : list[k], S0, P0, W, B, F, cur);
+    shade_slot<BATCH>(k < n, k < n ? (dense ? k : list[k]) : 0u, S0, P0, W, B, F, cur);
 }
 
 // The end of an iteration: the next iteration's number; in a graph, whether to run another one (the
