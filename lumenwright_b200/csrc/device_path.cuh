@@ -74,20 +74,24 @@ LW_DI Act on_extend(Path &p, const DevScene &S, const DevParams &P, Hit h) {
     uint32_t flags = 0u;
     V3 pos = v3(0.0f, 0.0f, 0.0f), albedo = pos, n = pos;
     float alpha = 0.0f, qemit = 0.0f;
+    // One exit: a lane that is done (the sky, water, a translucent pass, the last bounce) falls
+    // through the remaining steps.
+    Act act = A_EMIT_START;
+    bool done = false;
     if (water_plane(P, p.o, p.d, tp) && (!found || tp < h.t)) {
         if (p.in_water) p.beta = vmul(p.beta, transmittance(sigma, tp));
         wfront = p.d.y < 0.0f;
         wn = v3(0.0f, wfront ? 1.0f : -1.0f, 0.0f);
         wpos = p.o + p.d * tp;
         water = true;
-    } else {
-        if (!found) {
-            if (!p.in_water && !under_water_plane(P, p.o, p.d)) {
-                p.radiance = p.radiance + vmul(p.beta, sky_of(S, P, p.d, p.bounces == 0));
-                if (p.specular && p.bounces == 0) p.radiance = p.radiance + vmul(p.beta, sun_texture(S, P, p.d));
-            }
-            return A_END;
+    } else if (!found) {
+        if (!p.in_water && !under_water_plane(P, p.o, p.d)) {
+            p.radiance = p.radiance + vmul(p.beta, sky_of(S, P, p.d, p.bounces == 0));
+            if (p.specular && p.bounces == 0) p.radiance = p.radiance + vmul(p.beta, sun_texture(S, P, p.d));
         }
+        act = A_END;
+        done = true;
+    } else {
         if (p.in_water) p.beta = vmul(p.beta, transmittance(sigma, h.t));
         const DevQuad *q = S.quads + h.quad;
         float4 qn = ldg(&q->n_nn);
@@ -118,52 +122,59 @@ LW_DI Act on_extend(Path &p, const DevScene &S, const DevParams &P, Hit h) {
         p.o = no;
         p.specular = true;
         p.tmin = 0.0f;
-        return A_CONTINUE;
+        act = A_CONTINUE;
+        done = true;
     }
-    if (!forced && (flags & FLAG_ALPHA_MASK) == ALPHA_TRANSLUCENT && rng_next(p.rng) >= alpha) {
+    if (!done && !forced && (flags & FLAG_ALPHA_MASK) == ALPHA_TRANSLUCENT && rng_next(p.rng) >= alpha) {
         p.beta = vmul(p.beta, lerp(v3(1.0f, 1.0f, 1.0f), albedo, alpha));
         p.o = pos + p.d * eps;
         p.tmin = 0.0f;
-        return A_CONTINUE;
+        act = A_CONTINUE;
+        done = true;
     }
-    if (p.bounces >= P.frame.w) return A_END;
-    const uint32_t strategy = strategy_of(P);
-    float emittance = qemit * P.misc_f.x;
-    bool emits = emittance > 0.0f && (P.emitter.y == 0u || strategy == EMITTER_SAMPLING_NONE || p.bounces == 0u);
-    if (emits) p.radiance = p.radiance + vmul(p.beta, vmul(albedo, albedo)) * emittance;
-    p.bounces += 1;
-
-    p.n = n;
-    p.origin = pos + n * eps;
-    // beta.mul(albedo), the factor of the sun and emitter terms and the path's next beta.
-    p.beta = vmul(p.beta, albedo);
-    if (!emits && strategy != EMITTER_SAMPLING_NONE) {
-        emitter_cell(S, pos, p.list, p.count);  // no draw: evaluated here, used after the sun
-        p.emode = 1u;                           // emitters to sample
-    } else {
-        p.emode = 0u;
+    if (!done && p.bounces >= P.frame.w) {
+        act = A_END;
+        done = true;
     }
+    if (!done) {
+        const uint32_t strategy = strategy_of(P);
+        float emittance = qemit * P.misc_f.x;
+        bool emits = emittance > 0.0f && (P.emitter.y == 0u || strategy == EMITTER_SAMPLING_NONE || p.bounces == 0u);
+        if (emits) p.radiance = p.radiance + vmul(p.beta, vmul(albedo, albedo)) * emittance;
+        p.bounces += 1;
 
-    V3 sun = f4v(P.sun_dir);
-    float sin_r = __fsqrt_rn(fmax_r(1.0f - P.sun_dir.w * P.sun_dir.w, 0.0f));
-    bool lit = P.sun_color.x > 0.0f || P.sun_color.y > 0.0f || P.sun_color.z > 0.0f;
-    if (lit && dot(n, sun) > -sin_r && P.sun_dir.y > -sin_r) {
-        V3 l = sample_sun(P, p.rng);
-        float cos_l = dot(n, l);
-        if (cos_l > 0.0f && l.y >= 0.0f) {
-            // shadow (integrator.rs:319-346): the first segment.
-            p.cos_l = cos_l;
-            p.tr = v3(1.0f, 1.0f, 1.0f);
-            p.seg = 0;
-            p.o = p.origin;
-            p.d = l;
-            p.tmin = eps;
-            p.tmax = kINF;
-            p.kind = K_SHADOW;
-            return A_TRACE;
+        p.n = n;
+        p.origin = pos + n * eps;
+        // beta.mul(albedo), the factor of the sun and emitter terms and the path's next beta.
+        p.beta = vmul(p.beta, albedo);
+        if (!emits && strategy != EMITTER_SAMPLING_NONE) {
+            emitter_cell(S, pos, p.list, p.count);  // no draw: evaluated here, used after the sun
+            p.emode = 1u;                           // emitters to sample
+        } else {
+            p.emode = 0u;
+        }
+
+        V3 sun = f4v(P.sun_dir);
+        float sin_r = __fsqrt_rn(fmax_r(1.0f - P.sun_dir.w * P.sun_dir.w, 0.0f));
+        bool lit = P.sun_color.x > 0.0f || P.sun_color.y > 0.0f || P.sun_color.z > 0.0f;
+        if (lit && dot(n, sun) > -sin_r && P.sun_dir.y > -sin_r) {
+            V3 l = sample_sun(P, p.rng);
+            float cos_l = dot(n, l);
+            if (cos_l > 0.0f && l.y >= 0.0f) {
+                // shadow (integrator.rs:319-346): the first segment.
+                p.cos_l = cos_l;
+                p.tr = v3(1.0f, 1.0f, 1.0f);
+                p.seg = 0;
+                p.o = p.origin;
+                p.d = l;
+                p.tmin = eps;
+                p.tmax = kINF;
+                p.kind = K_SHADOW;
+                act = A_TRACE;
+            }
         }
     }
-    return A_EMIT_START;
+    return act;
 }
 
 // A shadow segment's result (integrator.rs:322-345).
