@@ -382,7 +382,7 @@ void reset_stats(lw_ctx *c) {
 // their last long traversals weigh less, at 328 bytes of device memory per slot.
 lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const WorkDesc &W) {
     const uint32_t n = wf_slots(c, (uint64_t)W.w * W.h * W.spp, W.n_items);
-    const uint32_t budget = c->tuning.budget ? c->tuning.budget : 4u;
+    const uint32_t budget = c->tuning.budget ? c->tuning.budget : kWfBudget;
     WfState F;
     lw_status s = wf_setup(c, c->wf, n, F, c->stream);
     if (s != LW_OK) return s;
@@ -476,7 +476,7 @@ lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32
 // iteration had rays to trace, all decided on the device; then the per-camera reduction.
 lw_status batch_graph_wavefront(lw_ctx *c, const BatchDesc &B, const DevParams &P0, uint64_t pixels, uint32_t slots) {
     if (!c->cap) CK(c, cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking), "creating a capture stream");
-    const uint32_t budget = c->tuning.budget ? c->tuning.budget : 4u;
+    const uint32_t budget = c->tuning.budget ? c->tuning.budget : kWfBudget;
     // The buffers first (cleared outside the graph too, which is harmless).
     WfState F;
     lw_status s = wf_setup(c, c->bwf, slots, F, c->stream);

@@ -93,6 +93,9 @@ struct WfState {
                       // iteration; [14..15]: rays traced (64-bit, 8-byte aligned)
     float4 *ts;       // 3 float4 per slot (word k at ts[k * n + i]): a carried-over traversal
 };
+// Visits through empty space per round of the wavefront's tracing kernel when the tuning leaves it
+// at 0 (5: +1 % over 4 at c2 and c4; 6 gives the same).
+constexpr uint32_t kWfBudget = 5u;
 LaunchShape wf_trace_shape(int device);
 cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, uint32_t blocks,
                             cudaStream_t st);

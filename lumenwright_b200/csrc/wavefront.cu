@@ -426,7 +426,7 @@ cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const 
 
 cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState &F, LaunchShape trace_shape,
                             uint32_t budget, uint32_t tail, cudaStream_t st) {
-    if (budget == 0u) budget = 4u;  // a round makes at least one visit
+    if (budget == 0u) budget = kWfBudget;  // a round makes at least one visit
     k_wf_trace<<<trace_shape.blocks, trace_shape.threads, 0, st>>>(S, P, F, budget, tail);
     return cudaGetLastError();
 }
