@@ -120,14 +120,17 @@ typedef struct {
  * engine: how lw_render_hq / lw_render_device run: LW_ENGINE_WAVEFRONT (the default) keeps each
  *   path in a slot of a pool in device memory and alternates a shading kernel with a tracing kernel
  *   whose lanes take the next queued ray as soon as theirs ends; LW_ENGINE_MEGAKERNEL runs one
- *   persistent kernel in which each lane follows its own paths. Both give the same image, bit for
- *   bit. The batched form runs the engine named here too (the wavefront as one CUDA graph); the
+ *   persistent kernel in which each lane follows its own paths. For the same samples per work
+ *   item (sub) both give the same image, bit for bit; left at 0, sub is 1 for the wavefront and
+ *   chosen from the frame for the megakernel, so the images then differ by the rounding of the
+ *   item sums. The batched form runs the engine named here too (the wavefront as one CUDA graph); the
  *   per-sample entry point and lw_render_accumulate_noalloc always run the megakernel.
  * threads: threads per block of the megakernel (64, 128 or 256).
  * budget: voxel visits a ray advances before its lane may take up other work: the megakernel's
  *   regrouping period (0 = a whole traversal at once), the wavefront's visits through empty
  *   space per round, between queue fetches (0 = 5).
- * sub: samples per work item (0: chosen from the frame so every lane gets many items).
+ * sub: samples per work item (0: one for the wavefront; for the megakernel and the batched form
+ *   chosen from the frame so every lane gets many items).
  * paths: path slots of the wavefront (0: sized from each launch's sample count, 2^16 to 2^23). */
 #define LW_ENGINE_WAVEFRONT 0u
 #define LW_ENGINE_MEGAKERNEL 1u
