@@ -102,12 +102,12 @@ class Autotuner:
     Candidates: the wavefront engine with queue depth (path slots) {automatic, 2^22, 2^23} x visits
     between queue fetches {4, 8}, and the persistent megakernel with threads per block {64, 128,
     256} x regrouping period {0 (whole traversals), 24}; each with samples per work item
-    {automatic, 16}. A trial renders the workload with every camera's spp cut to
+    {automatic, 4}. A trial renders the workload with every camera's spp cut to
     ``trial_fraction`` of it (at least 1). The winner is cached per workload class (the rounded
     totals of pixels and samples and the bounce range) in ``$LUMENWRIGHT_CACHE/autotune.json``
     (default ``~/.cache/lumenwright_b200``)."""
 
-    SUBS = (0, 16)
+    SUBS = (0, 4)
 
     @classmethod
     def candidates(cls):
