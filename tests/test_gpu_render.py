@@ -97,3 +97,16 @@ def test_wavefront_and_megakernel_give_the_same_image(ctx, c2, paths):
     got = ctx.render_hq(p, c2.sky, 12)
     ctx.set_tuning(engine=ENGINE_WAVEFRONT, paths=0, sub=0)
     assert np.array_equal(got, want)
+
+
+def test_wavefront_default_items_are_one_sample(ctx, c2):
+    # Left at 0, the wavefront's samples per item is one; the megakernel given one sample per item
+    # takes the same items in the same order of additions, so the images are equal bit for bit.
+    from lumenwright_b200.native import ENGINE_MEGAKERNEL, ENGINE_WAVEFRONT
+    p = c2.params
+    ctx.upload_hq_scene(c2.scene)
+    ctx.set_tuning(engine=ENGINE_MEGAKERNEL, sub=1)
+    want = ctx.render_hq(p, c2.sky, 6)
+    ctx.set_tuning(engine=ENGINE_WAVEFRONT, sub=0, paths=0)
+    got = ctx.render_hq(p, c2.sky, 6)
+    assert np.array_equal(got, want)
