@@ -96,7 +96,16 @@ def algorithmic_bytes(path):
         return json.load(f)
 
 
-def cpu_baseline(frame, budget_s=18.0):
+def torch_sm_count(device):
+    """The GPU's SM count (148 on a B200)."""
+    try:
+        import torch
+        return torch.cuda.get_device_properties(device).multi_processor_count
+    except Exception:
+        return None
+
+
+def cpu_baseline(frame, budget_s=12.0):
     """The CPU oracle (the reference's kernel and CPU backend loop, restated in C, f64 sums per
     pixel, OpenMP over rows) on all host cores, on full rows spread over the frame at the frame's
     spp cut to at most 64, with as many rows (at least 24) as fill about `budget_s` seconds."""
@@ -404,8 +413,18 @@ def main():
         # DRAM traffic per launch: the ncu capture's bytes per traced ray times this run's rays per
         # tracing launch.
         with open(os.path.join(ROOT, "profiles", "k_wf_trace_traffic_c2.json")) as f:
-            per_ray = json.load(f)["dram_bytes_per_ray"]
+            capture = json.load(f)
+        per_ray = capture["dram_bytes_per_ray"]
         traffic = per_ray * rays / max(1, trace_launches)
+        # The bound the tracing kernel actually meets is instruction issue (the scene is L1/L2
+        # resident): warp instructions per traced ray from the same capture, times this run's rays,
+        # over the kernel's event time, against one instruction per scheduler per cycle (4 per SM)
+        # at the SM clock sampled during the timed steps.
+        clk = clocks.summary()
+        sms = torch_sm_count(local)
+        issue_peak = sms * 4 * (clk.get("sm_mhz") or 0) / 1e3 if clk and sms else None
+        issue = (capture["warp_instructions_per_ray"] * rays / (trace_ms / 1e3) / 1e9
+                 if trace_ms > 0 and "warp_instructions_per_ray" in capture else None)
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
@@ -427,7 +446,12 @@ def main():
                          "algorithmic_bytes_per_launch": trace_bytes / max(1, trace_launches),
                          "avg_launch_ms": trace_ms / max(1, trace_launches),
                          "trace_bytes_per_sample": alg["trace_bytes_per_sample"]},
-            "clocks": clocks.summary(),
+            "roofline_issue": {"bound": "issue", "kernel": "k_wf_trace", "achieved": issue, "peak": issue_peak,
+                               "unit": "G warp instructions/s",
+                               "frac": issue / issue_peak if issue and issue_peak else None,
+                               "peak_kind": f"nominal: {sms} SMs x 4 schedulers x the sampled SM clock",
+                               "instructions": "ncu warp instructions per traced ray x rays"},
+            "clocks": clk,
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(frame)
