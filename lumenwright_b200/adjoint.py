@@ -147,6 +147,7 @@ class DiffProblem:
                  world_seed=1, target_seed=5, sigma=0.05, eye=(32.0, 100.0, 32.0), look=(0.0, 64.0, 0.0)):
         from .native import gamma_table
         self.ctx = ctx
+        self._pool = None  # the host thread gradient() computes the sky Jacobian on
         self.width, self.height, self.spp, self.bounces = width, height, spp, bounces
         world = S.generate_world(chunks, world_seed, emitters=True)
         atlas = S.build_atlas(world_seed)
@@ -188,13 +189,19 @@ class DiffProblem:
         return float(np.sum((image - self.target) ** 2))
 
     def gradient(self, theta):
-        """(loss, d loss / d theta) at theta by the adjoint."""
+        """(loss, d loss / d theta) at theta by the adjoint. The sky cache's Jacobian is computed on
+        a host thread while the device runs the forward and backward passes (the library's calls
+        release the interpreter lock)."""
         args = self._args(theta)
-        image = self.ctx.adjoint_forward(*args, self.spp)
-        g = self.ctx.adjoint_backward(*args, self.spp, 2.0 * (image - self.target))
         sp = split(theta)
         az, alt, tb = sp.sky
-        j_cache = sky_cache_jacobian(az, alt, tb)
+        if self._pool is None:
+            from concurrent.futures import ThreadPoolExecutor
+            self._pool = ThreadPoolExecutor(max_workers=1)
+        job = self._pool.submit(sky_cache_jacobian, az, alt, tb)
+        image = self.ctx.adjoint_forward(*args, self.spp)
+        g = self.ctx.adjoint_backward(*args, self.spp, 2.0 * (image - self.target))
+        j_cache = job.result()
         g_sky = g["sky"][:j_cache.shape[0]] @ j_cache
         g_sky[:2] += g["sun_dir"] @ sun_vector_jacobian(az, alt)
         out = np.concatenate([g["albedo"].ravel(), g["emitter_scale"], g_sky])
