@@ -1042,9 +1042,13 @@ lw_status lw_batch_prepare(lw_ctx *c, const lw_camera_job *jobs, uint32_t n) {
     // Layout: items, slots, accumulators, images, item sums.
     uint64_t total_samples = 0;
     for (uint32_t i = 0; i < n; i++) total_samples += (uint64_t)jobs[i].params.frame[0] * jobs[i].params.frame[1] * jobs[i].spp;
-    // Samples per item: as few as keep the item sums (16 B each, one launch) within 40 GiB; one
-    // sample per item drains the pool fastest (the 64-camera workload: +7 % over 9 per item).
-    const uint64_t max_items = (40ull << 30) / sizeof(float4);
+    // Samples per item: as few as keep the item sums (16 B each, one launch) within 40 GiB and a
+    // third of the device memory free now; one sample per item drains the pool fastest (the
+    // 64-camera workload: +7 % over 9 per item).
+    size_t free_b = 0, total_b = 0;
+    uint64_t sums_cap = 40ull << 30;
+    if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b / 3 < sums_cap) sums_cap = free_b / 3;
+    const uint64_t max_items = sums_cap / sizeof(float4) > 0 ? sums_cap / sizeof(float4) : 1;
     uint64_t sub = (total_samples + max_items - 1) / max_items;
     sub = sub < 1 ? 1 : (sub > 64 ? 64 : sub);
     if (c->tuning.sub) sub = c->tuning.sub;
