@@ -18,6 +18,12 @@ namespace {
 // Queue entries a warp takes from the fetch counter at a time (one atomic per 32 rays, not per
 // round); at least 32, the most a warp can need at once.
 constexpr uint32_t kFetchChunk = 32u;
+// Lanes of a warp without a ray take new ones once at least this many of them wait (or no lane has
+// work left): fewer fetch phases, each with more lanes (-1 % tracing time at c2 and c4; 16 is
+// slower).
+#ifndef LW_FETCH_MIN
+#define LW_FETCH_MIN 8
+#endif
 constexpr int kTraceThreads = 128;  // threads per block of the tracing kernel
 
 enum : uint32_t { F_ACTIVE = 1u, F_DEAD = 2u };
@@ -330,6 +336,12 @@ __global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(co
     for (;;) {
         bool need = !have && !done;
         unsigned m = __ballot_sync(FULL, need);
+#if LW_FETCH_MIN > 1
+        if (__popc(m) < LW_FETCH_MIN && __any_sync(FULL, have)) {
+            m = 0u;
+            need = false;
+        }
+#endif
         if (m) {
             const uint32_t rank = (uint32_t)__popc(m & ((1u << lane) - 1u));
             // The needing lanes take the warp's next entries in lane order: what is left of its
