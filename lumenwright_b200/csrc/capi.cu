@@ -68,6 +68,7 @@ struct lw_ctx {
     // scene
     bool has_scene = false;
     uint32_t dims[3] = {}, offsets[5] = {}, atlas_size[2] = {};
+    uint32_t sky_brick_y = 0;  // DevScene::sky_brick_y of the uploaded scene
     uint32_t nb = 0, n_bricks = 0, n_ov_bricks = 0;
     DBuf<uint32_t> grid, atlas, egrid;
     DBuf<uint2> top, occ;
@@ -204,6 +205,7 @@ DevScene dev_scene(const lw_ctx *c) {
     S.emitter_grid = c->egrid.p;
     S.sky = c->sky.p;
     S.gamma = c->gamma.p;
+    S.sky_brick_y = c->sky_brick_y;
     return S;
 }
 
@@ -789,6 +791,16 @@ lw_status install_scene(lw_ctx *c, const lw_scene_desc *d, uint32_t n_bricks, ui
     CK(c, cudaStreamSynchronize(c->stream), "uploading the scene");
     if (err & 1u) return fail(c, LW_ERR_BUFFER_LENGTH, "a top-level entry names a brick, model or overlay brick out of range");
     if (err & 2u) return fail(c, LW_ERR_BUFFER_LENGTH, "a voxel names a model out of range");
+    // The lowest brick row with nothing at or above it (bricks of the top level are (y, z, x)-major).
+    {
+        std::vector<uint2> top(nb);
+        CK(c, cudaMemcpy(top.data(), c->top.p, nb * sizeof(uint2), cudaMemcpyDeviceToHost), "reading the top level");
+        const uint64_t row = (uint64_t)d->dims[0] * d->dims[2];
+        uint32_t sky_y = 0;
+        for (uint64_t b = 0; b < nb; b++)
+            if (top[b].x != 0xFFFFFFFFu || top[b].y != 0xFFFFFFFFu) sky_y = (uint32_t)(b / row) + 1u;
+        c->sky_brick_y = sky_y;
+    }
     std::memcpy(c->dims, d->dims, sizeof c->dims);
     std::memcpy(c->offsets, d->offsets, sizeof c->offsets);
     std::memcpy(c->atlas_size, d->atlas_size, sizeof c->atlas_size);

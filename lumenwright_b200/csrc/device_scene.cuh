@@ -71,6 +71,9 @@ struct DevScene {
     const uint32_t *emitter_grid;
     const float *sky;
     const float *gamma;
+    // The lowest brick row above which every brick is empty (no block, no overlay): a ray in an
+    // empty brick at or above it that does not go down meets nothing more.
+    uint32_t sky_brick_y;
 };
 
 template <typename T>
@@ -340,6 +343,10 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
     }
     const V3 inv = ts.inv;
     if (bc.entry == EMPTY && bc.ov == EMPTY) {
+        // Above the last row with anything in it, a ray that does not go down stays in empty
+        // bricks until it leaves the grid: the reference's loop skips them one by one and ends
+        // without a hit, which is the result here at once.
+        if (R.s1 >= 0 && by >= S.sky_brick_y) return -1;
         // Skip the whole brick: jump to its exit face (trace.rs:184-226).
         int bc0 = (int)bx, bc1 = (int)by, bc2 = (int)bz;
         float t_out = kINF;
