@@ -36,9 +36,6 @@ constexpr uint32_t MAX_EVENTS = 48u;    // integrator.rs:24
 constexpr uint32_t NO_QUAD = 0xFFFFFFFFu;
 constexpr float COPLANAR = 1e-5f;       // trace.rs:73
 
-#ifndef LW_SUBBLOCK_SKIP
-#define LW_SUBBLOCK_SKIP 0
-#endif
 
 struct __align__(16) DevQuad {
     float4 n_nn;      // n = eu x ev, w = n . n
@@ -202,66 +199,6 @@ LW_DI bool dda_advance(Dda &s, V3 o, V3 inv, int s0, int s1, int s2, int gs0, in
     return true;
 }
 
-// Number of boundaries the DDA crosses along one axis from cell `c` before the crossing at `t_exit`
-// on the exit axis, at most `max_k`: crossing times (k - o) * inv (next_boundary) below t_exit, or
-// equal to it when this axis comes first in the DDA's tie rule (the higher axis index).
-LW_DI int crossings_before(int c, int max_k, float o, float inv, int st, float t_exit, bool first_on_tie) {
-    int k = 0;
-    for (int j = 0; j < max_k; j++) {
-        float tb = next_boundary(o, inv, c + j * st, st);
-        if (tb < t_exit || (tb == t_exit && first_on_tie)) k++;
-        else break;
-    }
-    return k;
-}
-
-// The DDA leaving an empty 4^3 sub-block (no voxel with a model, no overlay in the brick), in one
-// go. Stepping it voxel by voxel (trace.rs:267-287) takes the crossings of all three axes in the
-// order of their distances, ties to the higher axis; none of the voxels tests a quad. So the ray
-// leaves the sub-block through the face whose crossing comes first in that order, at exactly the
-// distance next_boundary gives for the last cell before that face, and on each other axis it has
-// crossed the boundaries that come before it in the same order. The resulting cell, distance and
-// next boundaries are the ones the voxel-by-voxel DDA reaches, bit for bit; the visits skipped are
-// counted towards MAX_STEPS. Returns -1 when the reference's loop would end inside (the range ends,
-// the grid is left, or the step budget runs out), 0 otherwise.
-LW_DI int skip_empty_sub_block(Dda &s, V3 o, V3 inv, int s0, int s1, int s2, int gs0, int gs1, int gs2, float t_end,
-                               uint32_t &it) {
-    const int b0 = s.c0 & ~3, b1 = s.c1 & ~3, b2 = s.c2 & ~3;
-    const int l0 = s0 > 0 ? b0 + 3 : b0, l1 = s1 > 0 ? b1 + 3 : b1, l2 = s2 > 0 ? b2 + 3 : b2;
-    float f0 = next_boundary(o.x, inv.x, l0, s0);
-    float f1 = next_boundary(o.y, inv.y, l1, s1);
-    float f2 = next_boundary(o.z, inv.z, l2, s2);
-    int axis = f0 < f1 ? (f0 < f2 ? 0 : 2) : (f1 < f2 ? 1 : 2);
-    float t_exit = axis == 0 ? f0 : (axis == 1 ? f1 : f2);
-    if (t_exit > t_end) return -1;
-    // Interior crossings: every one on the exit axis, and those before t_exit on the others.
-    int m0 = s0 == 0 ? 0 : (s0 > 0 ? l0 - s.c0 : s.c0 - l0);
-    int m1 = s1 == 0 ? 0 : (s1 > 0 ? l1 - s.c1 : s.c1 - l1);
-    int m2 = s2 == 0 ? 0 : (s2 > 0 ? l2 - s.c2 : s.c2 - l2);
-    int k0 = axis == 0 ? m0 : crossings_before(s.c0, m0, o.x, inv.x, s0, t_exit, 0 > axis);
-    int k1 = axis == 1 ? m1 : crossings_before(s.c1, m1, o.y, inv.y, s1, t_exit, 1 > axis);
-    int k2 = axis == 2 ? m2 : crossings_before(s.c2, m2, o.z, inv.z, s2, t_exit, 2 > axis);
-    uint32_t visits = (uint32_t)(k0 + k1 + k2);
-    if (it + visits > MAX_STEPS) return -1;
-    it += visits;
-    int n0c = s.c0 + k0 * s0, n1c = s.c1 + k1 * s1, n2c = s.c2 + k2 * s2;
-    // The exit crossing itself.
-    if (axis == 0) n0c += s0;
-    else if (axis == 1) n1c += s1;
-    else n2c += s2;
-    int ca = axis == 0 ? n0c : (axis == 1 ? n1c : n2c);
-    int ga = axis == 0 ? gs0 : (axis == 1 ? gs1 : gs2);
-    if (ca < 0 || ca >= ga) return -1;
-    s.c0 = n0c;
-    s.c1 = n1c;
-    s.c2 = n2c;
-    s.n0 = next_boundary(o.x, inv.x, n0c, s0);
-    s.n1 = next_boundary(o.y, inv.y, n1c, s1);
-    s.n2 = next_boundary(o.z, inv.z, n2c, s2);
-    s.t = t_exit;
-    return 0;
-}
-
 // The state of a traversal between two calls of trace_run: the DDA, the inverse direction, the
 // end of the range and the visit count. Everything else (the signs of the direction, the brick
 // cached in registers) is derived again when the traversal resumes.
@@ -322,8 +259,7 @@ LW_DI RayDda ray_dda(const DevParams &P, V3 d) {
 // brick or voxel, 1 when the cell has quads to test: its model in `model`, its brick's overlay
 // entry in bc.ov; the DDA then stays in that cell.
 //  * A voxel in an empty 4^3 sub-block of a brick without overlay is not read (its model is 0, it
-//    tests no quad); with LW_SUBBLOCK_SKIP the rest of that sub-block is crossed in one step
-//    (skip_empty_sub_block).
+//    tests no quad).
 //  * Every visit (brick skip, empty voxel, voxel with quads) counts towards MAX_STEPS as one
 //    iteration of the reference's loop does.
 LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, const RayDda &R, BrickCache &bc,
@@ -386,12 +322,7 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
             int lx = s.c0 & 15, ly = s.c1 & 15, lz = s.c2 & 15;
             uint32_t sb = (uint32_t)(((ly >> 2) * 4 + (lz >> 2)) * 4 + (lx >> 2));
             uint32_t word = sb < 32u ? bc.occ.x : bc.occ.y;
-            if ((word >> (sb & 31u)) & 1u) {
-                model = brick_voxel(S, bc.entry, lx, ly, lz);
-            } else if (LW_SUBBLOCK_SKIP && bc.ov == EMPTY) {
-                // An empty 4^3 sub-block: go to where the DDA would leave it.
-                return skip_empty_sub_block(s, o, inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end, ts.it) < 0 ? -1 : 0;
-            }
+            if ((word >> (sb & 31u)) & 1u) model = brick_voxel(S, bc.entry, lx, ly, lz);
         }
     }
     if (model != 0u || bc.ov != EMPTY) return 1;
