@@ -317,7 +317,7 @@ lw_status wf_setup(lw_ctx *c, lw_ctx::WfBufs &b, uint32_t n, WfState &F, cudaStr
 }
 
 // Blocks of the shading kernel: one thread per slot.
-uint32_t wf_shade_blocks(const lw_ctx *, uint32_t n) { return (n + 127u) / 128u; }
+uint32_t wf_shade_blocks(const lw_ctx *, uint32_t n) { return (n + kShadeThreads - 1u) / kShadeThreads; }
 
 // Path slots for a render of `samples` samples in `items` work items: one per 16 samples, a power
 // of two from 2^16 to 2^23, no more than the items (or the tuning's count).

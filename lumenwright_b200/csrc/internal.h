@@ -96,6 +96,11 @@ struct WfState {
 // Visits through empty space per round of the wavefront's tracing kernel when the tuning leaves it
 // at 0 (5: +1 % over 4 at c2 and c4; 6 gives the same).
 constexpr uint32_t kWfBudget = 5u;
+#ifndef LW_SHADE_THREADS
+#define LW_SHADE_THREADS 256
+#endif
+// Threads per block of the shading kernel (256: shading -2.6 % against 128 at c2; 64 is slower).
+constexpr uint32_t kShadeThreads = LW_SHADE_THREADS;
 LaunchShape wf_trace_shape(int device);
 cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, uint32_t blocks,
                             cudaStream_t st);

@@ -269,11 +269,12 @@ LW_DI void shade_slot(bool valid, uint32_t i, const DevScene &S0, const DevParam
 // the rays the tracing of iteration t - 1 carried over; the shading of iteration t reads set
 // (t - 1) % 3 and clears set (t + 1) % 3 for the next iteration. The iteration is the device word
 // ctr[12], advanced by k_wf_advance after each trace.
+// Blocks of 128 threads' worth per SM the shading kernel must fit: 6, so 80 registers a thread.
 #ifndef LW_WF_SHADE_MINB
 #define LW_WF_SHADE_MINB 6
 #endif
 template <bool BATCH>
-__global__ void __launch_bounds__(128, LW_WF_SHADE_MINB) k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
+__global__ void __launch_bounds__(kShadeThreads, LW_WF_SHADE_MINB * 128 / kShadeThreads) k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
                                                   const BatchDesc B, const WfState F) {
     const uint32_t t = *(volatile uint32_t *)&F.ctr[12];
     const uint32_t cur = t % 3u, prev = (t + 2u) % 3u, next = (t + 1u) % 3u;
@@ -425,14 +426,14 @@ LaunchShape wf_trace_shape(int device) {
 cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, uint32_t blocks,
                             cudaStream_t st) {
     BatchDesc none{};
-    k_wf_shade<false><<<blocks, 128, 0, st>>>(S, P, W, none, F);
+    k_wf_shade<false><<<blocks, kShadeThreads, 0, st>>>(S, P, W, none, F);
     return cudaGetLastError();
 }
 
 cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const BatchDesc &B, const WfState &F,
                                   uint32_t blocks, cudaStream_t st) {
     WorkDesc none{};
-    k_wf_shade<true><<<blocks, 128, 0, st>>>(S, P0, none, B, F);
+    k_wf_shade<true><<<blocks, kShadeThreads, 0, st>>>(S, P0, none, B, F);
     return cudaGetLastError();
 }
 
