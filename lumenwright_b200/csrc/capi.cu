@@ -112,7 +112,7 @@ struct lw_ctx {
     size_t partials_cap_bytes = size_t(4) << 30;
     // the wavefront engine: path slots (grown to the largest pool used), queue fetch settings
 #ifndef LW_WF_TAIL
-#define LW_WF_TAIL 8
+#define LW_WF_TAIL 12
 #endif
     uint32_t wf_tail = LW_WF_TAIL;
     // kernel_ms of the launches already timed when the last one is still running (stats.kernel_ms
