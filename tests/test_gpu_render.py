@@ -110,3 +110,37 @@ def test_wavefront_default_items_are_one_sample(ctx, c2):
     ctx.set_tuning(engine=ENGINE_WAVEFRONT, sub=0, paths=0)
     got = ctx.render_hq(p, c2.sky, 6)
     assert np.array_equal(got, want)
+
+
+def _same_hit(a, b):
+    if a is None or b is None:
+        return a is None and b is None
+    f = lambda x: np.float32(x).tobytes()
+    return a.quad == b.quad and a.texel == b.texel and f(a.t) == f(b.t) and f(a.s) == f(b.s) and f(a.tt) == f(b.tt)
+
+
+def test_traversal_over_the_terrain_matches_the_oracle(ctx, c1):
+    # Rays from points around the camera over the C1 terrain, in random directions and along the
+    # axes (straight up and down, exactly level), through `lw_trace_rays` against the oracle's trace
+    # of the reference algorithm: the hit (or its absence) is the same bit for bit. This covers
+    # the early exit of rays above the last occupied brick row that do not go down, which the
+    # reference reaches by skipping brick after brick.
+    p = c1.params
+    ctx.upload_hq_scene(c1.scene)
+    rng = np.random.default_rng(7)
+    eye = np.array(p["cam_pos"][:3], np.float32)
+    n = 2048
+    o = (eye + rng.uniform([-40, -45, -40], [40, 60, 40], (n, 3))).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    axes = np.array([[0, 1, 0], [0, -1, 0], [1, 0, 0], [-1, 0, 0], [0, 0, 1], [0, 0, -1]], np.float32)
+    d[: 6 * 64] = np.repeat(axes, 64, axis=0)
+    d[6 * 64: 8 * 64, 1] = 0.0  # level rays in random horizontal directions
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d = d.astype(np.float32)
+    got = ctx.trace_rays(p, o, d)
+    v = O.OracleScene.from_frame(c1)
+    want = [v.trace(oo, dd) for oo, dd in zip(o, d)]
+    bad = [i for i, (g, w) in enumerate(zip(got, want)) if not _same_hit(g, w)]
+    assert not bad, f"{len(bad)} of {n} rays differ from the oracle, first {bad[:5]}"
+    hits = sum(g is not None for g in got)
+    assert 0 < hits < n  # both hits and rays that leave the grid
