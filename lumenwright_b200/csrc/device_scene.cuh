@@ -283,30 +283,53 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
         // bricks until it leaves the grid: the reference's loop skips them one by one and ends
         // without a hit, which is the result here at once.
         if (R.s1 >= 0 && by >= S.sky_brick_y) return -1;
-        // Skip the whole brick: jump to its exit face (trace.rs:184-226).
+        // Skip the whole brick: jump to its exit face (trace.rs:184-226). The brick after a skip
+        // is the neighbour along the exit axis (the other axes' cells are clamped into the brick
+        // skipped), and the exit distances depend on the bricks alone, so a run of empty bricks is
+        // stepped brick by brick here, each one counted as the reference's loop counts it, and
+        // the cell, next boundaries and distance are formed once, as the last skip forms them.
         int bc0 = (int)bx, bc1 = (int)by, bc2 = (int)bz;
-        float t_out = kINF;
-        int axis = 0;
-        if (R.s0 != 0) {
-            float tt = ((float)(R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
-            if (tt < t_out) { t_out = tt; axis = 0; }
+        float e0 = R.s0 != 0 ? ((float)(R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x : kINF;
+        float e1 = R.s1 != 0 ? ((float)(R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y : kINF;
+        float e2 = R.s2 != 0 ? ((float)(R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z : kINF;
+        float t_out;
+        int axis;
+        for (;;) {
+            // The first axis with the smallest exit distance (trace.rs's strict comparisons).
+            t_out = kINF;
+            axis = 0;
+            if (R.s0 != 0 && e0 < t_out) { t_out = e0; axis = 0; }
+            if (R.s1 != 0 && e1 < t_out) { t_out = e1; axis = 1; }
+            if (R.s2 != 0 && e2 < t_out) { t_out = e2; axis = 2; }
+            if (t_out > ts.t_end) return -1;
+            const int nb0 = bc0 + (axis == 0 ? R.s0 : 0), nb1 = bc1 + (axis == 1 ? R.s1 : 0), nb2 = bc2 + (axis == 2 ? R.s2 : 0);
+            const int na = axis == 0 ? nb0 : (axis == 1 ? nb1 : nb2);
+            const int da = (int)(axis == 0 ? dx : (axis == 1 ? P.grid_dims.y : dz));
+            if (na < 0 || na >= da) return -1;  // the exit cell leaves the grid
+            const uint32_t nb = ((uint32_t)nb1 * dz + (uint32_t)nb2) * dx + (uint32_t)nb0;
+            const uint2 e = ldg(S.top + nb);
+            if (e.x != EMPTY || e.y != EMPTY) {
+                bc.b = nb;
+                bc.entry = e.x;
+                bc.ov = e.y;
+                if (bc.entry != EMPTY && !(bc.entry & UNIFORM)) bc.occ = ldg(S.occ + bc.entry);
+                break;
+            }
+            // The next brick is empty too: the reference's next visit, counted, skips it.
+            if (ts.it >= MAX_STEPS) return -1;
+            ts.it++;
+            if (R.s1 >= 0 && nb1 >= (int)S.sky_brick_y) return -1;
+            bc0 = nb0;
+            bc1 = nb1;
+            bc2 = nb2;
+            if (axis == 0) e0 = ((float)(R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
+            else if (axis == 1) e1 = ((float)(R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
+            else e2 = ((float)(R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
         }
-        if (R.s1 != 0) {
-            float tt = ((float)(R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
-            if (tt < t_out) { t_out = tt; axis = 1; }
-        }
-        if (R.s2 != 0) {
-            float tt = ((float)(R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
-            if (tt < t_out) { t_out = tt; axis = 2; }
-        }
-        if (t_out > ts.t_end) return -1;
         V3 pos = o + d * t_out;
         s.c0 = axis == 0 ? (R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
         s.c1 = axis == 1 ? (R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
         s.c2 = axis == 2 ? (R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
-        int ca = axis == 0 ? s.c0 : (axis == 1 ? s.c1 : s.c2);
-        int ga = axis == 0 ? R.gs0 : (axis == 1 ? R.gs1 : R.gs2);
-        if (ca < 0 || ca >= ga) return -1;
         s.n0 = next_boundary(o.x, inv.x, s.c0, R.s0);
         s.n1 = next_boundary(o.y, inv.y, s.c1, R.s1);
         s.n2 = next_boundary(o.z, inv.z, s.c2, R.s2);
