@@ -505,9 +505,11 @@ LW_DI int trace_round_warp(const DevScene &S, const DevParams &P, TraceState &ts
     uint32_t model = 0;
     int r = 0;
     if (have) {
-        for (uint32_t n = 0; n < budget; n++) {
+        uint32_t more = budget - 1u;  // visits left in this round after the next one
+        for (;;) {
             r = visit(S, P, ts, o, d, R, bc, model);
-            if (r != 0) break;
+            if (r != 0 || more == 0u) break;
+            more--;
         }
     }
     const bool pending = have && r > 0;
