@@ -261,7 +261,7 @@ LW_DI DV path(const DevScene &S0, const Theta &T, uint32_t px, uint32_t py, uint
     float tmin = 0.0f;
     const V3 sigma = f4v(P.water_color);
     for (uint32_t ev = 0; ev < MAX_EVENTS; ev++) {
-        Hit h = trace(S, P, o, d, tmin, kINF);
+        Hit h = trace<false>(S, P, o, d, tmin, kINF);
         bool found = h.quad != NO_QUAD, forced = false;
         if (bounces == 0 && P.see_through.y > 0u && found && !is_see_through(P, h.quad)) {
             Hit st = see_through_hit(S, P, o, d, h.t);
@@ -378,7 +378,7 @@ LW_DI DV path(const DevScene &S0, const Theta &T, uint32_t px, uint32_t py, uint
                 V3 tlam[8];
                 int nt = 0;
                 for (int sg = 0; sg < 8; sg++) {
-                    Hit sh = trace(S, P, so, l0, eps, tmax);
+                    Hit sh = trace<false>(S, P, so, l0, eps, tmax);
                     if (sh.quad == NO_QUAD) break;
                     const DevQuad *sq = S.quads + sh.quad;
                     uint32_t sf = __float_as_uint(ldg(&sq->p0_flags).w);
@@ -475,7 +475,7 @@ LW_DI DV path(const DevScene &S0, const Theta &T, uint32_t px, uint32_t py, uint
                         if (dot(to, n) > 0.0f) {
                             float dist = vlength(to);
                             V3 ll = vdiv(to, dist);
-                            Hit eh = trace(S, P, origin, ll, eps, dist + 2.0f * eps);
+                            Hit eh = trace<false>(S, P, origin, ll, eps, dist + 2.0f * eps);
                             if (eh.quad != NO_QUAD && !(fabs_r(eh.t - dist) >= 2.0f * eps)) {
                                 V3 nq = -f4v(ldg(&eq->n_nn));
                                 float area = vlength(nq);

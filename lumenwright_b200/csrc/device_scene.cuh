@@ -262,6 +262,7 @@ LW_DI RayDda ray_dda(const DevParams &P, V3 d) {
 //    tests no quad).
 //  * Every visit (brick skip, empty voxel, voxel with quads) counts towards MAX_STEPS as one
 //    iteration of the reference's loop does.
+template <bool RUNS = true>
 LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, const RayDda &R, BrickCache &bc,
                 uint32_t &model) {
     const uint32_t dx = P.grid_dims.x, dz = P.grid_dims.z;
@@ -283,6 +284,37 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
         // bricks until it leaves the grid: the reference's loop skips them one by one and ends
         // without a hit, which is the result here at once.
         if (R.s1 >= 0 && by >= S.sky_brick_y) return -1;
+        if (!RUNS) {
+            // Skip the whole brick: jump to its exit face (trace.rs:184-226).
+            int bc0 = (int)bx, bc1 = (int)by, bc2 = (int)bz;
+            float t_out = kINF;
+            int axis = 0;
+            if (R.s0 != 0) {
+                float tt = ((float)(R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
+                if (tt < t_out) { t_out = tt; axis = 0; }
+            }
+            if (R.s1 != 0) {
+                float tt = ((float)(R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
+                if (tt < t_out) { t_out = tt; axis = 1; }
+            }
+            if (R.s2 != 0) {
+                float tt = ((float)(R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
+                if (tt < t_out) { t_out = tt; axis = 2; }
+            }
+            if (t_out > ts.t_end) return -1;
+            V3 pos = o + d * t_out;
+            s.c0 = axis == 0 ? (R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
+            s.c1 = axis == 1 ? (R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
+            s.c2 = axis == 2 ? (R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
+            int ca = axis == 0 ? s.c0 : (axis == 1 ? s.c1 : s.c2);
+            int ga = axis == 0 ? R.gs0 : (axis == 1 ? R.gs1 : R.gs2);
+            if (ca < 0 || ca >= ga) return -1;
+            s.n0 = next_boundary(o.x, inv.x, s.c0, R.s0);
+            s.n1 = next_boundary(o.y, inv.y, s.c1, R.s1);
+            s.n2 = next_boundary(o.z, inv.z, s.c2, R.s2);
+            s.t = t_out;
+            return 0;
+        }
         // Skip the whole brick: jump to its exit face (trace.rs:184-226). The brick after a skip
         // is the neighbour along the exit axis (the other axes' cells are clamped into the brick
         // skipped), and the exit distances depend on the bricks alone, so a run of empty bricks is
@@ -389,6 +421,7 @@ LW_DI bool test_cell(const DevScene &S, const DevParams &P, const TraceState &ts
 // how the lanes of a warp are kept together: the loop is split in two (a "while-while" traversal),
 // an inner loop that steps through empty bricks and empty voxels until the ray reaches a cell with
 // quads, then the quads of that cell, so the lanes of a warp reach the quad tests together.
+template <bool RUNS = true>
 LW_DI int trace_run(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, float tmin, uint32_t budget,
                     Hit &out) {
     const RayDda R = ray_dda(P, d);
@@ -399,7 +432,7 @@ LW_DI int trace_run(const DevScene &S, const DevParams &P, TraceState &ts, V3 o,
         for (;;) {
             if (budget != 0u && n >= budget) return 0;
             n++;
-            int r = visit(S, P, ts, o, d, R, bc, model);
+            int r = visit<RUNS>(S, P, ts, o, d, R, bc, model);
             if (r < 0) return -1;
             if (r > 0) break;
         }
@@ -521,11 +554,14 @@ LW_DI int trace_round_warp(const DevScene &S, const DevParams &P, TraceState &ts
 }
 
 // trace (trace.rs:137-290): the closest hit along o + t d, t in (tmin, tmax), in one go.
+// RUNS: whether a visit steps a whole run of empty bricks (the adjoint's kernels, whose registers
+// are bounded tighter, run 10 % faster with one brick per visit).
+template <bool RUNS = true>
 LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, float tmax) {
     TraceState ts;
     if (!trace_begin(ts, P, o, d, tmax)) return no_hit();
     Hit h;
-    if (trace_run(S, P, ts, o, d, tmin, 0u, h) == 1) return h;
+    if (trace_run<RUNS>(S, P, ts, o, d, tmin, 0u, h) == 1) return h;
     return no_hit();
 }
 
