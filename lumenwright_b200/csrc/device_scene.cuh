@@ -260,6 +260,8 @@ LW_DI RayDda ray_dda(const DevParams &P, V3 d) {
 // entry in bc.ov; the DDA then stays in that cell.
 //  * A voxel in an empty 4^3 sub-block of a brick without overlay is not read (its model is 0, it
 //    tests no quad).
+//  * An empty brick is crossed in one step; with RUNS, so is a whole run of them. A ray in an
+//    empty brick above the last occupied brick row that does not go down ends there, no hit.
 //  * Every visit (brick skip, empty voxel, voxel with quads) counts towards MAX_STEPS as one
 //    iteration of the reference's loop does.
 template <bool RUNS = true>
