@@ -457,7 +457,6 @@ LW_DI bool warp_test_cells(const DevScene &S, const DevParams &P, const TraceSta
     const Dda &s = ts.s;
     float t_lo = 0.0f;
     uint32_t qbase = 0u, cnt = 0u;
-    V3 lo = v3(0.0f, 0.0f, 0.0f);
     Hit best = no_hit();
     if (pending) {
         float t_cell_exit = fmin_r(s.n0, fmin_r(s.n1, s.n2));
@@ -468,7 +467,6 @@ LW_DI bool warp_test_cells(const DevScene &S, const DevParams &P, const TraceSta
             qbase = m.x;
             cnt = m.y;
         }
-        lo = o - v3((float)s.c0, (float)s.c1, (float)s.c2);
     }
     // Exclusive scan of the lanes' quad counts.
     uint32_t incl = cnt;
@@ -487,7 +485,11 @@ LW_DI bool warp_test_cells(const DevScene &S, const DevParams &P, const TraceSta
             uint32_t p = __shfl_sync(FULL, pre, L + step);
             if (p <= k) L += step;
         }
-        const V3 olo = v3(__shfl_sync(FULL, lo.x, L), __shfl_sync(FULL, lo.y, L), __shfl_sync(FULL, lo.z, L));
+        // the owner's origin relative to its cell, formed here from its origin and cell (fewer
+        // registers live across the loop than keeping it in the owner)
+        const V3 olo = v3(__shfl_sync(FULL, o.x, L), __shfl_sync(FULL, o.y, L), __shfl_sync(FULL, o.z, L)) -
+                       v3((float)__shfl_sync(FULL, s.c0, L), (float)__shfl_sync(FULL, s.c1, L),
+                          (float)__shfl_sync(FULL, s.c2, L));
         const V3 od = v3(__shfl_sync(FULL, d.x, L), __shfl_sync(FULL, d.y, L), __shfl_sync(FULL, d.z, L));
         const float otlo = __shfl_sync(FULL, t_lo, L);
         const uint32_t oq = __shfl_sync(FULL, qbase, L) + (k - __shfl_sync(FULL, pre, L));
