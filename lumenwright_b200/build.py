@@ -48,9 +48,11 @@ def build(force=False, verbose=False) -> str:
         sys.stderr.write(r.stdout + r.stderr)
     if r.returncode != 0:
         raise RuntimeError("nvcc failed:\n" + r.stderr[-4000:])
-    # The register and spill record, without ptxas's compile times, which differ on every build.
+    # The register and spill record, without ptxas's compile times, which differ on every build,
+    # and with source paths relative to the package.
     with open(os.path.join(LIB_DIR, "ptxas.txt"), "w") as f:
-        f.writelines(l for l in r.stderr.splitlines(True) if "Compile time" not in l)
+        f.writelines(l.replace(HERE + os.sep, "") for l in r.stderr.splitlines(True)
+                     if "Compile time" not in l)
     return LIB_PATH
 
 

@@ -20,7 +20,6 @@ __device__ unsigned long long g_stats[16];
 #ifndef LW_MIN_BLOCKS
 #define LW_MIN_BLOCKS 4
 #endif
-constexpr int kThreads = 128;
 
 // The persistent render kernel. Each lane takes an item (sub consecutive samples of one pixel),
 // traces its samples one after another, and takes the next item as soon as it is done. Each loop
