@@ -49,6 +49,24 @@ def sun_direction_from_angle(angle) -> np.ndarray:
     return normalize32([-np.sin(t, dtype=F32), np.cos(t, dtype=F32), F32(0.0)])
 
 
+def sun_direction(altitude_deg, azimuth_deg) -> np.ndarray:
+    """sky.rs:41-44 (f32): the sun at an altitude and azimuth in degrees, azimuth 0 north (-z),
+    90 east (+x)."""
+    alt = F32(F32(altitude_deg) * F32(math.pi / 180.0))
+    az = F32(F32(azimuth_deg) * F32(math.pi / 180.0))
+    ca = np.cos(alt, dtype=F32)
+    return normalize32([np.sin(az, dtype=F32) * ca, np.sin(alt, dtype=F32), -np.cos(az, dtype=F32) * ca])
+
+
+def day_weight(factor, night, day) -> np.float32:
+    """sky.rs:824-829: where the sky light factor stands between its night and day values,
+    clamped to [0, 1]; 1 for a timeline whose two values do not differ."""
+    factor, night, day = F32(factor), F32(night), F32(day)
+    if F32(day - night) <= np.finfo(F32).eps:
+        return F32(1.0)
+    return F32(min(max(F32((factor - night) / F32(day - night)), F32(0.0)), F32(1.0)))
+
+
 def twilight(altitude) -> np.float32:
     """sky.rs:625-629: 1 while the sun's disc is up, falling linearly to the night's sky light
     at the end of civil twilight."""

@@ -245,3 +245,35 @@ def sky_dir(turns, el):
     az = np.float32(turns) * np.float32(2 * np.pi)
     el = np.float32(el)
     return np.array([np.cos(el) * np.cos(az), np.sin(el), np.cos(el) * np.sin(az)], dtype=np.float32)
+
+
+SUN_ATLAS = (40, 40)  # sky.rs:1153-1163: a 32x32 sun sprite at (3, 5) in a 40x40 atlas
+SUN_SPRITE = (3, 5, 32, 32)
+
+
+def sun_texel(x, y):
+    """sky.rs:1155-1157: every texel of the sprite differs."""
+    return 0xFF00_0000 | (x * 7 + 3) | ((y * 7 + 3) << 8) | (((x + y) * 3) << 16)
+
+
+def sun_atlas():
+    w, h = SUN_ATLAS
+    sx, sy, sw, sh = SUN_SPRITE
+    atlas = np.zeros(w * h, np.uint32)
+    for y in range(sh):
+        for x in range(sw):
+            atlas[(y + sy) * w + x + sx] = sun_texel(x, y)
+    return atlas
+
+
+def sun_sprite_params(p, sun):
+    """The sun-texture fields of `Params` for a sun direction, as `hq_params` sets them
+    (request.rs:1153-1225): `sun_su`/`sun_sv` from `sun_texture_axes` with the brightness and
+    half-width in w, the sprite's rectangle in the atlas."""
+    from lumenwright_b200 import sky as SK
+    su, sv = SK.sun_texture_axes(sun)
+    p["sun_dir"] = [sun[0], sun[1], sun[2], np.float32(np.cos(SK.SUN_RADIUS))]
+    p["sun_su"] = [su[0], su[1], su[2], SK.SUN_TEXTURE_BRIGHTNESS]
+    p["sun_sv"] = [sv[0], sv[1], sv[2], np.float32(4.0) * SK.SUN_RADIUS]
+    p["sun_sprite"] = [float(v) for v in SUN_SPRITE]
+    return su, sv

@@ -9,8 +9,8 @@ import math
 import numpy as np
 import pytest
 
-from kernel_fixtures import (INF, LAMP_EMITTANCE, LAMP_INTENSITY, basic_scene, lamp_scene, map_scene, norm,
-                             set_preetham_45, wall_rays, wall_scene)
+from kernel_fixtures import (INF, LAMP_EMITTANCE, LAMP_INTENSITY, SUN_ATLAS, basic_scene, lamp_scene, map_scene,
+                             norm, set_preetham_45, sun_atlas, sun_sprite_params, wall_rays, wall_scene)
 from lumenwright_b200 import layout as L
 from oracle import oracle as O
 
@@ -166,6 +166,37 @@ def test_lamp_room_per_sample(ctx, strategy, decoy):  # tests.rs:310-469 through
     p["sun_color"] = [1.0, 0.9, 0.8, 0.03]
     got = samples_match(ctx, ks, 8, 8, 16)
     assert np.isfinite(got).all()
+
+
+def test_the_camera_sees_the_sun_texture(ctx):  # integrator.rs:252-277, :617-621; sky.rs:1151-1253
+    # Camera rays above the grid, aimed at a 45-degree sun, miss everything: each sample is the
+    # sky through Chunky's cache plus the sun texture drawn from the 32x32 sprite of the
+    # reference's sun-texture test, bit for bit the oracle's.
+    from lumenwright_b200 import sky as SK
+    ks = basic_scene(False)
+    atlas = sun_atlas()
+    atlas[0], atlas[1] = 0xFFFF_FFFF, 0  # the cube's texels (outside the sprite)
+    ks.atlas = atlas
+    p = ks.params
+    p["off2"][1], p["off2"][2] = SUN_ATLAS
+    sun = SK.sun_direction(45.0, 135.0)
+    su, sv = sun_sprite_params(p, sun)
+    pre = SK.Preetham(sun)
+    p["sky_sun"] = [*pre.sun, 1.0]
+    p["sky_zenith"] = [*pre.zenith, 0.0]
+    for k, name in enumerate(("perez_a", "perez_b", "perez_c", "perez_d", "perez_e")):
+        p[name] = [*pre.perez[k], 0.0]
+    p["misc_f"][2] = 128
+    p["frame"] = [24, 24, 0, 2]
+    p["cam_pos"] = [24.0, 40.0, 8.0, 0.16]
+    p["cam_fwd"] = [*sun, 1.0]
+    p["cam_right"] = [*su, 0.0]
+    p["cam_up"] = [*sv, 0.0]
+    ks.sky = O.OracleScene(*ks.buffers()).build_sky_cache(128)
+    got = samples_match(ctx, ks, 24, 24, 4)
+    # the sprite (up to about 11 per channel) covers most of the view; the sky is below 1
+    lit = got.max(-1) > 1.0
+    assert 0.3 < lit.mean() < 0.95, lit.mean()
 
 
 def test_sky_maps_lens_and_light(ctx):  # tests.rs:805-831
