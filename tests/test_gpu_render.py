@@ -162,3 +162,18 @@ def test_small_and_ragged_frames_agree_between_engines(ctx, size):
     assert got.shape == (h, w, 3)
     assert np.array_equal(got, want)
     assert np.isfinite(got).all()
+
+
+def test_renders_are_deterministic(ctx, c2):
+    # render.rs:1015-1041 (byte-equal renders): the wavefront's rays go to whichever lane fetches
+    # them first, but every sample's radiance and every addition's order are fixed, so two renders
+    # of a frame are equal bit for bit, with the automatic pool and with a small one.
+    from lumenwright_b200.native import ENGINE_WAVEFRONT
+    p = c2.params
+    ctx.upload_hq_scene(c2.scene)
+    for paths in (0, 1 << 12):
+        ctx.set_tuning(engine=ENGINE_WAVEFRONT, sub=0, paths=paths)
+        a = ctx.render_hq(p, c2.sky, 8)
+        b = ctx.render_hq(p, c2.sky, 8)
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    ctx.set_tuning(engine=ENGINE_WAVEFRONT, sub=0, paths=0)

@@ -227,3 +227,83 @@ def test_the_oracle_draws_chunkys_sun_texture():  # sky.rs:1151-1253
     assert drawn > 4 * 90 * 90, drawn
     assert edge * 100 < checked, edge
     assert SUN_SPRITE[2] == 32 and SUN_SPRITE[3] == 32
+
+
+def to_hsl64(c):
+    """Chunky's `ColorUtil.RGBtoHSL` in FP64, per row of `c` (n x 3), the channels clamped to
+    [0, 1]; the hue of a red maximum keeps the sign of its remainder, as Java's % does."""
+    c = np.clip(c, 0.0, 1.0)
+    r, g, b = c[:, 0], c[:, 1], c[:, 2]
+    cmax, cmin = c.max(1), c.min(1)
+    delta = cmax - cmin
+    light = (cmax + cmin) / 2.0
+    sd = np.where(delta == 0.0, 1.0, delta)
+    hue = np.where(cmax == r, np.fmod((g - b) / sd, 6.0) / 6.0,
+                   np.where(cmax == g, ((b - r) / sd + 2.0) / 6.0, ((r - g) / sd + 4.0) / 6.0))
+    hue = np.where(delta == 0.0, 0.0, hue)
+    den = 1.0 - np.abs(2.0 * light - 1.0)
+    sat = np.where(delta < 5e-8, 0.0, delta / np.where(den == 0.0, 1.0, den))
+    return np.stack([hue, sat, light], -1)
+
+
+def from_hsl64(hsl):
+    """Chunky's `ColorUtil.RGBfromHSL` in FP64, per row (n x 3)."""
+    h, s, l = hsl[:, 0] * 6.0, hsl[:, 1], hsl[:, 2]
+    c = np.minimum((1.0 - np.abs(2.0 * l - 1.0)) * s, 1.0)
+    x = c * (1.0 - np.abs(np.fmod(h, 2.0) - 1.0))
+    z = np.zeros_like(c)
+    sector = np.select([h < 1.0, h < 2.0, h < 3.0, h < 4.0, h < 5.0], [0, 1, 2, 3, 4], 5)
+    rgb = np.choose(sector[:, None], [np.stack(v, -1) for v in
+                                      ((c, x, z), (x, c, z), (z, c, x), (z, x, c), (x, z, c), (c, z, x))])
+    return rgb + np.maximum(l - 0.5 * c, 0.0)[:, None]
+
+
+def test_the_oracle_reads_the_sky_through_chunkys_sky_cache():  # sky.rs:1255-1397
+    n = SK.SKY_CACHE_RESOLUTION
+    worst, count, saturated = 0.0, 0, 0
+    for alt, az in ((-0.005091, math.pi), (0.1, 2.0), (0.8, 0.7)):
+        # Chunky's `SkyCache.precalculateSky`: HSL of the sky at (n + 1)^2 directions, i over
+        # the azimuth, j over the elevation.
+        i, j = np.divmod(np.arange((n + 1) * (n + 1)), n + 1)
+        theta = i / n * 2.0 * math.pi
+        phi = j / n * math.pi - math.pi / 2
+        table = to_hsl64(preetham64(max(alt, 0.0), az, np.stack(
+            [np.cos(theta) * np.cos(phi), np.sin(phi), np.sin(theta) * np.cos(phi)], -1))).reshape(n + 1, n + 1, 3)
+        sun = np.array([math.cos(az) * math.cos(alt), math.sin(alt), math.sin(az) * math.cos(alt)], F32)
+        pre = SK.Preetham(sun)
+        p = L.new_params()
+        p["sky_sun"] = [*pre.sun, 1.0]
+        p["sky_zenith"] = [*pre.zenith, 0.0]
+        for k, name in enumerate(("perez_a", "perez_b", "perez_c", "perez_d", "perez_e")):
+            p[name] = [*pre.perez[k], 0.0]
+        p["misc_f"] = [0.0, 0.0, float(n), 0.0]
+        view = O.OracleScene(p, None, None, None, None, None, None)
+        cache = view.build_sky_cache(n)
+        assert cache.size == (n + 1) * (n + 1) * 3
+        view.set_sky(cache)
+        a_i, h_j = np.divmod(np.arange(97 * 41), 41)
+        a = a_i / 97.0 * 2.0 * math.pi + 0.013
+        h = h_j / 40.0 * 1.9 - 0.95
+        r = np.sqrt(1.0 - h * h)
+        d = np.stack([np.cos(a) * r, h, np.sin(a) * r], -1)
+        # `calcIncidentLight` and `getColorInterpolated`: bilinear in HSL between the cache's
+        # entries around the direction's (azimuth, elevation)
+        t = np.arctan2(d[:, 2], d[:, 0]) / (2.0 * math.pi)
+        t = np.fmod(np.fmod(t, 1.0) + 1.0, 1.0)
+        e = (np.arcsin(np.clip(d[:, 1], -1.0, 1.0)) + math.pi / 2) / math.pi
+        x, y = t * n, e * n
+        fx = np.clip(x, 0.0, n - 1.0).astype(np.int64)
+        fy = np.clip(y, 0.0, n - 1.0).astype(np.int64)
+        wx, wy = (x - fx)[:, None], (y - fy)[:, None]
+        y0 = table[fx, fy] + wx * (table[fx + 1, fy] - table[fx, fy])
+        y1 = table[fx, fy + 1] + wx * (table[fx + 1, fy + 1] - table[fx, fy + 1])
+        want = from_hsl64(y0 + wy * (y1 - y0))
+        got = view.sky_radiance_many(d.astype(F32)).astype(np.float64)
+        worst = max(worst, float(np.abs(got - want).max()))
+        bright = (preetham64(max(alt, 0.0), az, d) > 1.0).any(1)
+        saturated += int(bright.sum())
+        assert np.all(got[bright] <= 1.0 + 1e-5)
+        count += len(d)
+    assert count == 3 * 97 * 41
+    assert saturated > 0, "no direction near a sun brighter than the cache's limit"
+    assert worst < 1e-4, worst
