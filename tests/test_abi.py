@@ -1,9 +1,11 @@
 """The C-ABI library loads without a GPU and exports every function include/lumenwright_b200.h
-declares; the records keep the reference's sizes. CPU only: nothing here calls into CUDA."""
+declares; the records keep the reference's sizes, and the Python mirrors of the header's records
+are laid out as the C compiler lays the header out. CPU only: nothing here calls into CUDA."""
 
 import ctypes
 import os
 import re
+import subprocess
 
 from lumenwright_b200 import build, layout, native
 
@@ -31,3 +33,47 @@ def test_records_keep_the_reference_sizes():
     assert layout.QUAD_DTYPE.itemsize == 80
     assert layout.MODEL_DTYPE.itemsize == 16
     assert layout.EMITTER_DTYPE.itemsize == 32
+
+
+# The Python mirrors of the header's records: ctypes structures of the bindings and numpy dtypes
+# of the scene records, each with the C struct it must match field for field.
+MIRRORS = (
+    ("lw_scene_desc", native.SceneDesc), ("lw_stats", native.Stats), ("lw_tuning", native.Tuning),
+    ("lw_camera_job", native.CameraJob), ("lw_adj_frame", native.AdjFrame), ("lw_world_desc", native.WorldDesc),
+    ("lw_instances_desc", native.InstancesDesc), ("lw_build_info", native.BuildInfo),
+    ("lw_tonemap", native.ToneMap), ("lw_gradient", native.Gradient), ("lw_hit", native.HitRec),
+    ("lw_params", layout.PARAMS_DTYPE), ("lw_quad", layout.QUAD_DTYPE), ("lw_model", layout.MODEL_DTYPE),
+    ("lw_emitter", layout.EMITTER_DTYPE),
+)
+
+
+def mirror_fields(m):
+    """(size, [(field, offset, size)]) of a ctypes structure or a numpy record dtype."""
+    if isinstance(m, type) and issubclass(m, ctypes.Structure):
+        return ctypes.sizeof(m), [(f, getattr(m, f).offset, getattr(m, f).size) for f, *_ in m._fields_]
+    return m.itemsize, [(f, m.fields[f][1], m.fields[f][0].itemsize) for f in m.names]
+
+
+def test_python_mirrors_match_the_header_layout(tmp_path):
+    # Compiles a C program against the header that prints each record's size and each field's
+    # offset and size as the C compiler lays them out, and compares the Python mirrors with it.
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "lumenwright_b200.h"', "int main(void) {"]
+    for cname, m in MIRRORS:
+        lines.append(f'printf("{cname} . 0 %zu\\n", sizeof({cname}));')
+        for f, _, _ in mirror_fields(m)[1]:
+            lines.append(f'printf("{cname} {f} %zu %zu\\n", offsetof({cname}, {f}), sizeof((({cname} *)0)->{f}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    c = {}
+    for line in filter(None, out):
+        name, field, a, b = line.split()
+        c[(name, field)] = (int(a), int(b))
+    for cname, m in MIRRORS:
+        size, fields = mirror_fields(m)
+        assert c[(cname, ".")][1] == size, (cname, size)
+        for f, off, fsize in fields:
+            assert c[(cname, f)] == (off, fsize), (cname, f, off, fsize, c[(cname, f)])
