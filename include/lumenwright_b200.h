@@ -156,7 +156,11 @@ lw_status lw_get_stats(const lw_ctx *ctx, lw_stats *out);
  * slots, 128 threads, budget 0, sub automatic). */
 lw_status lw_set_tuning(lw_ctx *ctx, const lw_tuning *tuning);
 lw_status lw_get_tuning(const lw_ctx *ctx, lw_tuning *out);
-/* Asks a running render on `ctx` to stop; it returns LW_ERR_CANCELLED. Safe from any thread. */
+/* Asks a running render on `ctx` to stop; safe from any thread. The render's call returns
+ * LW_ERR_CANCELLED, or, where that call returns before its kernels end (lw_render_device,
+ * lw_batch_run), the call that waits for its results does (lw_read_accumulator,
+ * lw_read_accumulator_rgba, lw_batch_read): the results then lack samples. The next render on
+ * `ctx` starts uncancelled. */
 void lw_cancel(lw_ctx *ctx);
 /* Records timing mark `slot` (0..7), a CUDA event on the context's stream, and reads the time
  * between two marks once both are reached (the device's clock, not the host's). */

@@ -173,6 +173,25 @@ lw_status cuda_fail(lw_ctx *c, cudaError_t e, const char *what) {
         if (e_ != cudaSuccess) return cuda_fail(c, e_, what); \
     } while (0)
 
+// The start of a render: clears the cancel flag and the device cancel word. lw_cancel writes the
+// word on its own stream, so a write still queued from a cancel made before this call is waited
+// for first: landing after the clear, it would stop this render's kernels unseen.
+lw_status begin_render(lw_ctx *c) {
+    CK(c, cudaStreamSynchronize(c->aux), "waiting for an earlier cancel");
+    __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
+    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
+    return LW_OK;
+}
+
+// After the wait for a render's results: a cancel that came while the kernels ran (after the last
+// check between launches) may have stopped them before the last sample, so the results are
+// incomplete and the call reports the cancel.
+lw_status check_cancelled(lw_ctx *c) {
+    if (__atomic_load_n(c->cancel_host, __ATOMIC_RELAXED))
+        return fail(c, LW_ERR_CANCELLED, "cancelled: the render may have stopped before its last sample");
+    return LW_OK;
+}
+
 template <typename T>
 cudaError_t ensure(DBuf<T> &b, size_t n) {
     if (n == 0) n = 1;
@@ -847,8 +866,8 @@ lw_status lw_render_device(lw_ctx *c, const lw_params *params, uint32_t sample_s
     if (c->acc_w != params->frame[0] || c->acc_h != params->frame[1])
         return fail(c, LW_ERR_INVALID_ARGUMENT, "the accumulator is %ux%u, the frame %ux%u", c->acc_w, c->acc_h, params->frame[0], params->frame[1]);
     if (spp == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "spp is 0");
-    __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
-    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
+    s = begin_render(c);
+    if (s != LW_OK) return s;
     reset_stats(c);
     return render_batches(c, params, sample_start, spp, nullptr, nullptr, spp);
 }
@@ -872,7 +891,8 @@ lw_status lw_render_accumulate_noalloc(lw_ctx *c, const lw_params *params, uint3
     uint64_t batch = subs * pl.sub < spp ? subs * pl.sub : spp;
     DevScene S = dev_scene(c);
     DevParams P = dev_params(params);
-    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
+    s = begin_render(c);
+    if (s != LW_OK) return s;
     for (uint32_t done = 0; done < spp;) {
         uint32_t n = spp - done < batch ? spp - done : (uint32_t)batch;
         WorkDesc W = work(c, 0, 0, w, h, sample_start + done, n, pl.sub);
@@ -895,7 +915,7 @@ lw_status lw_read_accumulator(lw_ctx *c, float *out_rgb) {
     CK(c, launch_finalize(c->acc.p, (uint32_t)n, c->out_rgb.p, c->stream), "launching the finalize kernel");
     CK(c, cudaMemcpyAsync(out_rgb, c->out_rgb.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "reading the image");
     CK(c, cudaStreamSynchronize(c->stream), "reading the image");
-    return LW_OK;
+    return check_cancelled(c);
 }
 
 lw_status lw_render_hq(lw_ctx *c, const lw_params *params, const float *sky, uint64_t sky_len, uint32_t spp,
@@ -909,8 +929,8 @@ lw_status lw_render_hq(lw_ctx *c, const lw_params *params, const float *sky, uin
     if (s != LW_OK) return s;
     s = lw_clear_accumulator(c, params->frame[0], params->frame[1]);
     if (s != LW_OK) return s;
-    __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
-    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
+    s = begin_render(c);
+    if (s != LW_OK) return s;
     reset_stats(c);
     s = render_batches(c, params, 0, spp, progress, user, spp);
     if (s != LW_OK) return s;
@@ -929,13 +949,13 @@ lw_status lw_render_samples(lw_ctx *c, const lw_params *params, uint32_t x0, uin
     CK(c, ensure(c->samples, n), "allocating the samples");
     WorkDesc W = work(c, x0, y0, w, h, sample_start, count, 1);
     W.samples_out = c->samples.p;
-    __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
-    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
+    s = begin_render(c);
+    if (s != LW_OK) return s;
     CK(c, cudaMemsetAsync(c->counter.p, 0, 4, c->stream), "clearing the work counter");
     CK(c, launch_render(MODE_SAMPLES, dev_scene(c), dev_params(params), W, c->shape_samples, c->stream), "launching the render kernel");
     CK(c, cudaMemcpyAsync(out, c->samples.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "reading the samples");
     CK(c, cudaStreamSynchronize(c->stream), "rendering samples");
-    return LW_OK;
+    return check_cancelled(c);
 }
 
 lw_status lw_trace_rays(lw_ctx *c, const lw_params *params, uint32_t n, const float *o, const float *d, float tmin,
@@ -1141,7 +1161,8 @@ lw_status lw_batch_prepare(lw_ctx *c, const lw_camera_job *jobs, uint32_t n) {
 lw_status lw_batch_run(lw_ctx *c) {
     if (!c || !c->batch_graph) return fail(c, LW_ERR_INVALID_ARGUMENT, "no batch prepared");
     cudaSetDevice(c->device);
-    CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
+    lw_status s = begin_render(c);
+    if (s != LW_OK) return s;
     CK(c, cudaEventRecord(c->ev_a, c->stream), "recording an event");
     CK(c, cudaGraphLaunch(c->batch_graph, c->stream), "launching the batch graph");
     CK(c, cudaEventRecord(c->ev_b, c->stream), "recording an event");
@@ -1163,7 +1184,7 @@ lw_status lw_batch_read(lw_ctx *c) {
            "reading an image");
     }
     CK(c, cudaStreamSynchronize(c->stream), "reading the images");
-    return LW_OK;
+    return check_cancelled(c);
 }
 
 lw_status lw_render_batch(lw_ctx *c, const lw_camera_job *jobs, uint32_t n) {
@@ -1434,7 +1455,7 @@ lw_status lw_read_accumulator_rgba(lw_ctx *c, const lw_tonemap *tm, uint32_t *ou
     if (out_rgb)
         CK(c, cudaMemcpyAsync(out_rgb, c->out_rgb.p, 12 * n, cudaMemcpyDeviceToHost, c->stream), "reading the image");
     CK(c, cudaStreamSynchronize(c->stream), "reading the pixels");
-    return LW_OK;
+    return check_cancelled(c);
 }
 
 static lw_status world_check(lw_ctx *c, const lw_world_desc *w) {
