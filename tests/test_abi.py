@@ -54,11 +54,11 @@ def mirror_fields(m):
     return m.itemsize, [(f, m.fields[f][1], m.fields[f][0].itemsize) for f in m.names]
 
 
-def test_python_mirrors_match_the_header_layout(tmp_path):
-    # Compiles a C program against the header that prints each record's size and each field's
-    # offset and size as the C compiler lays them out, and compares the Python mirrors with it.
-    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "lumenwright_b200.h"', "int main(void) {"]
-    for cname, m in MIRRORS:
+def check_layout(tmp_path, include_dir, header, mirrors):
+    """Compiles a C program against `header` that prints each record's size and each field's
+    offset and size as the C compiler lays them out, and compares the Python mirrors with it."""
+    lines = ["#include <stddef.h>", "#include <stdio.h>", f'#include "{header}"', "int main(void) {"]
+    for cname, m in mirrors:
         lines.append(f'printf("{cname} . 0 %zu\\n", sizeof({cname}));')
         for f, _, _ in mirror_fields(m)[1]:
             lines.append(f'printf("{cname} {f} %zu %zu\\n", offsetof({cname}, {f}), sizeof((({cname} *)0)->{f}));')
@@ -66,14 +66,27 @@ def test_python_mirrors_match_the_header_layout(tmp_path):
     src = tmp_path / "layout.c"
     src.write_text("\n".join(lines))
     exe = tmp_path / "layout"
-    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    subprocess.run(["gcc", "-std=c11", "-I", include_dir, str(src), "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
     c = {}
     for line in filter(None, out):
         name, field, a, b = line.split()
         c[(name, field)] = (int(a), int(b))
-    for cname, m in MIRRORS:
+    for cname, m in mirrors:
         size, fields = mirror_fields(m)
         assert c[(cname, ".")][1] == size, (cname, size)
         for f, off, fsize in fields:
             assert c[(cname, f)] == (off, fsize), (cname, f, off, fsize, c[(cname, f)])
+
+
+def test_python_mirrors_match_the_header_layout(tmp_path):
+    check_layout(tmp_path, os.path.join(ROOT, "include"), "lumenwright_b200.h", MIRRORS)
+
+
+def test_oracle_bindings_match_the_oracle_header_layout(tmp_path):
+    # The oracle's ctypes records against oracle/lw_oracle.h, so the checker reads its inputs and
+    # writes its answers where the C code does.
+    from oracle import oracle as O
+    check_layout(tmp_path, os.path.join(ROOT, "oracle"), "lw_oracle.h",
+                 (("lwo_scene", O.Scene), ("lwo_hit", O.Hit), ("lwo_camera64", O.Camera64),
+                  ("lwo_theta", O.Theta), ("lwo_counters", O.Counters)))
