@@ -1,11 +1,14 @@
 """The multi-GPU sample sharding on the host: two gloo ranks render their sample ranges of a small
 frame with the CPU oracle, reduce their means to rank 0, and the result equals one process
-rendering every sample. CPU only (world size 2)."""
+rendering every sample; and a rank that does not join the reduction (it leaves, or it stalls)
+ends the waiting rank's reduction with an error within the process group's timeout. CPU only
+(world size 2)."""
 
 import os
 import socket
 
 import numpy as np
+import pytest
 import torch.multiprocessing as mp
 
 from kernel_fixtures import lamp_scene
@@ -62,3 +65,40 @@ def test_two_ranks_give_the_single_process_frame(tmp_path):
     assert shard.sample_range(0, 2, 8, 1) == (16, 8) and shard.sample_range(1, 2, 8, 1) == (24, 8)
     want = mean_of_range(16, 16)
     np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6)
+
+
+def leaving_worker(rank, world, port, out, mode):
+    import datetime
+    import time
+
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=5))
+    if rank == 1:
+        # This rank never joins the reduction: it leaves between steps with nothing in flight, or
+        # it stalls past the process group's timeout before leaving.
+        if mode == "stalls":
+            time.sleep(12.0)
+        dist.destroy_process_group()
+        return
+    t0 = time.monotonic()
+    try:
+        shard.reduce_means(np.ones((2, 3, 3), np.float32), dist)
+        result = "none"
+    except Exception as e:  # the reduction's error
+        result = type(e).__name__
+    with open(out, "w") as f:
+        f.write(f"{result} {time.monotonic() - t0:.1f}")
+
+
+@pytest.mark.parametrize("mode", ["leaves", "stalls"])
+def test_a_rank_that_does_not_join_ends_the_reduction_with_an_error(tmp_path, mode):
+    # Failure detection on the host: the rank left waiting in the reduction gets an error (at once
+    # when its peer has left, after the process group's 5 s timeout when its peer stalls) instead
+    # of waiting for good.
+    out = str(tmp_path / "r.txt")
+    mp.start_processes(leaving_worker, args=(2, free_port(), out, mode), nprocs=2, join=True, start_method="spawn")
+    result, seconds = open(out).read().split()
+    assert result != "none"
+    assert float(seconds) < 11.0
