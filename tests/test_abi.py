@@ -90,3 +90,17 @@ def test_oracle_bindings_match_the_oracle_header_layout(tmp_path):
     check_layout(tmp_path, os.path.join(ROOT, "oracle"), "lw_oracle.h",
                  (("lwo_scene", O.Scene), ("lwo_hit", O.Hit), ("lwo_camera64", O.Camera64),
                   ("lwo_theta", O.Theta), ("lwo_counters", O.Counters)))
+
+
+def test_the_header_compiles_strictly_as_c_and_cpp(tmp_path):
+    # A binding generator or a C caller reads the header as C99, a C++ caller as C++11; both
+    # with every warning an error.
+    src = tmp_path / "h.c"
+    src.write_text('#include "lumenwright_b200.h"\nint main(void) { return 0; }\n')
+    inc = os.path.join(ROOT, "include")
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", inc, "-fsyntax-only",
+                    str(src)], check=True)
+    cpp = tmp_path / "h.cpp"
+    cpp.write_text(src.read_text())
+    subprocess.run(["g++", "-std=c++11", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I", inc, "-fsyntax-only",
+                    str(cpp)], check=True)
