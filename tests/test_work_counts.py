@@ -47,7 +47,8 @@ def count_c2():
     per = {k: total[k] / n for k in total}
     trace_b = sum(b * per[k] for k, b in TRACE.items())
     shade_b = sum(b * per[k] for k, b in SHADE.items()) + 16.0
-    return {"workload": "c2", "sampled": n, "counts_per_sample": per, "trace_bytes_per_sample": trace_b,
+    return {"workload": "c2", "command": "LW_WRITE_COUNTS=1 python -m pytest tests/test_work_counts.py -q",
+            "sampled": n, "counts_per_sample": per, "trace_bytes_per_sample": trace_b,
             "shade_bytes_per_sample": shade_b, "bytes_per_sample": trace_b + shade_b,
             "bytes_per_access": {**TRACE, **SHADE, "accumulate": 16}}
 
