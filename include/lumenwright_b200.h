@@ -159,8 +159,9 @@ lw_status lw_get_tuning(const lw_ctx *ctx, lw_tuning *out);
 /* Asks a running render on `ctx` to stop; safe from any thread. The render's call returns
  * LW_ERR_CANCELLED, or, where that call returns before its kernels end (lw_render_device,
  * lw_batch_run), the call that waits for its results does (lw_read_accumulator,
- * lw_read_accumulator_rgba, lw_batch_read): the results then lack samples. The next render on
- * `ctx` starts uncancelled. */
+ * lw_read_accumulator_rgba, lw_batch_read): the results then lack samples. A cancel also stops
+ * the kernels of lw_render_accumulate_noalloc, which waits for nothing and so cannot report it: its
+ * accumulator then lacks samples. The next render on `ctx` starts uncancelled. */
 void lw_cancel(lw_ctx *ctx);
 /* Records timing mark `slot` (0..7), a CUDA event on the context's stream, and reads the time
  * between two marks once both are reached (the device's clock, not the host's). */
