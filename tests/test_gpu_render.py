@@ -178,17 +178,3 @@ def test_renders_are_deterministic(ctx, c2):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     ctx.set_tuning(engine=ENGINE_WAVEFRONT, sub=0, paths=0)
 
-
-def test_a_cancelled_render_reports_it_and_the_next_one_is_whole(ctx, c1):
-    # lw_cancel from the progress callback (the calling thread, between launches): the render
-    # returns LW_ERR_CANCELLED. The cancel's write to the device word lands before the next render
-    # clears it, so the next render is the whole frame, bit for bit an uncancelled render's.
-    from lumenwright_b200.native import LwError
-    p = c1.params
-    ctx.upload_hq_scene(c1.scene)
-    want = ctx.render_hq(p, c1.sky, 4)
-    with pytest.raises(LwError) as e:
-        ctx.render_hq(p, c1.sky, 4, progress=lambda done, total: ctx.cancel())
-    assert e.value.status == 6  # LW_ERR_CANCELLED
-    got = ctx.render_hq(p, c1.sky, 4)
-    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
