@@ -5,8 +5,8 @@
  *
  * It replaces the reference's CUDA entry `pt_render`
  * (crates/lumenwright-ptx/src/lib.rs:37-87) and its host launcher `CudaBackend::render_hq`
- * (crates/lumenwright/src/render/cuda.rs:77-184). A Rust `Backend` implementation calls these
- * functions (INTEGRATION.md shows the binding).
+ * (crates/lumenwright/src/render/cuda.rs:77-184); a Rust `Backend` implementation calls these
+ * functions through an FFI crate.
  *
  * Conventions: every length is in elements of its buffer, as `pt_render` takes them; the caller
  * owns every host buffer; the library owns device memory inside an `lw_ctx`. No function traps
@@ -159,9 +159,13 @@ lw_status lw_get_tuning(const lw_ctx *ctx, lw_tuning *out);
 /* Asks a running render on `ctx` to stop; safe from any thread. The render's call returns
  * LW_ERR_CANCELLED, or, where that call returns before its kernels end (lw_render_device,
  * lw_batch_run), the call that waits for its results does (lw_read_accumulator,
- * lw_read_accumulator_rgba, lw_batch_read): the results then lack samples. A cancel also stops
- * the kernels of lw_render_accumulate_noalloc, which waits for nothing and so cannot report it: its
- * accumulator then lacks samples. The next render on `ctx` starts uncancelled. */
+ * lw_read_accumulator_rgba, lw_batch_read). A render is cut into launches (a batch of samples
+ * each); a launch that a cancel reaches adds nothing to the accumulator, so every pixel keeps the
+ * whole launches done before it and its count says how many samples that is (a cancelled batch
+ * leaves its images at zero). A cancel also stops the kernels of lw_render_accumulate_noalloc,
+ * which returns before they run and so cannot report it: the caller's accumulator then holds the
+ * launches done before the cancel, and each record's count (its fourth float) tells how many
+ * samples. The next render on `ctx` starts uncancelled. */
 void lw_cancel(lw_ctx *ctx);
 /* Records timing mark `slot` (0..7), a CUDA event on the context's stream, and reads the time
  * between two marks once both are reached (the device's clock, not the host's). */
@@ -269,8 +273,10 @@ lw_status lw_render_batch(lw_ctx *ctx, const lw_camera_job *jobs, uint32_t n);
  * compensation r, g, b, unused; zero it before the first call), and allocates nothing: the
  * render kernel's work counter and item sums live in a fixed 32 MiB array inside the library.
  * The mean of a pixel is (sum - compensation) / count. Frames of more than 2,097,152 pixel slots
- * (8x4-pixel tiles, about 1920x1088) are refused with LW_ERR_INVALID_ARGUMENT. The work is queued
- * on the context's stream (lw_stream) and the call returns without waiting. Every call on every
+ * (8x4-pixel tiles, about 1920x1088) are refused with LW_ERR_INVALID_ARGUMENT, and so is an `accum`
+ * that is not device (or managed) memory of the context's GPU. The work is queued on the context's
+ * stream (lw_stream) and the call returns without waiting for the GPU (an earlier lw_cancel's
+ * write is waited for on the device, not on the host). Every call on every
  * context of a device shares the one array: calls whose work overlaps on the GPU (from several
  * threads, contexts or streams) race on it and must be serialised by the caller. The first call on
  * a device looks the array's address up (cudaGetSymbolAddress); make that first call before any
@@ -290,6 +296,12 @@ lw_status lw_trace_rays(lw_ctx *ctx, const lw_params *params, uint32_t n, const 
 /* `SceneView::voxel` (crates/lumenwright-kernel/src/scene.rs:271-284) on the re-laid grid, for n
  * voxels given as 3n int32 coordinates. */
 lw_status lw_voxel_lookup(lw_ctx *ctx, uint32_t n, const int32_t *xyz, uint32_t *out);
+
+/* The exponential the kernels apply in the water's Beer-Lambert transmittance, exp(-sigma * t)
+ * (`transmittance`, crates/lumenwright-kernel/src/math.rs:300), for n arguments: exp(x[i]) rounded
+ * to the nearest f32 (the project's own correctly rounded exponential, which the CPU oracle calls
+ * too), in out[i]. */
+lw_status lw_water_exp(lw_ctx *ctx, uint64_t n, const float *x, float *out);
 
 /* ---- the reference's CUDA backend, ported as written (for comparison) -------------------------
  * The render of lw_render_hq done the way the reference's CUDA backend does it: `pt_render`

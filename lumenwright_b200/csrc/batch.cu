@@ -96,7 +96,8 @@ k_render_batch(const DevScene S, const BatchDesc B) {
     }
 }
 
-// Every camera's item sums into its accumulator (Kahan, in item order), then its image.
+// Every camera's item sums into its accumulator (Kahan, in item order), then its image. A
+// cancelled batch adds nothing (its item sums may be stale), so its images are left at zero.
 __global__ void k_reduce_batch(const BatchDesc B) {
     uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= B.n_slots) return;
@@ -109,13 +110,15 @@ __global__ void k_reduce_batch(const BatchDesc B) {
     if (rx >= J.w || ry >= J.h) return;
     Accum &a = J.acc[(size_t)ry * J.w + rx];
     float4 s = a.sum, c = a.comp;
-    for (uint32_t jj = 0; jj < J.n_sub; jj++) {
-        float4 v = B.partials[J.partial_off + (size_t)jj * J.n_slots + slot];
-        kahan_add(s.x, c.x, v.x);
-        kahan_add(s.y, c.y, v.y);
-        kahan_add(s.z, c.z, v.z);
+    if (!*B.cancel) {
+        for (uint32_t jj = 0; jj < J.n_sub; jj++) {
+            float4 v = B.partials[J.partial_off + (size_t)jj * J.n_slots + slot];
+            kahan_add(s.x, c.x, v.x);
+            kahan_add(s.y, c.y, v.y);
+            kahan_add(s.z, c.z, v.z);
+        }
+        s.w += (float)J.spp;
     }
-    s.w += (float)J.spp;
     a.sum = s;
     a.comp = c;
     float cnt = fmax_r(s.w, 1.0f);

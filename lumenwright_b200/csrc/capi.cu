@@ -94,6 +94,7 @@ struct lw_ctx {
     int *cancel_host = nullptr;      // host flag, read between launches
     DBuf<uint32_t> cancel_word;      // device word the render kernel polls; set by lw_cancel
     cudaStream_t aux = nullptr;      // lw_cancel's stream, so the write lands while a render runs
+    cudaEvent_t cancel_ev = nullptr; // recorded on `aux` after each cancel's write
     cudaStream_t cap = nullptr;      // the stream a graph's loop body is captured on
     lw_stats stats{};
     lw_tuning tuning{128, 0, 0, LW_ENGINE_WAVEFRONT, 0};
@@ -174,10 +175,11 @@ lw_status cuda_fail(lw_ctx *c, cudaError_t e, const char *what) {
     } while (0)
 
 // The start of a render: clears the cancel flag and the device cancel word. lw_cancel writes the
-// word on its own stream, so a write still queued from a cancel made before this call is waited
-// for first: landing after the clear, it would stop this render's kernels unseen.
+// word on its own stream, so the clear is ordered after the write of every cancel made before
+// this call (the render's stream waits for the event recorded after it, on the device; the host
+// does not wait): landing after the clear, such a write would stop this render's kernels unseen.
 lw_status begin_render(lw_ctx *c) {
-    CK(c, cudaStreamSynchronize(c->aux), "waiting for an earlier cancel");
+    CK(c, cudaStreamWaitEvent(c->stream, c->cancel_ev, 0), "ordering after an earlier cancel");
     __atomic_store_n(c->cancel_host, 0, __ATOMIC_RELAXED);
     CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
     return LW_OK;
@@ -582,6 +584,7 @@ lw_status lw_ctx_create(int device, lw_ctx **out) {
         if ((e = cudaEventCreate(&m)) != cudaSuccess) return bail(e, "creating events");
     c->cancel_host = new int(0);
     if ((e = cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "creating a stream");
+    if ((e = cudaEventCreateWithFlags(&c->cancel_ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "creating events");
     if ((e = ensure(c->cancel_word, 1)) != cudaSuccess) return bail(e, "allocating the cancel word");
     if ((e = cudaMemset(c->cancel_word.p, 0, 4)) != cudaSuccess) return bail(e, "clearing the cancel word");
     float lut[256];
@@ -644,6 +647,7 @@ void lw_ctx_destroy(lw_ctx *c) {
     delete c->cancel_host;
     c->cancel_word.free_();
     if (c->aux) cudaStreamDestroy(c->aux);
+    if (c->cancel_ev) cudaEventDestroy(c->cancel_ev);
     if (c->cap) cudaStreamDestroy(c->cap);
     if (c->ev_a) cudaEventDestroy(c->ev_a);
     if (c->ev_b) cudaEventDestroy(c->ev_b);
@@ -662,6 +666,7 @@ void lw_cancel(lw_ctx *c) {
     __atomic_store_n(c->cancel_host, 1, __ATOMIC_RELAXED);
     cudaSetDevice(c->device);
     cudaMemsetAsync(c->cancel_word.p, 0xFF, 4, c->aux);  // lands while a render kernel runs
+    cudaEventRecord(c->cancel_ev, c->aux);               // the next render's clear waits for it
 }
 
 lw_status lw_set_tuning(lw_ctx *c, const lw_tuning *t) {
@@ -884,6 +889,19 @@ lw_status lw_render_accumulate_noalloc(lw_ctx *c, const lw_params *params, uint3
         return fail(c, LW_ERR_INVALID_ARGUMENT,
                     "a %ux%u frame needs %u pixel slots; the allocation-free entry point holds %zu (about 1920x1088)",
                     w, h, probe.n_slots, kNoallocPartials);
+    // The accumulator must be device memory of this context's GPU (a host pointer or another GPU's
+    // buffer would fault in the reduction); cudaPointerGetAttributes allocates nothing.
+    {
+        cudaPointerAttributes pa{};
+        cudaError_t e = cudaPointerGetAttributes(&pa, accum);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(c, LW_ERR_INVALID_ARGUMENT, "accum is not a CUDA pointer: %s", cudaGetErrorString(e));
+        }
+        if ((pa.type != cudaMemoryTypeDevice && pa.type != cudaMemoryTypeManaged) || pa.device != c->device)
+            return fail(c, LW_ERR_INVALID_ARGUMENT, "accum must be device memory on device %d (it is of type %d on device %d)",
+                        c->device, (int)pa.type, pa.device);
+    }
     float4 *scratch = nullptr;
     CK(c, noalloc_scratch(c->device, &scratch), "looking up the scratch array");
     Plan pl = plan(c, probe.n_slots, spp);
@@ -991,6 +1009,17 @@ lw_status lw_voxel_lookup(lw_ctx *c, uint32_t n, const int32_t *xyz, uint32_t *o
     CK(c, launch_voxel_lookup(dev_scene(c), dev_params(&p), n, c->xyz.p, c->vox.p, c->stream), "launching the lookup kernel");
     CK(c, cudaMemcpyAsync(out, c->vox.p, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream), "reading ids");
     CK(c, cudaStreamSynchronize(c->stream), "looking up voxels");
+    return LW_OK;
+}
+
+lw_status lw_water_exp(lw_ctx *c, uint64_t n, const float *x, float *out) {
+    if (!c || !x || !out || !n || n > (uint64_t(1) << 31)) return fail(c, LW_ERR_INVALID_ARGUMENT, "bad argument");
+    cudaSetDevice(c->device);
+    CK(c, ensure(c->rays, (size_t)2 * n), "allocating the arguments");
+    CK(c, cudaMemcpyAsync(c->rays.p, x, 4 * (size_t)n, cudaMemcpyHostToDevice, c->stream), "uploading the arguments");
+    CK(c, launch_water_exp(n, c->rays.p, c->rays.p + n, c->stream), "launching the exponential");
+    CK(c, cudaMemcpyAsync(out, c->rays.p + n, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream), "reading the results");
+    CK(c, cudaStreamSynchronize(c->stream), "evaluating the exponential");
     return LW_OK;
 }
 

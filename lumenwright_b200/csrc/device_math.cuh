@@ -7,6 +7,8 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "water_exp.h"
+
 namespace lw {
 
 #define LW_DI __device__ __forceinline__
@@ -53,7 +55,11 @@ LW_DI V3 vdiv(V3 a, float s) { return a * __fdiv_rn(1.0f, s); }
 LW_HDI float max_elem(V3 a) { return fmax_r(a.x, fmax_r(a.y, a.z)); }
 LW_HDI float vget(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
 LW_HDI V3 lerp(V3 a, V3 o, float t) { return a + (o - a) * t; }
-LW_DI V3 transmittance(V3 a, float t) { return v3(expf(-a.x * t), expf(-a.y * t), expf(-a.z * t)); }
+// Beer-Lambert through water (math.rs:300, `(-a * t).exp()`), with the project's exponential
+// (water_exp.h), which the CPU oracle calls too.
+LW_DI V3 transmittance(V3 a, float t) {
+    return v3(lw_water_expf(-a.x * t), lw_water_expf(-a.y * t), lw_water_expf(-a.z * t));
+}
 LW_HDI V3 f4v(float4 a) { return v3(a.x, a.y, a.z); }
 
 // Rust's saturating `as i32` / `as u32` (NaN gives 0): the PTX cvt.rzi.sat conversions.

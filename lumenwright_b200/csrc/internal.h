@@ -70,6 +70,7 @@ cudaError_t launch_trace_rays(const DevScene &S, const DevParams &P, uint32_t n,
                               float tmin, float tmax, void *out_hits, cudaStream_t st);
 cudaError_t launch_voxel_lookup(const DevScene &S, const DevParams &P, uint32_t n, const int32_t *xyz, uint32_t *out,
                                 cudaStream_t st);
+cudaError_t launch_water_exp(uint64_t n, const float *x, float *out, cudaStream_t st);
 
 // sky.cu
 cudaError_t launch_sky_cache(const DevParams &P, uint32_t n, float *out, cudaStream_t st);

@@ -149,10 +149,13 @@ k_render(const DevScene S, const DevParams P, const WorkDesc W) {
     }
 }
 
-// Adds the launch's item sums into the per-pixel accumulator, in item order (Kahan).
+// Adds the launch's item sums into the per-pixel accumulator, in item order (Kahan). After a
+// cancel the render kernels may have left items unwritten (their sums then hold whatever an
+// earlier launch left there), so a cancelled launch adds nothing: a pixel's record keeps whole
+// launches only, and its count is the samples its sums hold.
 __global__ void k_reduce(const WorkDesc W, Accum *acc, uint32_t frame_w) {
     uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= W.n_slots) return;
+    if (slot >= W.n_slots || *W.cancel) return;
     uint32_t tile = slot >> 5, in = slot & 31u;
     uint32_t rx = (tile % W.tiles_x) * 8u + (in & 7u);
     uint32_t ry = (tile / W.tiles_x) * 4u + (in >> 3);
@@ -200,6 +203,11 @@ __global__ void k_voxel_lookup(const DevScene S, const DevParams P, uint32_t n, 
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     out[i] = voxel(S, P, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+}
+
+__global__ void k_water_exp(uint64_t n, const float *x, float *out) {
+    uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = lw_water_expf(x[i]);
 }
 
 #if LW_STATS
@@ -257,6 +265,12 @@ cudaError_t launch_finalize(const Accum *acc, uint32_t n, float *out_rgb, cudaSt
 cudaError_t launch_trace_rays(const DevScene &S, const DevParams &P, uint32_t n, const float *o, const float *d,
                               float tmin, float tmax, void *out_hits, cudaStream_t st) {
     k_trace_rays<<<(n + 127) / 128, 128, 0, st>>>(S, P, n, o, d, tmin, tmax, (DevHit *)out_hits);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_water_exp(uint64_t n, const float *x, float *out, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_water_exp<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(n, x, out);
     return cudaGetLastError();
 }
 

@@ -31,7 +31,7 @@ EXPORTS = (
     "lw_blend_chunky_sky", "lw_render_hq_reference_port", "lw_render_accumulate_noalloc", "lw_batch_prepare",
     "lw_batch_run", "lw_batch_read", "lw_render_batch", "lw_adjoint_forward", "lw_adjoint_backward", "lw_adjoint_fd",
     "lw_gamma_table", "lw_tonemap_rgba", "lw_read_accumulator_rgba", "lw_scene_build_keys", "lw_scene_build_grid",
-    "lw_scene_read",
+    "lw_scene_read", "lw_water_exp",
 )
 
 # lw_tonemap operators (post.rs `Tonemap`)
@@ -162,6 +162,7 @@ def load(path: str = LIB_PATH):
     L.lw_render_samples.argtypes = [P, P] + [C.c_uint32] * 6 + [P]
     L.lw_trace_rays.argtypes = [P, P, C.c_uint32, P, P, C.c_float, C.c_float, P]
     L.lw_voxel_lookup.argtypes = [P, C.c_uint32, P, P]
+    L.lw_water_exp.argtypes = [P, C.c_uint64, P, P]
     L.lw_build_sky_cache.argtypes = [P, P, C.c_uint32, P]
     L.lw_render_accumulate_noalloc.argtypes = [P, P, C.c_uint32, C.c_uint32, P]
     L.lw_batch_prepare.argtypes = [P, P, C.c_uint32]
@@ -508,6 +509,13 @@ class Context:
         self._check(self.L.lw_scene_read(self.h, grid.ctypes.data, grid.size, em.ctypes.data, em.size, eg.ctypes.data,
                                          eg.size))
         return grid, em, eg
+
+    def water_exp(self, x):
+        """The kernels' exponential of the water transmittance, exp(x) rounded to f32, per element."""
+        x = np.ascontiguousarray(x, np.float32).ravel()
+        out = np.zeros_like(x)
+        self._check(self.L.lw_water_exp(self.h, x.size, x.ctypes.data, out.ctypes.data))
+        return out
 
     def voxel_lookup(self, xyz):
         xyz = np.ascontiguousarray(xyz, np.int32).reshape(-1, 3)

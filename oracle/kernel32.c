@@ -11,6 +11,10 @@
 #define R_SQRT sqrtf
 #define R_FLOOR floorf
 #define R_EXP expf
+/* The water transmittance's exponential: the function the CUDA kernels call (water_exp.h, the
+ * project's correctly rounded f32 exp), where the reference's CPU build calls the platform expf;
+ * tests/test_water_exp.py holds it against both the platform expf and f64 exp. */
+#define R_TEXP lw_water_expf
 #define R_FMOD fmodf
 #define R_ACOS k_acos
 #define R_ATAN2 k_atan2
@@ -23,6 +27,7 @@ static inline float k_atan2(float y, float x);
 static inline float k_gamma_to_linear(float c);
 static inline void k_sin_cos_turns(float u, float *s, float *c);
 
+#include "water_exp.h"
 #include "kernel_impl.h"
 
 uint64_t lwo_bounds_error_count;
@@ -141,6 +146,40 @@ void lwo32_sky_radiance(const lwo_scene *s, const float d[3], float out[3]) { v3
 void lwo32_sky_lens(const lwo_scene *s, const float d[3], float out[3]) { v3o(sky_lens(s, v3a(d)), out); }
 void lwo32_sky_light(const lwo_scene *s, const float d[3], float out[3]) { v3o(sky_light(s, v3a(d)), out); }
 void lwo32_sun_texture(const lwo_scene *s, const float d[3], float out[3]) { v3o(sun_texture(s, v3a(d)), out); }
+
+/* The transmittance's exponential (water_exp.h) and the platform expf over n arguments. */
+void lwo32_water_exp(uint64_t n, const float *x, float *out) {
+    for (uint64_t i = 0; i < n; i++) out[i] = lw_water_expf(x[i]);
+}
+void lwo_platform_expf(uint64_t n, const float *x, float *out) {
+    for (uint64_t i = 0; i < n; i++) out[i] = expf(x[i]);
+}
+
+/* Every `stride`-th float x with bits in [lo_bits, hi_bits] (as unsigned words): counts where
+ * lw_water_expf(x) differs from the platform expf(x) and from exp((double)x) rounded to f32, and
+ * the largest difference from each in units of the last place of the f32 result. */
+void lwo32_water_exp_sweep(uint32_t lo_bits, uint32_t hi_bits, uint32_t stride, uint64_t out[5]) {
+    uint64_t n = 0, diff_platform = 0, diff_f64 = 0, ulp_platform = 0, ulp_f64 = 0;
+    if (stride == 0) stride = 1;
+    int64_t steps = ((int64_t)hi_bits - (int64_t)lo_bits) / (int64_t)stride + 1;
+#pragma omp parallel for schedule(static) reduction(+ : n, diff_platform, diff_f64) reduction(max : ulp_platform, ulp_f64)
+    for (int64_t i = 0; i < steps; i++) {
+        float x = f32_of(lo_bits + (uint32_t)(i * (int64_t)stride));
+        float a = lw_water_expf(x), b = expf(x), c = (float)exp((double)x);
+        uint32_t ab = bits_of(a), bb = bits_of(b), cb = bits_of(c);
+        uint64_t db = ab > bb ? ab - bb : bb - ab, dc = ab > cb ? ab - cb : cb - ab;
+        n++;
+        if (db) diff_platform++;
+        if (dc) diff_f64++;
+        if (db > ulp_platform) ulp_platform = db;
+        if (dc > ulp_f64) ulp_f64 = dc;
+    }
+    out[0] = n;
+    out[1] = diff_platform;
+    out[2] = ulp_platform;
+    out[3] = diff_f64;
+    out[4] = ulp_f64;
+}
 
 void lwo32_sky_radiance_many(const lwo_scene *s, uint64_t n, const float *d, float *out) {
 #pragma omp parallel for schedule(static)

@@ -12,6 +12,7 @@
 #define R_SQRT sqrt
 #define R_FLOOR floor
 #define R_EXP exp
+#define R_TEXP exp
 #define R_FMOD fmod
 #define R_ACOS acos
 #define R_ATAN2 atan2

@@ -9,6 +9,7 @@
  * The including file defines:
  *   REAL, PFX(name), K(lit)                 type, symbol prefix, literal of type REAL
  *   R_SQRT, R_FLOOR, R_EXP, R_FMOD          libm functions of type REAL
+ *   R_TEXP                                  the exponential of the water transmittance
  *   R_ACOS, R_ATAN2, R_GAMMA, R_SINCOS_TURNS the kernel's transcendental functions
  *   LWO_F64                                  defined in the double build
  */
@@ -148,7 +149,7 @@ static inline REAL vmax_elem(V3 a) { return rmax(a.x, rmax(a.y, a.z)); }
 static inline REAL vget(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
 static inline V3 vlerp(V3 a, V3 o, REAL t) { return vadd(a, vmuls(vsub(o, a), t)); }
 static inline V3 vtransmittance(V3 a, REAL t) { /* math.rs:300 */
-    return v3(R_EXP(-a.x * t), R_EXP(-a.y * t), R_EXP(-a.z * t));
+    return v3(R_TEXP(-a.x * t), R_TEXP(-a.y * t), R_TEXP(-a.z * t));
 }
 static const V3 V3_ZERO = {0, 0, 0};
 static const V3 V3_ONE = {1, 1, 1};

@@ -342,6 +342,18 @@ def gamma_to_linear(c):
     return lib().lwo32_gamma_to_linear(c)
 
 
+def water_exp(x):
+    """The water transmittance's exponential (lumenwright_b200/csrc/water_exp.h, the oracle's build
+    of it), elementwise over f32 arguments."""
+    L = lib()
+    L.lwo32_water_exp.argtypes = [C.c_uint64, C.c_void_p, C.c_void_p]
+    L.lwo32_water_exp.restype = None
+    x = np.ascontiguousarray(x, np.float32).ravel()
+    out = np.zeros_like(x)
+    L.lwo32_water_exp(x.size, x.ctypes.data, out.ctypes.data)
+    return out
+
+
 def bounds_errors():
     return lib().lwo_bounds_errors()
 

@@ -44,6 +44,31 @@ def test_batch_matches_separate_renders(ctx):
         assert np.array_equal(a, b)
 
 
+def test_batch_cameras_match_the_oracle(ctx):
+    # Directly against the oracle: the batch's cameras (the two times of day, game-sky maps and
+    # Chunky's cache) from one graph launch against the oracle's CPU-backend loop (f64 sums / spp)
+    # over the same inputs, every pixel within 1e-4 relative.
+    from oracle import oracle as O
+    hq, jobs = BT.c3_jobs(ctx, small_cameras())
+    ctx.upload_hq_scene(hq)
+    outs = ctx.batch_prepare(jobs)
+    ctx.batch_run()
+    ctx.batch_read()
+    checked = set()
+    for (p, sky, spp), got in zip(jobs, outs):
+        kind = "maps" if float(p["sky_map"][0]) >= 1.0 else "cache"
+        if kind in checked:
+            continue
+        checked.add(kind)
+        w, h = int(p["frame"][0]), int(p["frame"][1])
+        v = O.OracleScene(p, hq.grid, hq.models, hq.quads, hq.atlas, hq.emitters, hq.emitter_grid, sky)
+        want = v.render_mean(0, 0, w, h, spp)
+        ok = np.abs(got - want) <= 1e-4 * np.maximum(np.abs(got), np.abs(want)) + 1e-6
+        print(f"batch camera {w}x{h} at {spp} spp ({kind}): {ok.mean():.6f} within 1e-4")
+        assert ok.all(), (w, h, np.abs(got - want).max())
+    assert checked == {"maps", "cache"}
+
+
 def test_autotuner_picks_a_tuning(ctx, tmp_path):
     hq, jobs = BT.c3_jobs(ctx, small_cameras())
     ctx.upload_hq_scene(hq)

@@ -1,7 +1,7 @@
 """CUDA parity on the reference kernel tests' fixtures (`crates/lumenwright-kernel/src/tests.rs`):
 each query runs through the C ABI on the B200 and is checked against the FP32 oracle and against
 the reference test's own known answer. Integer results (hit quad, texel, voxel id) must be equal;
-floats must be bit-equal except where noted (the water transmittance calls each platform's expf).
+floats must be bit-equal except where noted.
 """
 
 import math
@@ -108,6 +108,20 @@ def test_voxel_lookup_is_bit_exact(ctx):  # scene.rs:271-284 on the re-laid bric
         v = O.OracleScene(*ks.buffers())
         want = np.array([v.voxel(*map(int, p)) for p in xyz[:: max(1, len(xyz) // 20000)]], np.uint32)
         assert np.array_equal(got[:: max(1, len(xyz) // 20000)], want)
+
+
+def test_water_exp_is_the_oracles_bit_for_bit(ctx):
+    # The transmittance's exponential on the device against the oracle's build of the same source
+    # (tests/test_water_exp.py holds that one against f64 exp and the platform expf): every 16th
+    # float of [-104, 0], every float near 0 and the special values, bit for bit.
+    lo, hi = np.array([-0.0, -104.0], np.float32).view(np.uint32)
+    x = np.arange(lo, hi + 1, 16, dtype=np.uint64).astype(np.uint32).view(np.float32)
+    tiny = np.arange(0x80000000, 0x80100000, dtype=np.uint64).astype(np.uint32).view(np.float32)
+    special = np.array([0.0, np.inf, -np.inf, np.nan, -150.0, -200.0, 88.72284, 100.0, 1e30, 5.5], np.float32)
+    x = np.concatenate([x, tiny, special])
+    got = ctx.water_exp(x)
+    want = O.water_exp(x)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), np.argwhere(got.view(np.uint32) != want.view(np.uint32))[:5]
 
 
 def samples_match(ctx, ks, w, h, count, rel=0.0):

@@ -35,3 +35,40 @@ def test_a_cancelled_render_reports_it_and_the_next_one_is_whole(ctx, c1):
     assert e.value.status == 6  # LW_ERR_CANCELLED
     got = ctx.render_hq(p, c1.sky, 4)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+def test_a_cancel_leaves_whole_launches_in_the_accumulator(ctx, c1):
+    # lw_cancel right after an allocation-free render was queued (it returns before its kernels
+    # run), while the render's kernels run: a launch the cancel reaches adds nothing, so every
+    # pixel's record holds the whole launches done before it (none, usually), and its mean is the
+    # mean of that many samples. The next call adds its samples in full.
+    import torch
+    p = c1.params
+    w, h = int(p["frame"][0]), int(p["frame"][1])
+    ctx.upload_hq_scene(c1.scene)
+    ctx.upload_sky(c1.sky)
+    spp = 2048
+    acc = torch.zeros(w * h * 8, dtype=torch.float32, device="cuda:0")
+    torch.cuda.synchronize()
+    ctx.render_accumulate_noalloc(p, 0, spp, acc.data_ptr())
+    ctx.cancel()
+    torch.cuda.synchronize()
+    a = acc.cpu().numpy().reshape(-1, 8).astype(np.float64)
+    counts = np.unique(a[:, 3])
+    print(f"sample counts per pixel after the cancel: {counts.tolist()}")
+    for cnt in counts:
+        sel = a[:, 3] == cnt
+        if cnt == 0:
+            assert not a[sel].any()  # untouched records
+            continue
+        assert cnt <= spp
+        want = ctx.render_hq(p, c1.sky, int(cnt)).reshape(-1, 3)[sel]
+        got = (a[sel, 0:3] - a[sel, 4:7]) / cnt
+        assert np.all(np.abs(got - want) <= 1e-4 * np.maximum(np.abs(got), np.abs(want)) + 1e-6)
+    # uncancelled again: 16 more samples in every record
+    ctx.upload_sky(c1.sky)
+    before = acc.cpu().numpy().reshape(-1, 8)[:, 3].copy()
+    ctx.render_accumulate_noalloc(p, 0, 16, acc.data_ptr())
+    torch.cuda.synchronize()
+    after = acc.cpu().numpy().reshape(-1, 8)[:, 3]
+    assert np.array_equal(after, before + 16)
