@@ -14,6 +14,13 @@ device (CUDA events on the library's stream, max over ranks); ``e2e`` times the 
 kernel and CPU backend loop) is timed on the host cores on a bounded sample of the same frame.
 Under ``torchrun`` (N > 1) each rank renders its own range of samples of the frame (weak
 scaling) and the accumulators are summed to rank 0 with one NCCL reduce.
+
+At N = 1 the line also carries the north star's other forms, each on its own configuration and
+timed the same way (unless --no-extras): ``reference_cuda_port`` (the reference's CUDA backend
+ported as written, on the same frame), ``batched_c3`` (64 cameras in one CUDA graph against 64
+separate renders), ``adjoint_c4`` (forward + backward), ``precision_c5`` (3840x2160 at --c5-spp
+with its FP64-oracle error), the drop-in image's FP64-oracle error (``accuracy``) and the tracing
+kernel against the L2 read bandwidth measured in the run (``roofline_l2``).
 """
 
 import argparse
@@ -134,6 +141,152 @@ def cpu_baseline(frame, budget_s=12.0):
     dt = time.perf_counter() - t0
     return {"value": samples / dt / 1e6, "unit": "Msamples/s", "cores": threads, "kind": "port",
             "sample": f"{n_rows} full rows spread over the frame at {spp} spp ({samples} samples, {dt:.1f} s)"}
+
+
+def camera64(frame):
+    """The frame's camera with its f64 eye (rebased to the grid in f64), for the FP64 oracle."""
+    from oracle import oracle as O
+    p = frame.params
+    return O.Camera64(tuple(float(x) for x in frame.eye64), tuple(float(x) for x in p["cam_fwd"][:3]),
+                      tuple(float(x) for x in p["cam_right"][:3]), tuple(float(x) for x in p["cam_up"][:3]),
+                      float(p["cam_pos"][3]), float(p["cam_fwd"][3]))
+
+
+def accuracy(frame, img, crop=64):
+    """The image's error against the FP64 oracle (FP64 throughout, camera rays from the f64 eye, the
+    same random streams) on the crop x crop pixels at the frame's centre, relative to the crop's
+    mean radiance."""
+    from oracle import oracle as O
+    p = frame.params
+    w, h = int(p["frame"][0]), int(p["frame"][1])
+    x0, y0 = w // 2 - crop // 2, h // 2 - crop // 2
+    t0 = time.perf_counter()
+    ref = O.OracleScene.from_frame(frame).render_mean64(x0, y0, crop, crop, frame.spp, cam=camera64(frame))
+    dt = time.perf_counter() - t0
+    err = img[y0:y0 + crop, x0:x0 + crop].astype(np.float64) - ref
+    mean = float(ref.mean())
+    rmse = float(np.sqrt(np.mean(err ** 2)))
+    return {"crop": [x0, y0, crop, crop], "spp": frame.spp, "rmse_rel_vs_fp64_oracle": rmse / mean,
+            "max_abs_err": float(np.abs(err).max()), "crop_mean": mean, "oracle_s": round(dt, 1)}
+
+
+def extra_reference_port(frame, device):
+    """The reference's CUDA backend ported as written (one thread per pixel in 16x16 blocks, 1-64
+    spp per launch towards 150 ms, a synchronize after each; its own library) on the same frame:
+    `value` from its kernels' CUDA-event time, `e2e` from the whole call (the scene and sky copied
+    in, the image read back and divided on the host), as CudaBackend::render_hq does."""
+    from baseline.refport import port as RP
+    RP.render_hq(device, frame, spp=8)  # warm-up: module load and first launches
+    p = frame.params
+    samples = int(p["frame"][0]) * int(p["frame"][1]) * frame.spp
+    with ClockSampler(device) as clocks:
+        img, t = RP.render_hq(device, frame)
+    return img, {"value": samples / t["kernel_ms"] / 1e3, "unit": "Msamples/s",
+                 "e2e": samples / t["total_ms"] / 1e3, "kernel_ms": t["kernel_ms"], "total_ms": t["total_ms"],
+                 "launches": t["launches"], "spp": frame.spp, "clocks": clocks.summary(),
+                 "what": "pt_render + CudaBackend::render_hq ported to CUDA C++ as written (baseline/refport), "
+                         "nvcc for sm_100a; the reference's own Rust-to-PTX build needs a nightly Rust toolchain "
+                         "that this box lacks"}
+
+
+def extra_batched(device, scale=1.0):
+    """The batched form at its configuration: 64 seeded cameras (320x180..1920x1080, spp from {16,
+    64, 256, 1024}, 4-8 bounces, ticks 4000 and 12800) over the 12x12-chunk world in one CUDA graph,
+    tuned by the autotuner (trial batches at 1/64 of each camera's spp), against the same cameras
+    as 64 separate plain renders. One timed replay (the trials warmed the kernels)."""
+    from lumenwright_b200 import batch as BT
+    from lumenwright_b200.native import Context
+    ctx = Context(device)
+    hq, jobs = BT.c3_jobs(ctx, spp_scale=scale)
+    ctx.upload_hq_scene(hq)
+    samples = sum(int(p["frame"][0]) * int(p["frame"][1]) * spp for p, _, spp in jobs)
+    t0 = time.perf_counter()
+    tuning, entry = BT.Autotuner(ctx, trial_fraction=1 / 64).tune(jobs)
+    tune_s = time.perf_counter() - t0
+    ctx.batch_prepare(jobs)
+    with ClockSampler(device) as clocks:
+        ctx.mark(0)
+        ctx.batch_run()
+        ctx.mark(1)
+        batched_ms = ctx.elapsed(0, 1)
+    ctx.set_tuning(threads=128, budget=0, sub=0, engine=0, paths=0)
+    sep_ms = 0.0
+    last_sky = None
+    for i in sorted(range(len(jobs)), key=lambda i: id(jobs[i][1])):
+        p, sky, spp = jobs[i]
+        if sky is not last_sky:
+            ctx.upload_sky(sky)
+            last_sky = sky
+        ctx.clear_accumulator(int(p["frame"][0]), int(p["frame"][1]))
+        ctx.mark(2)
+        ctx.render_device(p, 0, spp)
+        ctx.mark(3)
+        sep_ms += ctx.elapsed(2, 3)
+    ctx.close()
+    return {"value": samples / batched_ms / 1e3, "unit": "Msamples/s", "ms": batched_ms, "samples": samples,
+            "cameras": len(jobs), "spp_scale": scale, "tuning": tuning, "autotune_s": round(tune_s, 1),
+            "separate_launches": {"value": samples / sep_ms / 1e3, "ms": sep_ms},
+            "speedup_vs_separate": sep_ms / batched_ms, "clocks": clocks.summary()}
+
+
+def extra_adjoint(device, steps=3):
+    """The differentiable form: forward (FP64 image) + path-replay backward of the L2 image loss on
+    the differentiation configuration (8x8 chunks, 512x288, 64 spp, 4 bounces, Chunky sky);
+    `value` from the two kernels' CUDA-event time, `e2e` from DiffProblem.gradient (host set-up,
+    copies and the sky cache's FP64 Jacobian included)."""
+    from lumenwright_b200 import adjoint as A
+    from lumenwright_b200.native import Context
+    ctx = Context(device)
+    prob = A.DiffProblem(ctx)
+    a = prob._args(prob.theta0)
+    samples = prob.width * prob.height * prob.spp
+    img = ctx.adjoint_forward(*a, prob.spp)
+    ctx.adjoint_backward(*a, prob.spp, 2.0 * (img - prob.target))
+    fwd = bwd = 0.0
+    with ClockSampler(device) as clocks:
+        for _ in range(steps):
+            img = ctx.adjoint_forward(*a, prob.spp)
+            fwd += ctx.stats()["kernel_ms"]
+            ctx.adjoint_backward(*a, prob.spp, 2.0 * (img - prob.target))
+            bwd += ctx.stats()["kernel_ms"]
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        prob.gradient(prob.theta0)
+    e2e_s = (time.perf_counter() - t0) / steps
+    ctx.close()
+    ms = (fwd + bwd) / steps
+    return {"value": samples / ms / 1e3, "unit": "Msamples/s (forward + backward)", "forward_ms": fwd / steps,
+            "backward_ms": bwd / steps, "e2e": samples / e2e_s / 1e6, "steps": steps, "parameters": A.N_THETA,
+            "clocks": clocks.summary()}
+
+
+def extra_precision(device, spp):
+    """The precision configuration's frame (32x32 chunks translated to x = 1,000,000, 3840x2160, 8
+    bounces) at `spp` (of its 4096), FP32 traversal, Kahan FP32 sums; its error against the FP64
+    oracle on the 64x64 centre crop."""
+    from lumenwright_b200 import request as R
+    from lumenwright_b200.native import Context
+    ctx = Context(device)
+    frame = R.make_frame(R.CONFIGS["c5"], sky_backend=ctx, spp=spp)
+    p = frame.params
+    w, h = int(p["frame"][0]), int(p["frame"][1])
+    ctx.upload_hq_scene(frame.scene)
+    ctx.upload_sky(frame.sky)
+    ctx.clear_accumulator(w, h)
+    ctx.render_device(p, 0, 2)  # warm-up
+    ctx.stats()
+    ctx.clear_accumulator(w, h)
+    with ClockSampler(device) as clocks:
+        ctx.mark(0)
+        ctx.render_device(p, 0, spp)
+        ctx.mark(1)
+        ms = ctx.elapsed(0, 1)
+    st = ctx.stats()
+    img = ctx.read_accumulator(w, h)
+    ctx.close()
+    return {"value": w * h * spp / ms / 1e3, "unit": "Msamples/s", "ms": ms, "width": w, "height": h, "spp": spp,
+            "of_spp": R.CONFIGS["c5"].spp, "launches": st["launches"], "trace_ms": st["trace_ms"],
+            "shade_ms": st["shade_ms"], "accuracy": accuracy(frame, img), "clocks": clocks.summary()}
 
 
 def run_reference(args, rank, world):
@@ -312,6 +465,9 @@ def main():
                     help="c2: the drop-in frame (default); c3: the batched form, 64 cameras; "
                          "c4: the differentiable form, one loss gradient")
     ap.add_argument("--c3-scale", type=float, default=0.25, help="spp scale of the 64 cameras (c3)")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="leave out the other forms' lines (reference port, batched, adjoint, precision)")
+    ap.add_argument("--c5-spp", type=int, default=2048, help="spp of the precision frame in the extras")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -392,7 +548,7 @@ def main():
     h2d = frame.scene.memory_bytes() + frame.sky.nbytes + 432
     d2h = w * h * 3 * 4
     e2e_frame = frame
-    be.render_hq(e2e_frame)  # warm-up
+    e2e_img = be.render_hq(e2e_frame).reshape(h, w, 3)  # warm-up (its image is checked below)
     be._scene_key = None
     if dist:
         dist.barrier()
@@ -461,6 +617,23 @@ def main():
         }
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(frame)
+        if world == 1 and not args.no_extras:
+            # The other forms of the north star, each on its own configuration, timed the same way.
+            line["accuracy"] = accuracy(frame, e2e_img)
+            port_img, port = extra_reference_port(frame, local)
+            port["image_rel_rmse_vs_product"] = float(np.sqrt(np.mean((port_img - e2e_img) ** 2)) / e2e_img.mean())
+            line["reference_cuda_port"] = port
+            line["vs_reference_cuda_port"] = {"value": value / port["value"], "e2e": e2e / port["e2e"]}
+            from baseline.refport import port as RP
+            l2 = RP.l2_read_gbs(local)
+            line["roofline_l2"] = {"bound": "l2", "kernel": "k_wf_trace", "achieved": achieved, "peak": l2,
+                                   "unit": "GB/s", "frac": achieved / l2 if achieved and l2 else None,
+                                   "peak_kind": "measured in this run: a 32 MB buffer read 200 times over by every "
+                                                "SM (16-byte L2 loads), CUDA events",
+                                   "warp_execution_efficiency": capture.get("active_lanes_per_instruction", 0) / 32.0}
+            line["batched_c3"] = extra_batched(local, scale=1.0)
+            line["adjoint_c4"] = extra_adjoint(local)
+            line["precision_c5"] = extra_precision(local, args.c5_spp)
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:

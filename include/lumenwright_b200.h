@@ -303,17 +303,6 @@ lw_status lw_voxel_lookup(lw_ctx *ctx, uint32_t n, const int32_t *xyz, uint32_t 
  * too), in out[i]. */
 lw_status lw_water_exp(lw_ctx *ctx, uint64_t n, const float *x, float *out);
 
-/* ---- the reference's CUDA backend, ported as written (for comparison) -------------------------
- * The render of lw_render_hq done the way the reference's CUDA backend does it: `pt_render`
- * (crates/lumenwright-ptx/src/lib.rs:37-87) ported to CUDA C++ as written (one thread per pixel in
- * 16x16 blocks, the nested render_sample, the reference grid layout, f32 sums) driven by
- * CudaBackend::render_hq's loop (crates/lumenwright/src/render/cuda.rs:127-169: batches of 1 to 64
- * spp adapting towards 150 ms a launch, a synchronize after each). Same inputs and output as
- * lw_render_hq; lw_get_stats reports its launches and kernel time. It is the baseline the B200
- * kernels are measured against, not a product path. */
-lw_status lw_render_hq_reference_port(lw_ctx *ctx, const lw_params *params, const float *sky, uint64_t sky_len,
-                                      uint32_t spp, float *out_rgb);
-
 /* ---- sky precompute on the device -----------------------------------------------------------
  * Chunky's sky cache for the sky in `params` (sky_sun, sky_zenith, perez_a..e) at resolution n:
  * `build_sky_cache` (crates/lumenwright-kernel/src/integrator.rs:133-148), which the reference

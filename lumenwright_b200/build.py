@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "liblumenwright_b200.so")
-SOURCES = ["render.cu", "batch.cu", "scene.cu", "sky.cu", "refport.cu", "noalloc.cu", "adjoint.cu", "wavefront.cu", "post.cu", "build.cu", "capi.cu"]
+SOURCES = ["render.cu", "batch.cu", "scene.cu", "sky.cu", "noalloc.cu", "adjoint.cu", "wavefront.cu", "post.cu", "build.cu", "capi.cu"]
 HEADERS = ["water_exp.h", "device_math.cuh", "device_scene.cuh", "device_integrator.cuh", "device_path.cuh", "internal.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 

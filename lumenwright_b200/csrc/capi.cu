@@ -76,7 +76,7 @@ struct lw_ctx {
     DBuf<uint4> models;
     DBuf<DevQuad> quads;
     DBuf<float4> emitters;
-    DBuf<uint8_t> ref_quads;  // the reference's 80-byte quads (read by the reference-port kernel)
+    DBuf<uint8_t> ref_quads;  // the reference's 80-byte quads, re-laid into `quads` at upload
     uint64_t grid_len = 0, models_len = 0, quads_len = 0, atlas_len = 0, emitters_len = 0, egrid_len = 0;
     // frame
     DBuf<float> sky, gamma, out_rgb;
@@ -1021,56 +1021,6 @@ lw_status lw_water_exp(lw_ctx *c, uint64_t n, const float *x, float *out) {
     CK(c, cudaMemcpyAsync(out, c->rays.p + n, 4 * (size_t)n, cudaMemcpyDeviceToHost, c->stream), "reading the results");
     CK(c, cudaStreamSynchronize(c->stream), "evaluating the exponential");
     return LW_OK;
-}
-
-lw_status lw_render_hq_reference_port(lw_ctx *c, const lw_params *params, const float *sky, uint64_t sky_len,
-                                      uint32_t spp, float *out_rgb) {
-    if (!c || !out_rgb) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
-    cudaSetDevice(c->device);
-    if (spp < 1) spp = 1;
-    lw_status s = lw_sky_upload(c, sky, sky_len);
-    if (s != LW_OK) return s;
-    if ((s = check_params(c, params, true)) != LW_OK) return s;
-    const uint32_t w = params->frame[0], h = params->frame[1];
-    DBuf<float4> acc;
-    CK(c, ensure(acc, (size_t)w * h), "allocating the accumulator");
-    CK(c, cudaMemsetAsync(acc.p, 0, sizeof(float4) * (size_t)w * h, c->stream), "clearing the accumulator");
-    DevScene Sv = dev_scene(c);
-    DevParams P = dev_params(params);
-    reset_stats(c);
-    uint32_t done = 0, batch = 1;
-    lw_status result = LW_OK;
-    while (done < spp) {
-        uint32_t n = batch < spp - done ? batch : spp - done;
-        auto t0 = std::chrono::steady_clock::now();
-        cudaError_t e = cudaEventRecord(c->ev_a, c->stream);
-        if (e == cudaSuccess) e = launch_refport(c->grid.p, c->models.p, c->ref_quads.p, c->atlas.p, c->emitters.p, c->egrid.p,
-                                                 c->sky.p, c->gamma.p, Sv, P, acc.p, done, n, c->stream);
-        if (e == cudaSuccess) e = cudaEventRecord(c->ev_b, c->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        if (e != cudaSuccess) {
-            result = cuda_fail(c, e, "running the reference-port kernel");
-            break;
-        }
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, c->ev_a, c->ev_b);
-        c->stats.kernel_ms += ms;
-        c->stats.launches++;
-        c->stats.samples += (uint64_t)w * h * n;
-        double took = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-        done += n;
-        if (took < 75.0) batch = batch * 2 < 64 ? batch * 2 : 64;
-        else if (took > 300.0 && batch > 1) batch /= 2;
-    }
-    if (result == LW_OK) {
-        CK(c, ensure(c->out_rgb, (size_t)3 * w * h), "allocating the output");
-        cudaError_t e = launch_refport_finalize(acc.p, w * h, c->out_rgb.p, c->stream);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(out_rgb, c->out_rgb.p, (size_t)12 * w * h, cudaMemcpyDeviceToHost, c->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        if (e != cudaSuccess) result = cuda_fail(c, e, "reading the image");
-    }
-    acc.free_();
-    return result;
 }
 
 lw_status lw_batch_prepare(lw_ctx *c, const lw_camera_job *jobs, uint32_t n) {

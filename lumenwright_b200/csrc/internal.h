@@ -165,13 +165,6 @@ cudaError_t launch_adj_backward(const DevScene &S, const AdjFrame &F, uint32_t s
 cudaError_t launch_adj_fd(const DevScene &S, const AdjFrame &plus, const AdjFrame &minus, const float *albedo0,
                           float4 sun0, uint32_t spp, double *diff, double *mean, cudaStream_t st);
 
-// refport.cu
-cudaError_t launch_refport(const void *grid, const void *models, const void *ref_quads, const void *atlas,
-                           const void *emitters, const void *egrid, const float *sky, const float *gamma,
-                           const DevScene &Sv, const DevParams &P, float4 *accum, uint32_t sample_start, uint32_t n,
-                           cudaStream_t st);
-cudaError_t launch_refport_finalize(const float4 *acc, uint32_t n, float *out, cudaStream_t st);
-
 // noalloc.cu: the fixed scratch array of the allocation-free entry point.
 extern const size_t kNoallocPartials;
 cudaError_t noalloc_scratch(int device, float4 **out);

@@ -5,22 +5,25 @@
  *
  * The reference's CPU path calls the platform `expf` (Rust's f32::exp) and its PTX build calls the
  * `libm` crate's expf; CUDA's expf is a third implementation, and a last-place difference between
- * them can flip a later Russian-roulette draw. This function is the project's own: it returns
- * exp(x) rounded to the nearest f32, which is what a correctly rounded expf returns, computed as
+ * them can flip a later Russian-roulette draw. This function is the project's own, in f32
+ * arithmetic with fused multiply-adds (an evaluation in double costs the shading kernel 12 % on a
+ * B200, a table-driven one in pairs of floats 9 %; this one under 1 %):
  *
  *   1. Cody and Waite's additive argument reduction (W. J. Cody and W. Waite, "Software Manual for
- *      the Elementary Functions", 1980): x = k ln2 + r with k = round(x / ln2), |r| <= ln2 / 2
- *      (plus a rounding), ln2 split into a high part with 32 significant bits, so k * ln2_hi and
- *      x - k * ln2_hi are exact for the k that occur here, and a low part;
- *   2. the Taylor series of e^r to degree 13 by Horner's rule (remainder below 2^-57 relative);
- *   3. the scaling by 2^k, exact;
- * all in IEEE double, with one rounding to f32 at the end. The double result is within a few
- * units of 2^-53 relative of e^x, so the f32 result is the correctly rounded one except where e^x
- * lies that close to the midpoint between two floats.
+ *      the Elementary Functions", 1980): x = k ln2 + r with k the integer nearest x / ln2 and
+ *      |r| <= ln2 / 2 (plus a rounding), r = (x - k C1) - k C2 with ln 2 = C1 + C2 split into its
+ *      nearest float and the nearest float to the rest, each step one fused multiply-add;
+ *   2. e^r by its Taylor series to degree 8 with Horner's rule, one fused multiply-add a step (the
+ *      next term is below 2^-32 of the result);
+ *   3. the scaling by 2^k, in two steps at the ends of the range; exact while the result is normal.
+ * Measured over every float of [-87.3365, 0] (the transmittance's arguments with a normal
+ * result), it is within one unit in the last place of exp(x) rounded to the nearest float, and
+ * equal to it on all but about 0.45 % of them.
  *
- * Every operation is an IEEE double add, multiply or floor, with no fused multiply-add (the
- * library is built with --fmad=false, the oracle with -ffp-contract=off), so the host and the
- * device give the same bits.
+ * Every operation is an IEEE f32 add, multiply or fused multiply-add written out as such (the
+ * library is built with --fmad=false, the oracle with -ffp-contract=off, so nothing else is fused,
+ * and neither compiler reorders floating-point operations), so the host and the device give the
+ * same bits.
  */
 #ifndef LW_WATER_EXP_H
 #define LW_WATER_EXP_H
@@ -35,46 +38,52 @@
 #include <math.h>
 #endif
 
-/* 2^k as a double, for -1022 <= k <= 1023. */
-LW_WEXP_FN double lw_pow2i(int k) {
-    uint64_t bits = (uint64_t)(int64_t)(k + 1023) << 52;
 #ifdef __CUDA_ARCH__
-    return __longlong_as_double((long long)bits);
+#define LW_WEXP_FMA(a, b, c) __fmaf_rn(a, b, c)
 #else
-    double d;
-    memcpy(&d, &bits, sizeof d);
-    return d;
+#define LW_WEXP_FMA(a, b, c) fmaf(a, b, c)
+#endif
+
+LW_WEXP_FN float lw_f32_of_bits(uint32_t u) {
+#ifdef __CUDA_ARCH__
+    return __uint_as_float(u);
+#else
+    float f;
+    memcpy(&f, &u, sizeof f);
+    return f;
 #endif
 }
 
-/* exp(x) rounded to f32. NaN gives NaN, -inf 0, +inf +inf; below -150 the result is 0 and above
- * 100 +inf, as the rounded e^x is there. */
+/* 2^e for -126 <= e <= 127. */
+LW_WEXP_FN float lw_pow2f(int e) { return lw_f32_of_bits((uint32_t)(e + 127) << 23); }
+
+/* exp(x) in f32 (see above). NaN gives NaN, anything below -104 (-inf included) 0, and anything
+ * above 88.72283 (+inf included) +inf, as the rounded e^x is there. */
 LW_WEXP_FN float lw_water_expf(float x) {
     if (x != x) return x;
-    double xd = (double)x;
-    xd = xd < -150.0 ? -150.0 : (xd > 100.0 ? 100.0 : xd);
-    const double LN2_HI = 6.93147180369123816490e-01; /* ln 2 to 32 significant bits */
-    const double LN2_LO = 1.90821492927058770002e-10; /* ln 2 - LN2_HI */
-    const double INV_LN2 = 1.44269504088896338700e+00;
-    double kd = floor(xd * INV_LN2 + 0.5);
-    int k = (int)kd;
-    double r = (xd - kd * LN2_HI) - kd * LN2_LO;
-    /* e^r = sum r^n / n!, n = 0..13, by Horner's rule. */
-    double p = 1.0 / 6227020800.0;                /* 1/13! */
-    p = 1.0 / 479001600.0 + r * p;                /* 1/12! */
-    p = 1.0 / 39916800.0 + r * p;                 /* 1/11! */
-    p = 1.0 / 3628800.0 + r * p;                  /* 1/10! */
-    p = 1.0 / 362880.0 + r * p;                   /* 1/9!  */
-    p = 1.0 / 40320.0 + r * p;                    /* 1/8!  */
-    p = 1.0 / 5040.0 + r * p;                     /* 1/7!  */
-    p = 1.0 / 720.0 + r * p;                      /* 1/6!  */
-    p = 1.0 / 120.0 + r * p;                      /* 1/5!  */
-    p = 1.0 / 24.0 + r * p;                       /* 1/4!  */
-    p = 1.0 / 6.0 + r * p;                        /* 1/3!  */
-    p = 0.5 + r * p;                              /* 1/2!  */
-    p = 1.0 + r * p;                              /* 1/1!  */
-    p = 1.0 + r * p;                              /* 1/0!  */
-    return (float)(p * lw_pow2i(k));
+    if (x > 88.72283172607421875f) return lw_f32_of_bits(0x7F800000u);
+    if (x < -104.0f) return 0.0f;
+    const float INV_LN2 = 0x1.715476p+0f;  /* 1 / ln 2, rounded */
+    const float C1 = 0x1.62e43p-1f;        /* ln 2, rounded */
+    const float C2 = -0x1.05c61p-29f;      /* ln 2 - C1, rounded */
+    const float MAGIC = 12582912.0f;       /* 1.5 * 2^23: adding and subtracting it rounds to an integer */
+    const float kf = (x * INV_LN2 + MAGIC) - MAGIC;
+    float r = LW_WEXP_FMA(-kf, C1, x);
+    r = LW_WEXP_FMA(-kf, C2, r);
+    /* e^r = sum r^n / n!, n = 0..8 */
+    float p = 1.0f / 40320.0f;
+    p = LW_WEXP_FMA(r, p, 1.0f / 5040.0f);
+    p = LW_WEXP_FMA(r, p, 1.0f / 720.0f);
+    p = LW_WEXP_FMA(r, p, 1.0f / 120.0f);
+    p = LW_WEXP_FMA(r, p, 1.0f / 24.0f);
+    p = LW_WEXP_FMA(r, p, 1.0f / 6.0f);
+    p = LW_WEXP_FMA(r, p, 0.5f);
+    p = LW_WEXP_FMA(r, p, 1.0f);
+    p = LW_WEXP_FMA(r, p, 1.0f);
+    const int k = (int)kf; /* -150 .. 128 */
+    if (k > 126) return (p * lw_pow2f(k - 1)) * 2.0f;
+    if (k >= -126) return p * lw_pow2f(k);
+    return (p * lw_pow2f(k + 64)) * lw_pow2f(-64);
 }
 
 #endif

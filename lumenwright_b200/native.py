@@ -28,7 +28,7 @@ EXPORTS = (
     "lw_elapsed_ms", "lw_set_tuning", "lw_get_tuning",
     "lw_scene_upload", "lw_render_hq", "lw_sky_upload", "lw_clear_accumulator", "lw_render_device",
     "lw_read_accumulator", "lw_render_samples", "lw_trace_rays", "lw_voxel_lookup", "lw_build_sky_cache",
-    "lw_blend_chunky_sky", "lw_render_hq_reference_port", "lw_render_accumulate_noalloc", "lw_batch_prepare",
+    "lw_blend_chunky_sky", "lw_render_accumulate_noalloc", "lw_batch_prepare",
     "lw_batch_run", "lw_batch_read", "lw_render_batch", "lw_adjoint_forward", "lw_adjoint_backward", "lw_adjoint_fd",
     "lw_gamma_table", "lw_tonemap_rgba", "lw_read_accumulator_rgba", "lw_scene_build_keys", "lw_scene_build_grid",
     "lw_scene_read", "lw_water_exp",
@@ -169,7 +169,6 @@ def load(path: str = LIB_PATH):
     L.lw_batch_run.argtypes = [P]
     L.lw_batch_read.argtypes = [P]
     L.lw_render_batch.argtypes = [P, P, C.c_uint32]
-    L.lw_render_hq_reference_port.argtypes = [P, P, P, C.c_uint64, C.c_uint32, P]
     L.lw_blend_chunky_sky.argtypes = [P, P, P, C.c_uint64, P, P, C.c_float]
     L.lw_adjoint_forward.argtypes = [P, C.POINTER(AdjFrame), C.c_uint32, P]
     L.lw_adjoint_backward.argtypes = [P, C.POINTER(AdjFrame), C.c_uint32, P, C.POINTER(Gradient)]
@@ -300,17 +299,6 @@ class Context:
         out = np.zeros((h, w, 3), np.float32)
         cb = PROGRESS_FN((lambda d, t, u: progress(d, t)) if progress else (lambda d, t, u: None))
         self._check(self.L.lw_render_hq(self.h, p.ctypes.data, _ptr(sky), sky.size, spp, cb, None, out.ctypes.data))
-        return out
-
-    def render_hq_reference_port(self, params, sky, spp):
-        """The reference's CUDA backend ported as written (the comparison baseline): mean radiance,
-        shape (h, w, 3)."""
-        p = self._params(params)
-        sky = np.ascontiguousarray(sky if sky is not None else np.zeros(0), np.float32)
-        w, h = int(p["frame"][0]), int(p["frame"][1])
-        out = np.zeros((h, w, 3), np.float32)
-        self._check(self.L.lw_render_hq_reference_port(self.h, p.ctypes.data, _ptr(sky), sky.size, spp,
-                                                        out.ctypes.data))
         return out
 
     def upload_sky(self, sky):
