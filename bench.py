@@ -12,8 +12,9 @@ device (CUDA events on the library's stream, max over ranks); ``e2e`` times the 
 ``render_hq`` call with host buffers (scene and sky uploaded, image read back) every step. With
 ``--impl reference`` the reference's CPU path (the CPU oracle, a restatement of the reference's
 kernel and CPU backend loop) is timed on the host cores on a bounded sample of the same frame.
-Under ``torchrun`` (N > 1) each rank renders its own range of samples of the frame (weak
-scaling) and the accumulators are summed to rank 0 with one NCCL reduce.
+Under ``torchrun`` (N > 1) the frame's spp is N x 1024 and each rank renders every sample of its
+1/N of the frame's 8x4-pixel tiles (weak scaling); one NCCL reduce of the accumulators per step,
+inside the timed region, gives rank 0 the frame bit for bit as one GPU renders it.
 
 At N = 1 the line also carries the north star's other forms, each on its own configuration and
 timed the same way (unless --no-extras): ``reference_cuda_port`` (the reference's CUDA backend
@@ -332,12 +333,16 @@ def run_reference(args, rank, world):
 
 class OracleSkyOnHost:
     """Sky inputs built on the host by the oracle (for the CPU reference arm, which must not need
-    a GPU): Chunky's sky cache, and the blend of Chunky's sky into the maps."""
+    a GPU): Chunky's sky cache, the game sky's maps, and the blend of Chunky's sky into them."""
 
     def build_sky_cache(self, params, n):
         from oracle import oracle as O
         v = O.OracleScene(params, None, None, None, None, None, None)
         return v.build_sky_cache(n)
+
+    def draw_sky_map(self, quick_sky, stars, w, h, atlas, atlas_w):
+        from oracle import oracle as O
+        return O.draw_sky_map(quick_sky, stars, w, h, atlas, atlas_w)
 
     def blend_chunky_sky(self, params, cache, maps, sizes, weight):
         from lumenwright_b200 import sky as SK
@@ -506,11 +511,19 @@ def main():
 
     from lumenwright_b200 import shard
 
+    # Under N ranks the frame's spp is N times the single GPU's and each rank renders every sample
+    # of 1/N of the frame's tiles (weak scaling: each rank's work is one frame at `spp`); one NCCL
+    # SUM reduce of the accumulator records per step, inside the timed region, gives rank 0 the
+    # frame bit for bit as one GPU would render it.
+    fspp = shard.frame_spp(spp, world)
+
     def device_step(i):
-        # Each rank renders its own sample range of the frame (weak scaling).
-        start, count = shard.sample_range(rank, world, spp, step=i)
         ctx.clear_accumulator(w, h)
-        ctx.render_device(p, start, count)
+        if dist:
+            ctx.render_device_shard(p, i * fspp, fspp, rank, world)
+            shard.reduce_accumulator(ctx, dist)
+        else:
+            ctx.render_device(p, i * spp, spp)
 
     for i in range(args.warmup):
         device_step(i)
@@ -538,8 +551,6 @@ def main():
         t = torch.tensor([total_ms], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms = float(t.item())
-        # The frame: every rank's mean over its samples, reduced to rank 0 (one NCCL reduce).
-        shard.reduce_means(ctx.read_accumulator(w, h), dist, device=f"cuda:{local}")
     value = samples_per_step * args.steps * world / (total_ms / 1e3) / 1e6
 
     # End to end through the public render_hq with host buffers, every step.
@@ -548,14 +559,16 @@ def main():
     h2d = frame.scene.memory_bytes() + frame.sky.nbytes + 432
     d2h = w * h * 3 * 4
     e2e_frame = frame
-    e2e_img = be.render_hq(e2e_frame).reshape(h, w, 3)  # warm-up (its image is checked below)
-    be._scene_key = None
+    # one GPU: the public render_hq; N ranks: the same calls with host buffers on each rank's tiles,
+    # the accumulators reduced and read back on rank 0 (shard.render_hq_sharded)
+    e2e_step = ((lambda: be.render_hq(e2e_frame).reshape(h, w, 3)) if not dist else
+                (lambda: shard.render_hq_sharded(be.ctx, e2e_frame, dist, rank, world, spp=fspp)))
+    e2e_img = e2e_step()  # warm-up (its image is checked below)
     if dist:
         dist.barrier()
     t0 = time.perf_counter()
     for i in range(args.steps):
-        be._scene_key = None  # upload the scene every step
-        be.render_hq(e2e_frame)
+        e2e_step()
     e2e_s = time.perf_counter() - t0
     if dist:
         import torch
@@ -592,7 +605,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "width": w, "height": h, "spp": spp, "bounces": int(p["frame"][3]),
-                       "parallelism": f"sample ranges x{world}" if world > 1 else "1 GPU",
+                       "parallelism": f"interleaved tiles x{world}, frame spp {fspp}" if world > 1 else "1 GPU",
                        "engine": "wavefront", "tuning": ctx.get_tuning(),
                        "l2": "the scene and sky maps (~30 MB) stay L2-resident by design; the path slots "
                              "(up to 2.7 GB) and the partial sums are larger than L2",

@@ -69,7 +69,7 @@ typedef enum {
     LW_ERR_BUFFER_LENGTH = 2,    /* a buffer shorter than the layout it must hold, or an index
                                     in one buffer that points outside another */
     LW_ERR_OUT_OF_MEMORY = 3,
-    LW_ERR_DEVICE_TIMEOUT = 4, /* a bounded wait on the device ran out */
+    LW_ERR_DEVICE_TIMEOUT = 4, /* a wait for the GPU ran past the deadline of lw_set_timeout */
     LW_ERR_LAUNCH = 5,         /* a CUDA launch or copy failed */
     LW_ERR_CANCELLED = 6,      /* lw_cancel was called during the render */
     LW_ERR_NO_DEVICE = 7,      /* no CUDA device, or not an sm_100 one */
@@ -167,6 +167,14 @@ lw_status lw_get_tuning(const lw_ctx *ctx, lw_tuning *out);
  * launches done before the cancel, and each record's count (its fourth float) tells how many
  * samples. The next render on `ctx` starts uncancelled. */
 void lw_cancel(lw_ctx *ctx);
+/* A deadline, in seconds, for every wait of a call on `ctx` for its render's work on the GPU
+ * (0, the default: no limit). The reference's CUDA backend waits without a limit for each batch
+ * (crates/lumenwright/src/render/cuda.rs:154-159). With a deadline, a wait polls the work's
+ * completion; if the deadline passes first, the render's kernels are cancelled as lw_cancel
+ * cancels them, the call waits at most 10 s more for them to end, and it returns
+ * LW_ERR_DEVICE_TIMEOUT (the accumulator then holds the launches done before, as after a cancel).
+ * The next render on `ctx` starts uncancelled. */
+lw_status lw_set_timeout(lw_ctx *ctx, double seconds);
 /* Records timing mark `slot` (0..7), a CUDA event on the context's stream, and reads the time
  * between two marks once both are reached (the device's clock, not the host's). */
 lw_status lw_mark(lw_ctx *ctx, uint32_t slot);
@@ -243,6 +251,21 @@ lw_status lw_clear_accumulator(lw_ctx *ctx, uint32_t width, uint32_t height);
 lw_status lw_render_device(lw_ctx *ctx, const lw_params *params, uint32_t sample_start, uint32_t spp);
 lw_status lw_read_accumulator(lw_ctx *ctx, float *out_rgb);
 
+/* One shard of a frame split over GPUs (one process and context per GPU): the samples
+ * [sample_start, sample_start + spp) of the frame's 8x4-pixel tiles shard, shard + shards,
+ * shard + 2 shards, ... (tiles numbered row by row), added to the context's accumulator. Every
+ * (pixel, sample) is independent (crates/lumenwright-kernel/src/rng.rs:23-27) and a pixel's sums
+ * depend only on its own samples, so a pixel's record is the one a render of the whole frame
+ * gives, bit for bit; the other pixels' records are left as they are (zero after
+ * lw_clear_accumulator), so a sum of the shards' accumulators over the GPUs (an NCCL reduce of the
+ * records lw_accumulator_device names) is exactly the whole frame's accumulator. */
+lw_status lw_render_device_shard(lw_ctx *ctx, const lw_params *params, uint32_t sample_start, uint32_t spp, uint32_t shard,
+                                 uint32_t shards);
+/* The context's device accumulator: frame[0] * frame[1] records of 8 floats (Kahan sum r, g, b,
+ * sample count; compensation r, g, b, unused), valid until the next lw_clear_accumulator or
+ * render of another frame size; for a caller that combines accumulators across GPUs. */
+lw_status lw_accumulator_device(lw_ctx *ctx, void **records, uint32_t *width, uint32_t *height);
+
 /* ---- the batched form ----------------------------------------------------------------------
  * Many cameras of uneven resolution and spp over the uploaded scene in one persistent launch:
  * every camera's work items go into one queue, so the GPU stays full until the last sample of
@@ -314,6 +337,25 @@ lw_status lw_build_sky_cache(lw_ctx *ctx, const lw_params *params, uint32_t n, f
  * map in `maps` (sizes lens w, h, light w, h), in place: weight * chunky + (1 - weight) * map. */
 lw_status lw_blend_chunky_sky(lw_ctx *ctx, const lw_params *params, const float *cache, uint64_t cache_len,
                               float *maps, const float sizes[4], float weight);
+
+/* The game's sky (SkyLook::Game, or a day weight below 1): the client's sky drawn into the two
+ * equirectangular maps the kernel's `sky_lens` / `sky_light` read (crates/lumenwright/src/render/
+ * sky.rs:855-952), which the reference draws on the host per frame. `lw_quick_sky` is `QuickSky`
+ * (sky.rs:274-305), 608 bytes, as `QuickSky::new` packs it (its camera fields are not read). */
+typedef struct {
+    float sky_color[4], fog_color[4], fog_dist[4], sunrise[4], flags[4];
+    float sun[4][4], moon[4][4], star_rot[3][4], fan[18][4];
+    float cam_forward[4], cam_right[4], cam_up[4], cam_misc[4];
+} lw_quick_sky;
+/* `draw_map` (sky.rs:861-878): `QuickSky::background` (sky.rs:509-530: the fog colour, the sky
+ * disc, the sunrise glow, the sun and moon sprites from `atlas`, the stars of `stars`, the table
+ * `star_table` builds, sky.rs:158-217) for the direction of every texel of a w x h map (row 0 at
+ * the nadir, `map_direction`, sky.rs:853-858), decoded to linear with c^2.2, into out (w * h * 3
+ * floats). `atlas` is atlas_len RGBA8 texels, atlas_w a row; the sun's and moon's rectangles must
+ * lie inside it. */
+lw_status lw_draw_sky_map(lw_ctx *ctx, const lw_quick_sky *sky, const uint32_t *stars, uint64_t stars_len,
+                          const uint32_t *atlas, uint64_t atlas_len, uint32_t atlas_w, uint32_t w, uint32_t h,
+                          float *out);
 
 /* ---- the display pass ---------------------------------------------------------------------------
  * `post::tonemap` / `post::tonemap_mix` (crates/lumenwright/src/render/post.rs:152-217) on the

@@ -16,6 +16,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from . import gamesky as G
 from . import request as R
 from . import sky as SK
 from . import synth as S
@@ -82,7 +83,8 @@ def c3_jobs(sky_backend, cams=None, spp_scale=1.0):
             if weight >= 1.0:
                 skies[c.time] = (cache, None)
             else:
-                maps, sizes = SK.synthetic_game_maps(sun_dir)
+                desc, factor, colour = G.stated_sky(c.time, hq.sun_sprite)
+                maps, sizes, _ = G.game_sky_maps(sky_backend, desc, factor, colour, hq.atlas, hq.atlas_size[0])
                 maps = sky_backend.blend_chunky_sky(p, cache, maps, sizes, weight)
                 skies[c.time] = (maps, sizes)
         sky, sizes = skies[c.time]

@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/lumenwright_b200.h"
@@ -19,6 +20,7 @@ using namespace lw;
 
 static_assert(sizeof(lw_params) == sizeof(DevParams), "Params layout");
 static_assert(sizeof(lw_quad) == 80 && sizeof(lw_model) == 16 && sizeof(lw_emitter) == 32, "record layout");
+static_assert(sizeof(lw_quick_sky) == 608, "QuickSky layout");
 
 namespace {
 
@@ -95,6 +97,8 @@ struct lw_ctx {
     DBuf<uint32_t> cancel_word;      // device word the render kernel polls; set by lw_cancel
     cudaStream_t aux = nullptr;      // lw_cancel's stream, so the write lands while a render runs
     cudaEvent_t cancel_ev = nullptr; // recorded on `aux` after each cancel's write
+    double timeout_s = 0.0;          // deadline of every wait on the render's work (0: none)
+    cudaEvent_t wait_ev = nullptr;   // marks the work a bounded wait waits for
     cudaStream_t cap = nullptr;      // the stream a graph's loop body is captured on
     lw_stats stats{};
     lw_tuning tuning{128, 0, 0, LW_ENGINE_WAVEFRONT, 0};
@@ -184,6 +188,61 @@ lw_status begin_render(lw_ctx *c) {
     CK(c, cudaMemsetAsync(c->cancel_word.p, 0, 4, c->stream), "clearing the cancel word");
     return LW_OK;
 }
+
+// The device half of lw_cancel: the cancel word on the aux stream, which the render kernels poll.
+void cancel_device(lw_ctx *c) {
+    __atomic_store_n(c->cancel_host, 1, __ATOMIC_RELAXED);
+    cudaMemsetAsync(c->cancel_word.p, 0xFF, 4, c->aux);  // lands while a render kernel runs
+    cudaEventRecord(c->cancel_ev, c->aux);               // the next render's clear waits for it
+}
+
+// How long a wait that ran out gives the cancelled kernels to end before it returns anyway.
+constexpr double kDrainSeconds = 10.0;
+
+// Waits for event `ev`. With a deadline set (lw_set_timeout) the wait is a poll of the event
+// against it: spinning briefly, then sleeping 50 us between polls. If the deadline passes first,
+// the render's kernels are cancelled (they stop taking work at their next poll of the cancel
+// word), the wait goes on for at most kDrainSeconds more for them to end, and the call returns
+// LW_ERR_DEVICE_TIMEOUT; the results of the render are then incomplete.
+lw_status wait_event(lw_ctx *c, cudaEvent_t ev, const char *what) {
+    if (c->timeout_s <= 0.0) {
+        CK(c, cudaEventSynchronize(ev), what);
+        return LW_OK;
+    }
+    using clock = std::chrono::steady_clock;
+    const auto deadline = clock::now() + std::chrono::duration<double>(c->timeout_s);
+    for (unsigned polls = 0;; polls++) {
+        cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return LW_OK;
+        if (e != cudaErrorNotReady) return cuda_fail(c, e, what);
+        if (clock::now() >= deadline) break;
+        if (polls < 64) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+    cancel_device(c);
+    const auto drain = clock::now() + std::chrono::duration<double>(kDrainSeconds);
+    cudaError_t e = cudaEventQuery(ev);
+    while (e == cudaErrorNotReady && clock::now() < drain) {
+        std::this_thread::sleep_for(std::chrono::milliseconds(1));
+        e = cudaEventQuery(ev);
+    }
+    if (e != cudaSuccess && e != cudaErrorNotReady) return cuda_fail(c, e, what);
+    return fail(c, LW_ERR_DEVICE_TIMEOUT, "%s: not done within the %.6g s deadline; %s", what, c->timeout_s,
+                e == cudaSuccess ? "its kernels were stopped and have ended"
+                                 : "its kernels were asked to stop and had not ended 10 s later");
+}
+
+// Waits for the work queued on the context's stream so far (see wait_event).
+lw_status wait_stream(lw_ctx *c, const char *what) {
+    CK(c, cudaEventRecord(c->wait_ev, c->stream), "recording an event");
+    return wait_event(c, c->wait_ev, what);
+}
+
+#define WAIT(c, what)                                \
+    do {                                             \
+        lw_status ws_ = wait_stream((c), (what));    \
+        if (ws_ != LW_OK) return ws_;                \
+    } while (0)
 
 // After the wait for a render's results: a cancel that came while the kernels ran (after the last
 // check between launches) may have stopped them before the last sample, so the results are
@@ -291,7 +350,10 @@ Plan plan(const lw_ctx *c, uint64_t n_slots, uint32_t spp, uint32_t sub_override
     return Plan{(uint32_t)sub, (uint32_t)batch};
 }
 
-WorkDesc work(lw_ctx *c, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t spp, uint32_t sub) {
+// A launch over the rectangle's 8x4-pixel tiles shard, shard + shards, shard + 2 shards, ...
+// (all of them for shard 0 of 1).
+WorkDesc work(lw_ctx *c, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint32_t s0, uint32_t spp, uint32_t sub,
+              uint32_t shard = 0, uint32_t shards = 1) {
     WorkDesc W{};
     W.x0 = x0;
     W.y0 = y0;
@@ -299,7 +361,10 @@ WorkDesc work(lw_ctx *c, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h, uint3
     W.h = h;
     W.tiles_x = (w + 7) / 8;
     uint32_t tiles_y = (h + 3) / 4;
-    W.n_slots = W.tiles_x * tiles_y * 32u;
+    const uint32_t tiles = W.tiles_x * tiles_y;
+    W.tile_step = shards;
+    W.tile_first = shard;
+    W.n_slots = (tiles > shard ? (tiles - shard + shards - 1) / shards : 0u) * 32u;
     W.sample_start = s0;
     W.spp = spp;
     W.sub = sub;
@@ -430,7 +495,7 @@ lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const 
         if ((t & 15u) == 15u) {
             CK(c, cudaMemcpyAsync(c->wf_host, F.ctr + 4 * (t % 3u), 4, cudaMemcpyDeviceToHost, c->stream),
                "reading the queue length");
-            CK(c, cudaStreamSynchronize(c->stream), "running the iterations");
+            WAIT(c, "running the iterations");
             for (int k = 0; k < 16; k++) {
                 float a = 0.f, b = 0.f;
                 cudaEventElapsedTime(&a, c->wf_ev[3 * k], c->wf_ev[3 * k + 1]);
@@ -450,9 +515,10 @@ lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const 
 // Launches the accumulating render of samples [s0, s0 + spp) over the whole frame, in batches.
 // With `progress`, each batch is waited for and reported; without it nothing waits.
 lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32_t spp, lw_progress_fn progress,
-                         void *user, uint32_t progress_total) {
+                         void *user, uint32_t progress_total, uint32_t shard = 0, uint32_t shards = 1) {
     const uint32_t w = params->frame[0], h = params->frame[1];
-    WorkDesc probe = work(c, 0, 0, w, h, 0, 1, 1);
+    WorkDesc probe = work(c, 0, 0, w, h, 0, 1, 1, shard, shards);
+    if (probe.n_slots == 0) return LW_OK;  // a shard with no tile of the frame
     Plan pl = plan(c, probe.n_slots, spp);
     if (c->tuning.engine == LW_ENGINE_WAVEFRONT && c->tuning.sub == 0) {
         // Items of one sample: a slot that ends a sample takes the next item at once, and when the
@@ -467,7 +533,7 @@ lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32
     uint32_t done = 0;
     while (done < spp) {
         uint32_t n = spp - done < pl.batch ? spp - done : pl.batch;
-        WorkDesc W = work(c, 0, 0, w, h, s0 + done, n, pl.sub);
+        WorkDesc W = work(c, 0, 0, w, h, s0 + done, n, pl.sub, shard, shards);
         CK(c, cudaMemsetAsync(c->counter.p, 0, sizeof(uint32_t), c->stream), "clearing the work counter");
         CK(c, cudaEventRecord(c->ev_a, c->stream), "recording an event");
         if (c->tuning.engine == LW_ENGINE_WAVEFRONT) {
@@ -482,7 +548,10 @@ lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32
         c->stats.samples += (uint64_t)w * h * n;
         done += n;
         if (progress || done < spp) {
-            CK(c, cudaEventSynchronize(c->ev_b), "waiting for the render kernel");
+            {
+                lw_status ws = wait_event(c, c->ev_b, "waiting for the render kernel");
+                if (ws != LW_OK) return ws;
+            }
             float ms = 0.f;
             cudaEventElapsedTime(&ms, c->ev_a, c->ev_b);
             c->stats.kernel_ms += ms;
@@ -584,7 +653,9 @@ lw_status lw_ctx_create(int device, lw_ctx **out) {
         if ((e = cudaEventCreate(&m)) != cudaSuccess) return bail(e, "creating events");
     c->cancel_host = new int(0);
     if ((e = cudaStreamCreateWithFlags(&c->aux, cudaStreamNonBlocking)) != cudaSuccess) return bail(e, "creating a stream");
-    if ((e = cudaEventCreateWithFlags(&c->cancel_ev, cudaEventDisableTiming)) != cudaSuccess) return bail(e, "creating events");
+    if ((e = cudaEventCreateWithFlags(&c->cancel_ev, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&c->wait_ev, cudaEventDisableTiming)) != cudaSuccess)
+        return bail(e, "creating events");
     if ((e = ensure(c->cancel_word, 1)) != cudaSuccess) return bail(e, "allocating the cancel word");
     if ((e = cudaMemset(c->cancel_word.p, 0, 4)) != cudaSuccess) return bail(e, "clearing the cancel word");
     float lut[256];
@@ -648,6 +719,7 @@ void lw_ctx_destroy(lw_ctx *c) {
     c->cancel_word.free_();
     if (c->aux) cudaStreamDestroy(c->aux);
     if (c->cancel_ev) cudaEventDestroy(c->cancel_ev);
+    if (c->wait_ev) cudaEventDestroy(c->wait_ev);
     if (c->cap) cudaStreamDestroy(c->cap);
     if (c->ev_a) cudaEventDestroy(c->ev_a);
     if (c->ev_b) cudaEventDestroy(c->ev_b);
@@ -663,10 +735,15 @@ void *lw_stream(lw_ctx *c) { return c ? (void *)c->stream : nullptr; }
 
 void lw_cancel(lw_ctx *c) {
     if (!c || !c->cancel_host) return;
-    __atomic_store_n(c->cancel_host, 1, __ATOMIC_RELAXED);
     cudaSetDevice(c->device);
-    cudaMemsetAsync(c->cancel_word.p, 0xFF, 4, c->aux);  // lands while a render kernel runs
-    cudaEventRecord(c->cancel_ev, c->aux);               // the next render's clear waits for it
+    cancel_device(c);
+}
+
+lw_status lw_set_timeout(lw_ctx *c, double seconds) {
+    if (!c) return LW_ERR_INVALID_ARGUMENT;
+    if (!(seconds >= 0.0) || seconds > 1e6) return fail(c, LW_ERR_INVALID_ARGUMENT, "timeout %g s", seconds);
+    c->timeout_s = seconds;
+    return LW_OK;
 }
 
 lw_status lw_set_tuning(lw_ctx *c, const lw_tuning *t) {
@@ -877,6 +954,31 @@ lw_status lw_render_device(lw_ctx *c, const lw_params *params, uint32_t sample_s
     return render_batches(c, params, sample_start, spp, nullptr, nullptr, spp);
 }
 
+lw_status lw_render_device_shard(lw_ctx *c, const lw_params *params, uint32_t sample_start, uint32_t spp, uint32_t shard,
+                                 uint32_t shards) {
+    if (!c) return LW_ERR_INVALID_ARGUMENT;
+    if (shards == 0 || shard >= shards) return fail(c, LW_ERR_INVALID_ARGUMENT, "shard %u of %u", shard, shards);
+    cudaSetDevice(c->device);
+    lw_status s = check_params(c, params, true);
+    if (s != LW_OK) return s;
+    if (c->acc_w != params->frame[0] || c->acc_h != params->frame[1])
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "the accumulator is %ux%u, the frame %ux%u", c->acc_w, c->acc_h, params->frame[0], params->frame[1]);
+    if (spp == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "spp is 0");
+    s = begin_render(c);
+    if (s != LW_OK) return s;
+    reset_stats(c);
+    return render_batches(c, params, sample_start, spp, nullptr, nullptr, spp, shard, shards);
+}
+
+lw_status lw_accumulator_device(lw_ctx *c, void **records, uint32_t *width, uint32_t *height) {
+    if (!c || !records) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument");
+    if (!c->acc_w) return fail(c, LW_ERR_INVALID_ARGUMENT, "no accumulator");
+    *records = c->acc.p;
+    if (width) *width = c->acc_w;
+    if (height) *height = c->acc_h;
+    return LW_OK;
+}
+
 lw_status lw_render_accumulate_noalloc(lw_ctx *c, const lw_params *params, uint32_t sample_start, uint32_t spp,
                                        void *accum) {
     if (!c || !params || !accum || spp == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "null argument or spp 0");
@@ -932,7 +1034,7 @@ lw_status lw_read_accumulator(lw_ctx *c, float *out_rgb) {
     CK(c, ensure(c->out_rgb, 3 * n), "allocating the output");
     CK(c, launch_finalize(c->acc.p, (uint32_t)n, c->out_rgb.p, c->stream), "launching the finalize kernel");
     CK(c, cudaMemcpyAsync(out_rgb, c->out_rgb.p, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "reading the image");
-    CK(c, cudaStreamSynchronize(c->stream), "reading the image");
+    WAIT(c, "reading the image");
     return check_cancelled(c);
 }
 
@@ -972,7 +1074,7 @@ lw_status lw_render_samples(lw_ctx *c, const lw_params *params, uint32_t x0, uin
     CK(c, cudaMemsetAsync(c->counter.p, 0, 4, c->stream), "clearing the work counter");
     CK(c, launch_render(MODE_SAMPLES, dev_scene(c), dev_params(params), W, c->shape_samples, c->stream), "launching the render kernel");
     CK(c, cudaMemcpyAsync(out, c->samples.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream), "reading the samples");
-    CK(c, cudaStreamSynchronize(c->stream), "rendering samples");
+    WAIT(c, "rendering samples");
     return check_cancelled(c);
 }
 
@@ -989,7 +1091,7 @@ lw_status lw_trace_rays(lw_ctx *c, const lw_params *params, uint32_t n, const fl
     CK(c, launch_trace_rays(dev_scene(c), dev_params(params), n, c->rays.p, c->rays.p + 3 * (size_t)n, tmin, tmax, c->hits.p, c->stream),
        "launching the trace kernel");
     CK(c, cudaMemcpyAsync(out, c->hits.p, sizeof(lw_hit) * (size_t)n, cudaMemcpyDeviceToHost, c->stream), "reading hits");
-    CK(c, cudaStreamSynchronize(c->stream), "tracing rays");
+    WAIT(c, "tracing rays");
     return LW_OK;
 }
 
@@ -1162,7 +1264,7 @@ lw_status lw_batch_read(lw_ctx *c) {
         CK(c, cudaMemcpyAsync(j.out_rgb, c->batch_out.p + 3 * c->batch_out_off[i], n * 4, cudaMemcpyDeviceToHost, c->stream),
            "reading an image");
     }
-    CK(c, cudaStreamSynchronize(c->stream), "reading the images");
+    WAIT(c, "reading the images");
     return check_cancelled(c);
 }
 
@@ -1215,6 +1317,44 @@ lw_status lw_blend_chunky_sky(lw_ctx *c, const lw_params *params, const float *c
     cbuf.free_();
     mbuf.free_();
     if (e != cudaSuccess) return cuda_fail(c, e, "blending the sky maps");
+    return LW_OK;
+}
+
+lw_status lw_draw_sky_map(lw_ctx *c, const lw_quick_sky *q, const uint32_t *stars, uint64_t stars_len,
+                          const uint32_t *atlas, uint64_t atlas_len, uint32_t atlas_w, uint32_t w, uint32_t h, float *out) {
+    if (!c || !q || !stars || !atlas || !out || !w || !h || !atlas_w || w > 16384 || h > 16384)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "bad argument");
+    cudaSetDevice(c->device);
+    // The star table: bin starts (non-decreasing) and an end, then 9 words per entry.
+    const uint64_t nb = 128u * 64u;
+    if (stars_len < nb + 1) return fail(c, LW_ERR_BUFFER_LENGTH, "the star table is shorter than its bins");
+    for (uint64_t b = 0; b < nb; b++)
+        if (stars[b + 1] < stars[b]) return fail(c, LW_ERR_BUFFER_LENGTH, "star bin %llu ends before it starts", (unsigned long long)b);
+    if (nb + 1 + (uint64_t)stars[nb] * 9u > stars_len)
+        return fail(c, LW_ERR_BUFFER_LENGTH, "the star table's bins name %u entries it does not hold", stars[nb]);
+    // The sun's and moon's sprite rectangles: every texel the quads can read lies in the atlas.
+    for (const float(*b)[4] : {q->sun, q->moon}) {
+        if (b[0][3] == 0.0f || !(b[3][2] > 0.0f)) continue;
+        const double x = b[3][0], y = b[3][1], bw = b[3][2], bh = b[3][3];
+        if (!(x >= 0.0 && y >= 0.0 && bh >= 0.0) || std::floor(x + bw) >= (double)atlas_w ||
+            std::floor(y + bh) * atlas_w + std::floor(x + bw) >= (double)atlas_len)
+            return fail(c, LW_ERR_BUFFER_LENGTH, "a sprite rectangle (%g, %g, %g, %g) reaches outside the %ux%llu atlas", x, y,
+                        bw, bh, atlas_w, (unsigned long long)(atlas_len / atlas_w));
+    }
+    DBuf<uint32_t> dstars, datlas;
+    DBuf<float> dout;
+    cudaError_t e = ensure(dstars, stars_len);
+    if (e == cudaSuccess) e = ensure(datlas, atlas_len);
+    if (e == cudaSuccess) e = ensure(dout, (size_t)w * h * 3);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dstars.p, stars, stars_len * 4, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(datlas.p, atlas, atlas_len * 4, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = launch_sky_map(q, datlas.p, atlas_w, dstars.p, w, h, dout.p, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout.p, (size_t)w * h * 12, cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    dstars.free_();
+    datlas.free_();
+    dout.free_();
+    if (e != cudaSuccess) return cuda_fail(c, e, "drawing the sky map");
     return LW_OK;
 }
 
@@ -1296,7 +1436,10 @@ lw_status adj_timed(lw_ctx *c, cudaError_t (*launch)(lw_ctx *, void *), void *ar
     CK(c, cudaEventRecord(c->ev_a, c->stream), "recording an event");
     CK(c, launch(c, arg), "launching the adjoint kernel");
     CK(c, cudaEventRecord(c->ev_b, c->stream), "recording an event");
-    CK(c, cudaEventSynchronize(c->ev_b), "running the adjoint kernel");
+    {
+        lw_status ws = wait_event(c, c->ev_b, "running the adjoint kernel");
+        if (ws != LW_OK) return ws;
+    }
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, c->ev_a, c->ev_b);
     c->stats.kernel_ms = ms;
@@ -1433,7 +1576,7 @@ lw_status lw_read_accumulator_rgba(lw_ctx *c, const lw_tonemap *tm, uint32_t *ou
     CK(c, cudaMemcpyAsync(out_rgba, c->out_rgba.p, 4 * n, cudaMemcpyDeviceToHost, c->stream), "reading the pixels");
     if (out_rgb)
         CK(c, cudaMemcpyAsync(out_rgb, c->out_rgb.p, 12 * n, cudaMemcpyDeviceToHost, c->stream), "reading the image");
-    CK(c, cudaStreamSynchronize(c->stream), "reading the pixels");
+    WAIT(c, "reading the pixels");
     return check_cancelled(c);
 }
 

@@ -13,7 +13,9 @@ namespace lw {
 struct WorkDesc {
     uint32_t x0, y0, w, h;       // the rectangle
     uint32_t tiles_x;            // 8x4-pixel tiles per rectangle row
-    uint32_t n_slots;            // pixel slots: tiles * 32
+    uint32_t tile_step, tile_first;  // the launch's tiles: tile_first, tile_first + tile_step, ...
+                                     // (one shard of a frame split over GPUs; 1, 0 for all tiles)
+    uint32_t n_slots;            // pixel slots: the launch's tiles * 32
     uint32_t sample_start, spp;  // the launch's samples
     uint32_t sub;                // samples per item
     uint32_t n_sub;              // items per pixel: ceil(spp / sub)
@@ -76,6 +78,8 @@ cudaError_t launch_water_exp(uint64_t n, const float *x, float *out, cudaStream_
 cudaError_t launch_sky_cache(const DevParams &P, uint32_t n, float *out, cudaStream_t st);
 cudaError_t launch_blend_chunky(const DevScene &S, const DevParams &P, float *map, uint32_t w, uint32_t h, float weight,
                                 cudaStream_t st);
+cudaError_t launch_sky_map(const void *quick_sky, const uint32_t *atlas, uint32_t atlas_w, const uint32_t *stars,
+                           uint32_t w, uint32_t h, float *out, cudaStream_t st);
 
 // batch.cu
 LaunchShape batch_shape(int device, int threads, bool resume);

@@ -59,7 +59,7 @@ k_render(const DevScene S, const DevParams P, const WorkDesc W) {
                 } else {
                     j = item / W.n_slots;
                     slot = item - j * W.n_slots;
-                    uint32_t tile = slot >> 5, in = slot & 31u;
+                    uint32_t tile = (slot >> 5) * W.tile_step + W.tile_first, in = slot & 31u;
                     uint32_t rx = (tile % W.tiles_x) * 8u + (in & 7u);
                     uint32_t ry = (tile / W.tiles_x) * 4u + (in >> 3);
                     if (rx < W.w && ry < W.h) {
@@ -156,7 +156,7 @@ k_render(const DevScene S, const DevParams P, const WorkDesc W) {
 __global__ void k_reduce(const WorkDesc W, Accum *acc, uint32_t frame_w) {
     uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= W.n_slots || *W.cancel) return;
-    uint32_t tile = slot >> 5, in = slot & 31u;
+    uint32_t tile = (slot >> 5) * W.tile_step + W.tile_first, in = slot & 31u;
     uint32_t rx = (tile % W.tiles_x) * 8u + (in & 7u);
     uint32_t ry = (tile / W.tiles_x) * 4u + (in >> 3);
     if (rx >= W.w || ry >= W.h) return;
@@ -253,6 +253,7 @@ cudaError_t launch_render(int mode, const DevScene &S, const DevParams &P, const
 }
 
 cudaError_t launch_reduce(const WorkDesc &W, Accum *acc, uint32_t frame_w, cudaStream_t st) {
+    if (W.n_slots == 0) return cudaSuccess;
     k_reduce<<<(W.n_slots + 255) / 256, 256, 0, st>>>(W, acc, frame_w);
     return cudaGetLastError();
 }

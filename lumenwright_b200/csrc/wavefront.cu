@@ -140,7 +140,7 @@ struct ItemRef {
 template <bool BATCH>
 LW_DI ItemRef decode_item(const WorkDesc &W, const BatchDesc &B, uint32_t item) {
     ItemRef r{};
-    uint32_t n_slots, tiles_x, w, h, x0 = 0, y0 = 0, sample_start, spp, sub, local = item;
+    uint32_t n_slots, tiles_x, w, h, x0 = 0, y0 = 0, sample_start, spp, sub, local = item, step = 1, first = 0;
     if (BATCH) {
         r.job = find_job(B.item_begin, B.n_jobs, item);
         const DevJob &J = B.jobs[r.job];
@@ -149,11 +149,12 @@ LW_DI ItemRef decode_item(const WorkDesc &W, const BatchDesc &B, uint32_t item) 
         sample_start = J.sample_start, spp = J.spp, sub = J.sub;
     } else {
         n_slots = W.n_slots, tiles_x = W.tiles_x, w = W.w, h = W.h, x0 = W.x0, y0 = W.y0;
+        step = W.tile_step, first = W.tile_first;
         sample_start = W.sample_start, spp = W.spp, sub = W.sub;
     }
     r.j = local / n_slots;
     r.pslot = local - r.j * n_slots;
-    uint32_t tile = r.pslot >> 5, in = r.pslot & 31u;
+    uint32_t tile = (r.pslot >> 5) * step + first, in = r.pslot & 31u;
     uint32_t rx = (tile % tiles_x) * 8u + (in & 7u);
     uint32_t ry = (tile / tiles_x) * 4u + (in >> 3);
     r.valid = rx < w && ry < h;

@@ -31,7 +31,8 @@ EXPORTS = (
     "lw_blend_chunky_sky", "lw_render_accumulate_noalloc", "lw_batch_prepare",
     "lw_batch_run", "lw_batch_read", "lw_render_batch", "lw_adjoint_forward", "lw_adjoint_backward", "lw_adjoint_fd",
     "lw_gamma_table", "lw_tonemap_rgba", "lw_read_accumulator_rgba", "lw_scene_build_keys", "lw_scene_build_grid",
-    "lw_scene_read", "lw_water_exp",
+    "lw_scene_read", "lw_water_exp", "lw_draw_sky_map", "lw_set_timeout", "lw_render_device_shard",
+    "lw_accumulator_device",
 )
 
 # lw_tonemap operators (post.rs `Tonemap`)
@@ -163,6 +164,10 @@ def load(path: str = LIB_PATH):
     L.lw_trace_rays.argtypes = [P, P, C.c_uint32, P, P, C.c_float, C.c_float, P]
     L.lw_voxel_lookup.argtypes = [P, C.c_uint32, P, P]
     L.lw_water_exp.argtypes = [P, C.c_uint64, P, P]
+    L.lw_set_timeout.argtypes = [P, C.c_double]
+    L.lw_render_device_shard.argtypes = [P, P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
+    L.lw_accumulator_device.argtypes = [P, C.POINTER(P), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+    L.lw_draw_sky_map.argtypes = [P, P, P, C.c_uint64, P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, P]
     L.lw_build_sky_cache.argtypes = [P, P, C.c_uint32, P]
     L.lw_render_accumulate_noalloc.argtypes = [P, P, C.c_uint32, C.c_uint32, P]
     L.lw_batch_prepare.argtypes = [P, P, C.c_uint32]
@@ -239,6 +244,11 @@ class Context:
     def cancel(self):
         self.L.lw_cancel(self.h)
 
+    def set_timeout(self, seconds: float):
+        """A deadline for every wait on the GPU's work (0: none); past it a call returns
+        LW_ERR_DEVICE_TIMEOUT after stopping its kernels."""
+        self._check(self.L.lw_set_timeout(self.h, float(seconds)))
+
     def set_tuning(self, threads=None, budget=None, sub=None, engine=None, paths=None):
         """Launch tuning of the render (see `lw_tuning`); the knobs not given keep their values."""
         t = self.get_tuning()
@@ -312,6 +322,18 @@ class Context:
         p = self._params(params)
         self._keep = [p]
         self._check(self.L.lw_render_device(self.h, p.ctypes.data, sample_start, spp))
+
+    def render_device_shard(self, params, sample_start, spp, shard, shards):
+        """Samples of the frame's tiles shard, shard + shards, ... added to the accumulator."""
+        p = self._params(params)
+        self._keep = [p]
+        self._check(self.L.lw_render_device_shard(self.h, p.ctypes.data, sample_start, spp, shard, shards))
+
+    def accumulator_device(self):
+        """(device address, width, height) of the context's accumulator records (8 floats each)."""
+        ptr, w, h = C.c_void_p(), C.c_uint32(), C.c_uint32()
+        self._check(self.L.lw_accumulator_device(self.h, C.byref(ptr), C.byref(w), C.byref(h)))
+        return ptr.value, w.value, h.value
 
     def render_accumulate_noalloc(self, params, sample_start, spp, accum_device_ptr: int):
         """Adds samples to a caller-owned device accumulator (w*h records of 8 floats) without
@@ -398,6 +420,17 @@ class Context:
         p = self._params(params)
         out = np.zeros((n + 1) * (n + 1) * 3, np.float32)
         self._check(self.L.lw_build_sky_cache(self.h, p.ctypes.data, n, out.ctypes.data))
+        return out
+
+    def draw_sky_map(self, quick_sky, stars, w, h, atlas, atlas_w):
+        """`draw_map` (sky.rs:861-878) of a packed `QuickSky` (``gamesky.QUICK_SKY_DTYPE``) on the
+        device: (h, w, 3) linear RGB, row 0 at the nadir."""
+        q = np.ascontiguousarray(quick_sky)
+        stars = np.ascontiguousarray(stars, np.uint32)
+        atlas = np.ascontiguousarray(atlas, np.uint32)
+        out = np.zeros((h, w, 3), np.float32)
+        self._check(self.L.lw_draw_sky_map(self.h, q.ctypes.data, stars.ctypes.data, stars.size, atlas.ctypes.data,
+                                           atlas.size, atlas_w, w, h, out.ctypes.data))
         return out
 
     def blend_chunky_sky(self, params, cache, maps, sizes, weight):
@@ -530,7 +563,6 @@ class B200Backend:
 
     def __init__(self, device: int = 0):
         self.ctx = Context(device)
-        self._scene_key = None
 
     def name(self) -> str:
         return f"b200 device {self.ctx.device} (cuda, sm_100a)"
@@ -540,12 +572,11 @@ class B200Backend:
 
     def render_hq(self, frame, progress=None) -> np.ndarray:
         """Mean linear radiance per pixel, row-major from the top row, as (w*h, 3) float32
-        (the reference's `Vec<[f32; 3]>`). The scene is uploaded once and kept while the same
-        `HqScene` object is drawn again."""
-        key = id(frame.scene)
-        if key != self._scene_key:
-            self.ctx.upload_hq_scene(frame.scene)
-            self._scene_key = key
+        (the reference's `Vec<[f32; 3]>`). The scene is copied to the device for every frame, as
+        `CudaBackend` copies it (cuda.rs:96-111): a cache keyed by the scene object's identity
+        would draw a new scene at a reused address, or one changed in place, from stale buffers,
+        and a content hash of the scene takes longer than its copy."""
+        self.ctx.upload_hq_scene(frame.scene)
         img = self.ctx.render_hq(frame.params, frame.sky, max(int(frame.spp), 1), progress)
         return img.reshape(-1, 3)
 

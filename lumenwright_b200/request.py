@@ -9,6 +9,7 @@ from typing import Optional
 
 import numpy as np
 
+from . import gamesky as G
 from . import layout as L
 from . import sky as SK
 from . import synth as S
@@ -138,8 +139,10 @@ def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None)
     """The hq frame of a configuration, as `render()` assembles it (request.rs:640-653, 751-930).
 
     ``sky_backend`` builds the sky inputs: an object with ``build_sky_cache(params, n)`` (`sky_cache`,
-    crates/lumenwright/src/render/sky.rs:593-611) and ``blend_chunky_sky(params, cache, maps,
-    sizes, weight)`` (sky.rs:836-850); by default the library's device kernels on device 0.
+    crates/lumenwright/src/render/sky.rs:593-611), ``draw_sky_map(quick_sky, stars, w, h, atlas,
+    atlas_w)`` (`draw_map`, sky.rs:861-878: the game sky's maps, from the stated sky of the tick,
+    ``gamesky.stated_sky``) and ``blend_chunky_sky(params, cache, maps, sizes, weight)``
+    (sky.rs:836-850); by default the library's device kernels on device 0.
     """
     width = width or cfg.width
     height = height or cfg.height
@@ -169,7 +172,8 @@ def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None)
         if weight >= 1.0:
             sky = cache
         else:
-            maps, sizes = SK.synthetic_game_maps(sun_dir)
+            desc, factor, colour = G.stated_sky(cfg.time, hq.sun_sprite)
+            maps, sizes, _ = G.game_sky_maps(sky_backend, desc, factor, colour, hq.atlas, hq.atlas_size[0])
             if weight > 0.0:
                 maps = sky_backend.blend_chunky_sky(p, cache, maps, sizes, weight)
                 p["sun_color"][:3] = p["sun_color"][:3] * weight

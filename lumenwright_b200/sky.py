@@ -3,11 +3,8 @@
 the sun texture axes, the game sky's map geometry) and the sky parts of
 `crates/lumenwright/src/request.rs`. FP64 where the reference computes in f64.
 
-The game sky's maps are the client's sky drawn per direction (`QuickSky::background` with the
-jar's environment attributes, sky.rs:909-952). No jar is available here, so
-``synthetic_game_maps`` draws a seeded stand-in of the same sizes and layout: a smooth dusk
-gradient with a glow around the sun, and the light map normalised as `game_sky_maps` normalises
-it.
+The game sky's maps (the client's sky drawn per direction, sky.rs:855-952) are
+``lumenwright_b200.gamesky``'s.
 """
 
 import math
@@ -178,45 +175,3 @@ def dusk_day_weight(ticks: int) -> np.float32:
     if 13140 <= t <= 22860:
         return F32(0.0)
     return F32(((t - 22860) % 24000) / 1870.0) if t > 22860 else F32((t + 24000 - 22860) / 1870.0)
-
-
-def synthetic_game_maps(sun_dir, seed: int = 7):
-    """A stand-in for `game_sky_maps` (sky.rs:909-952) at dusk: the lens map (2048x1024) and the
-    light map (360x180), linear RGB, row 0 at the nadir, laid out as the kernel's `map_lookup`
-    reads them. The client's sky is replaced by a seeded smooth gradient: a dark blue zenith, an
-    orange horizon glow strongest towards the sun and a dim ground; the light map is scaled so its
-    cosine-weighted upper-hemisphere mean is the lightmap colour of a dusk tick, as the
-    reference's normalisation makes it."""
-    sun = np.asarray(sun_dir, np.float64)
-    rng = np.random.default_rng(seed)
-    tint = 1.0 + 0.05 * rng.standard_normal(3)
-
-    def draw(w, h, with_sun):
-        j, i = np.mgrid[0:h, 0:w]
-        d = map_direction(i, j, w, h).astype(np.float64)
-        y = d[..., 1]
-        toward = np.clip(d @ sun, -1.0, 1.0)
-        zenith = np.array([0.02, 0.04, 0.12]) * tint
-        horizon = np.array([0.45, 0.22, 0.10]) * tint
-        ground = np.array([0.03, 0.025, 0.02])
-        up = np.clip(y, 0.0, 1.0)[..., None]
-        glow = np.exp(-np.abs(y) * 6.0)[..., None] * (0.35 + 0.65 * ((toward + 1.0) / 2.0) ** 4)[..., None]
-        c = zenith * up + horizon * glow + np.where(y[..., None] < 0, ground, 0.0)
-        if with_sun:
-            disc = (toward > math.cos(0.05))[..., None]
-            c = np.where(disc, np.array([6.0, 3.5, 1.5]), c)
-        return c.astype(F32)
-
-    lens = draw(*LENS_MAP, True)
-    light = draw(*LIGHT_MAP, False)
-    gw, gh = LIGHT_MAP
-    j, i = np.mgrid[0:gh, 0:gw]
-    d = map_direction(i, j, gw, gh)
-    w = np.where(d[..., 1] > 0, d[..., 1] * np.sqrt(np.clip(1.0 - d[..., 1] ** 2, 0, None)), 0.0).astype(np.float64)
-    mean = (light.astype(np.float64) * w[..., None]).sum((0, 1)) / w.sum()
-    target = np.array([0.09, 0.075, 0.07])  # a dusk lightmap colour, linear
-    scale = min(float(MAX_SKY_LIGHT), float(np.min(target / mean)))
-    veil = np.maximum(target / scale - mean, 0.0)
-    light = ((light + veil) * scale).astype(F32)
-    buf = np.concatenate([lens.ravel(), light.ravel()]).astype(F32)
-    return buf, np.array([LENS_MAP[0], LENS_MAP[1], LIGHT_MAP[0], LIGHT_MAP[1]], F32)

@@ -168,6 +168,18 @@ void lwo_reset_bounds_errors(void);
 void lwo_tonemap(const float *hdr, uint64_t n, float exposure, uint32_t op, uint32_t mix, uint32_t op_b, float weight,
                  uint32_t *out);
 void lwo_game_tone_curve(float out[7]);
+
+/* `QuickSky` (crates/lumenwright/src/render/sky.rs:274-305), 608 bytes: the record the game
+ * sky's per-texel pass reads. */
+typedef struct {
+    float sky_color[4], fog_color[4], fog_dist[4], sunrise[4], flags[4];
+    float sun[4][4], moon[4][4], star_rot[3][4], fan[18][4];
+    float cam_forward[4], cam_right[4], cam_up[4], cam_misc[4];
+} lwo_quick_sky;
+/* `draw_map` (sky.rs:861-878): QuickSky::background for every texel of a w x h equirectangular
+ * map, decoded to linear, into out (w * h * 3 floats, row 0 at the nadir). */
+void lwo_draw_sky_map(const lwo_quick_sky *q, const uint32_t *atlas, uint32_t atlas_w, const uint32_t *stars, uint32_t w,
+                      uint32_t h, float *out, int threads);
 double lwo_mid_grey_gain(void);
 double lwo_game_before_gamma(double x);
 

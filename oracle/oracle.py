@@ -354,6 +354,21 @@ def water_exp(x):
     return out
 
 
+def draw_sky_map(quick_sky, stars, w, h, atlas, atlas_w, threads=0):
+    """`draw_map` (sky.rs:861-878) of a packed `QuickSky` (``lumenwright_b200.gamesky``) on the host:
+    (h, w, 3) linear RGB, row 0 at the nadir."""
+    L = lib()
+    L.lwo_draw_sky_map.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p,
+                                   C.c_int]
+    L.lwo_draw_sky_map.restype = None
+    q = np.ascontiguousarray(quick_sky)
+    atlas = np.ascontiguousarray(atlas, np.uint32)
+    stars = np.ascontiguousarray(stars, np.uint32)
+    out = np.zeros((h, w, 3), np.float32)
+    L.lwo_draw_sky_map(q.ctypes.data, atlas.ctypes.data, atlas_w, stars.ctypes.data, w, h, out.ctypes.data, threads)
+    return out
+
+
 def bounds_errors():
     return lib().lwo_bounds_errors()
 

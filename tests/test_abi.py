@@ -7,7 +7,7 @@ import os
 import re
 import subprocess
 
-from lumenwright_b200 import build, layout, native
+from lumenwright_b200 import build, gamesky, layout, native
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -43,7 +43,7 @@ MIRRORS = (
     ("lw_instances_desc", native.InstancesDesc), ("lw_build_info", native.BuildInfo),
     ("lw_tonemap", native.ToneMap), ("lw_gradient", native.Gradient), ("lw_hit", native.HitRec),
     ("lw_params", layout.PARAMS_DTYPE), ("lw_quad", layout.QUAD_DTYPE), ("lw_model", layout.MODEL_DTYPE),
-    ("lw_emitter", layout.EMITTER_DTYPE),
+    ("lw_emitter", layout.EMITTER_DTYPE), ("lw_quick_sky", gamesky.QUICK_SKY_DTYPE),
 )
 
 
@@ -89,7 +89,7 @@ def test_oracle_bindings_match_the_oracle_header_layout(tmp_path):
     from oracle import oracle as O
     check_layout(tmp_path, os.path.join(ROOT, "oracle"), "lw_oracle.h",
                  (("lwo_scene", O.Scene), ("lwo_hit", O.Hit), ("lwo_camera64", O.Camera64),
-                  ("lwo_theta", O.Theta), ("lwo_counters", O.Counters)))
+                  ("lwo_theta", O.Theta), ("lwo_counters", O.Counters), ("lwo_quick_sky", gamesky.QUICK_SKY_DTYPE)))
 
 
 def test_the_header_compiles_strictly_as_c_and_cpp(tmp_path):

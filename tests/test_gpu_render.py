@@ -223,3 +223,45 @@ def test_renders_are_deterministic(ctx, c2):
         assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
     ctx.set_tuning(engine=ENGINE_WAVEFRONT, sub=0, paths=0)
 
+
+
+def test_a_scene_changed_in_place_is_drawn_as_it_now_is():
+    # The backend copies the scene for every frame: the same HqScene object, changed in place
+    # between two frames (its atlas recoloured), is drawn as it is now, as a fresh backend draws it.
+    from lumenwright_b200.native import B200Backend
+    import copy
+    be = B200Backend(0)
+    frame = R.make_frame(R.CONFIGS["c1"], sky_backend=be.ctx, spp=4)
+    first = be.render_hq(frame)
+    frame.scene.atlas[:] = (frame.scene.atlas & np.uint32(0xFF000000)) | (~frame.scene.atlas & np.uint32(0x00FFFFFF))
+    second = be.render_hq(frame)
+    fresh = B200Backend(0).render_hq(copy.deepcopy(frame))
+    assert not np.array_equal(first, second)
+    assert np.array_equal(second.view(np.uint32), fresh.view(np.uint32))
+
+
+@pytest.mark.parametrize("shards", [2, 3])
+def test_frame_shards_add_up_to_the_frame_bit_for_bit(ctx, c2, shards):
+    # lw_render_device_shard: each shard renders its tiles (r, r + N, ...) into the accumulator and
+    # leaves every other pixel's record as it is, so the shards rendered one after another into one
+    # accumulator give the whole frame's render bit for bit; the records of one shard alone are zero
+    # outside its tiles (what a SUM reduce over GPUs adds).
+    from lumenwright_b200 import shard
+    p = c2.params
+    w, h = int(p["frame"][0]), int(p["frame"][1])
+    ctx.upload_hq_scene(c2.scene)
+    ctx.upload_sky(c2.sky)
+    ctx.clear_accumulator(w, h)
+    ctx.render_device(p, 0, 3)
+    want = ctx.read_accumulator(w, h)
+    ctx.clear_accumulator(w, h)
+    for r in range(shards):
+        ctx.render_device_shard(p, 0, 3, r, shards)
+    got = ctx.read_accumulator(w, h)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    ctx.clear_accumulator(w, h)
+    ctx.render_device_shard(p, 0, 3, 1, shards)
+    one = ctx.read_accumulator(w, h)
+    m = shard.tile_mask(w, h, 1, shards)
+    assert not one[~m].any()
+    assert np.array_equal(one[m].view(np.uint32), want[m].view(np.uint32))

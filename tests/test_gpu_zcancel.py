@@ -72,3 +72,32 @@ def test_a_cancel_leaves_whole_launches_in_the_accumulator(ctx, c1):
     torch.cuda.synchronize()
     after = acc.cpu().numpy().reshape(-1, 8)[:, 3]
     assert np.array_equal(after, before + 16)
+
+
+def test_a_wait_past_its_deadline_returns_a_timeout_and_the_next_render_is_whole(ctx, c1):
+    # A deadline far shorter than an ordinary C1 render at 256 spp: the call's wait runs out, the
+    # render's kernels are stopped (no kernel is made to hang: they are cancelled as lw_cancel
+    # cancels them) and the call returns LW_ERR_DEVICE_TIMEOUT; without the deadline the next
+    # render of the frame is bit for bit an uninterrupted one.
+    import time
+
+    from lumenwright_b200.native import LwError
+    p = c1.params
+    ctx.upload_hq_scene(c1.scene)
+    want = ctx.render_hq(p, c1.sky, 256)
+    ctx.set_timeout(1e-4)
+    t0 = time.perf_counter()
+    with pytest.raises(LwError) as e:
+        ctx.render_hq(p, c1.sky, 256)
+    took = time.perf_counter() - t0
+    assert e.value.status == 4, e.value  # LW_ERR_DEVICE_TIMEOUT
+    assert "stopped" in str(e.value)
+    print(f"timed out and drained in {took * 1e3:.1f} ms: {e.value}")
+    ctx.set_timeout(0.0)
+    got = ctx.render_hq(p, c1.sky, 256)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+    # a generous deadline changes nothing
+    ctx.set_timeout(60.0)
+    again = ctx.render_hq(p, c1.sky, 256)
+    ctx.set_timeout(0.0)
+    assert np.array_equal(again.view(np.uint32), want.view(np.uint32))

@@ -1,8 +1,8 @@
-"""The multi-GPU sample sharding on the host: two gloo ranks render their sample ranges of a small
-frame with the CPU oracle, reduce their means to rank 0, and the result equals one process
-rendering every sample; and a rank that does not join the reduction (it leaves, or it stalls)
-ends the waiting rank's reduction with an error within the process group's timeout. CPU only
-(world size 2)."""
+"""The multi-GPU frame split on the host: the ranks' tiles partition the frame; two gloo ranks
+render their tiles of a small frame with the CPU oracle and reduce their images to rank 0, and the
+result equals one process rendering the whole frame bit for bit; and a rank that does not join the
+reduction (it leaves, or it stalls) ends the waiting rank's reduction with an error within the
+process group's timeout. CPU only (world size 2)."""
 
 import os
 import socket
@@ -15,11 +15,13 @@ from kernel_fixtures import lamp_scene
 from lumenwright_b200 import layout as L
 from lumenwright_b200 import shard
 
+W, H = 20, 11  # not a multiple of the 8x4 tile
+
 
 def frame_scene():
     ks = lamp_scene(L.EMITTER_SAMPLING_ONE, True)
     p = ks.params
-    p["frame"] = [12, 8, 0, 3]
+    p["frame"] = [W, H, 0, 3]
     p["cam_pos"] = [8.0, 12.0, 8.0, 0.9]
     p["cam_fwd"] = [0.0, -1.0, 0.0, 1.5]
     p["cam_right"] = [1.0, 0.0, 0.0, 0.0]
@@ -29,12 +31,19 @@ def frame_scene():
     return ks
 
 
-def mean_of_range(start, count):
+def frame_mean(spp):
     from oracle import oracle as O
     ks = frame_scene()
-    s = O.OracleScene(*ks.buffers()).render_samples(0, 0, 12, 8, start, count)
-    s = np.where(np.isfinite(s).all(-1, keepdims=True), s, 0.0)
-    return s.astype(np.float64).sum(2).astype(np.float32) / np.float32(count)
+    return O.OracleScene(*ks.buffers()).render_mean(0, 0, W, H, spp)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+@pytest.mark.parametrize("size", [(1, 1), (7, 3), (8, 4), (20, 11), (1280, 720)])
+def test_the_ranks_tiles_partition_the_frame(world, size):
+    w, h = size
+    masks = np.stack([shard.tile_mask(w, h, r, world) for r in range(world)])
+    assert np.array_equal(masks.sum(0), np.ones((h, w)))
+    assert shard.frame_spp(1024, world) == 1024 * world
 
 
 def worker(rank, world, port, out):
@@ -42,8 +51,8 @@ def worker(rank, world, port, out):
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world)
-    start, count = shard.sample_range(rank, world, 8, step=1)
-    m = shard.reduce_means(mean_of_range(start, count), dist)
+    local = np.where(shard.tile_mask(W, H, rank, world)[..., None], frame_mean(8), np.float32(0.0))
+    m = shard.reduce_images(local.astype(np.float32), dist)
     if rank == 0:
         np.save(out, m)
     dist.barrier()
@@ -62,9 +71,8 @@ def test_two_ranks_give_the_single_process_frame(tmp_path):
     out = str(tmp_path / "m.npy")
     mp.start_processes(worker, args=(2, free_port(), out), nprocs=2, join=True, start_method="spawn")
     got = np.load(out)
-    assert shard.sample_range(0, 2, 8, 1) == (16, 8) and shard.sample_range(1, 2, 8, 1) == (24, 8)
-    want = mean_of_range(16, 16)
-    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6)
+    want = frame_mean(8)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
 
 
 def leaving_worker(rank, world, port, out, mode):
@@ -84,7 +92,7 @@ def leaving_worker(rank, world, port, out, mode):
         return
     t0 = time.monotonic()
     try:
-        shard.reduce_means(np.ones((2, 3, 3), np.float32), dist)
+        shard.reduce_images(np.ones((2, 3, 3), np.float32), dist)
         result = "none"
     except Exception as e:  # the reduction's error
         result = type(e).__name__

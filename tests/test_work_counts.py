@@ -33,6 +33,9 @@ class OracleSky:
     def blend_chunky_sky(self, params, cache, maps, sizes, weight):
         return maps
 
+    def draw_sky_map(self, quick_sky, stars, w, h, atlas, atlas_w):
+        return np.full((h, w, 3), 0.1, np.float32)
+
 
 def count_c2():
     cfg = R.CONFIGS["c2"]
