@@ -273,7 +273,12 @@ lw_status lw_accumulator_device(lw_ctx *ctx, void **records, uint32_t *width, ui
  * lays out their accumulators and partial sums, and captures clear + render + reduce into a CUDA
  * graph; lw_batch_run replays the graph (asynchronously, on lw_stream); lw_batch_read waits and
  * copies each camera's mean radiance to its `out_rgb` (skipped when NULL). lw_render_batch does
- * all three. A camera's image is what lw_render_hq gives for the same Params, sky and spp. */
+ * all three. A camera's image is what lw_render_hq gives for the same Params, sky and spp. With
+ * the wavefront engine and automatic items (lw_tuning.sub 0), every work item is one sample and
+ * the graph runs the batch in as many passes as keep a pass's item sums (16 bytes an item) within
+ * 40 GiB and a third of the free device memory (LUMENWRIGHT_BATCH_SUMS_MB in the environment
+ * lowers that cap), each pass an equal slice of every camera's samples; a camera's pixel sums run
+ * on across the passes in sample order. */
 typedef struct {
     lw_params params;      /* the camera's frame: camera, frame size, bounces, sky and sun settings */
     const float *sky;      /* the camera's sky buffer (HqFrame.sky) */

@@ -114,6 +114,7 @@ struct lw_ctx {
     std::vector<size_t> batch_out_off;
     cudaGraphExec_t batch_graph = nullptr;
     uint64_t batch_samples = 0;
+    uint32_t batch_passes = 1;  // passes of the prepared batch (the wavefront's one-sample items)
     size_t partials_cap_bytes = size_t(4) << 30;
     // the wavefront engine: path slots (grown to the largest pool used), queue fetch settings
 #ifndef LW_WF_TAIL
@@ -566,11 +567,13 @@ lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32
     return LW_OK;
 }
 
-// The batched form on the wavefront engine as one CUDA graph: clear the work counter, the
-// accumulators and the path slots; then a loop node (a conditional WHILE node) whose body is one
-// iteration (shade every slot, trace the queue, advance) and which runs again while the last
-// iteration had rays to trace, all decided on the device; then the per-camera reduction.
-lw_status batch_graph_wavefront(lw_ctx *c, const BatchDesc &B, const DevParams &P0, uint64_t pixels, uint32_t slots) {
+// The batched form on the wavefront engine as one CUDA graph: clear the accumulators; then per pass
+// clear the work counter and the path slots, a loop node (a conditional WHILE node) whose body is
+// one iteration (shade every slot, trace the queue, advance) and which runs again while the last
+// iteration had rays to trace, all decided on the device, and the pass's per-camera reduction,
+// which carries every pixel's Kahan sums on from the pass before.
+lw_status batch_graph_wavefront(lw_ctx *c, const std::vector<BatchDesc> &Bs, const DevParams &P0, uint64_t pixels,
+                               uint32_t slots) {
     if (!c->cap) CK(c, cudaStreamCreateWithFlags(&c->cap, cudaStreamNonBlocking), "creating a capture stream");
     const uint32_t budget = c->tuning.budget ? c->tuning.budget : kWfBudget;
     // The buffers first (cleared outside the graph too, which is harmless).
@@ -581,41 +584,45 @@ lw_status batch_graph_wavefront(lw_ctx *c, const BatchDesc &B, const DevParams &
     DevScene S = dev_scene(c);
     cudaGraph_t graph = nullptr;
     CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal), "starting the graph capture");
-    cudaError_t e = cudaMemsetAsync(B.counter, 0, 4, c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(c->batch_acc.p, 0, sizeof(Accum) * pixels, c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(F.state + (size_t)4 * F.n, 0, (size_t)F.n * sizeof(float4), c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(F.ctr, 0, 16 * sizeof(uint32_t), c->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(F.hit0, 0, (size_t)F.n * sizeof(float4), c->stream);
-    cudaGraphNode_t loop_node = nullptr;
-    if (e == cudaSuccess) {
-        cudaStreamCaptureStatus status;
-        cudaGraph_t g = nullptr;
-        const cudaGraphNode_t *deps = nullptr;
-        size_t ndeps = 0;
-        e = cudaStreamGetCaptureInfo(c->stream, &status, nullptr, &g, &deps, &ndeps);
-        cudaGraphConditionalHandle loop{};
-        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault);
-        cudaGraphNodeParams np{};
-        np.type = cudaGraphNodeTypeConditional;
-        np.conditional.handle = loop;
-        np.conditional.type = cudaGraphCondTypeWhile;
-        np.conditional.size = 1;
-        if (e == cudaSuccess) e = cudaGraphAddNode(&loop_node, g, deps, ndeps, &np);
+    cudaError_t e = cudaMemsetAsync(c->batch_acc.p, 0, sizeof(Accum) * pixels, c->stream);
+    // Per pass: clear the work counter and the path slots, the loop node, the pass's reduction.
+    for (size_t k = 0; k < Bs.size() && e == cudaSuccess; k++) {
+        const BatchDesc &B = Bs[k];
+        e = cudaMemsetAsync(B.counter, 0, 4, c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(F.state + (size_t)4 * F.n, 0, (size_t)F.n * sizeof(float4), c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(F.ctr, 0, 16 * sizeof(uint32_t), c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(F.hit0, 0, (size_t)F.n * sizeof(float4), c->stream);
+        cudaGraphNode_t loop_node = nullptr;
         if (e == cudaSuccess) {
-            cudaGraph_t body = np.conditional.phGraph_out[0];
-            e = cudaStreamBeginCaptureToGraph(c->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+            cudaStreamCaptureStatus status;
+            cudaGraph_t g = nullptr;
+            const cudaGraphNode_t *deps = nullptr;
+            size_t ndeps = 0;
+            e = cudaStreamGetCaptureInfo(c->stream, &status, nullptr, &g, &deps, &ndeps);
+            cudaGraphConditionalHandle loop{};
+            if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&loop, g, 1u, cudaGraphCondAssignDefault);
+            cudaGraphNodeParams np{};
+            np.type = cudaGraphNodeTypeConditional;
+            np.conditional.handle = loop;
+            np.conditional.type = cudaGraphCondTypeWhile;
+            np.conditional.size = 1;
+            if (e == cudaSuccess) e = cudaGraphAddNode(&loop_node, g, deps, ndeps, &np);
             if (e == cudaSuccess) {
-                cudaError_t eb = launch_wf_shade_batch(S, P0, B, F, wf_shade_blocks(c, F.n), c->cap);
-                if (eb == cudaSuccess) eb = launch_wf_trace(S, P0, F, c->shape_wf, budget, c->wf_tail, c->cap);
-                if (eb == cudaSuccess) eb = launch_wf_advance_graph(F, loop, c->cap);
-                cudaGraph_t done = nullptr;
-                e = cudaStreamEndCapture(c->cap, &done);
-                if (eb != cudaSuccess) e = eb;
+                cudaGraph_t body = np.conditional.phGraph_out[0];
+                e = cudaStreamBeginCaptureToGraph(c->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess) {
+                    cudaError_t eb = launch_wf_shade_batch(S, P0, B, F, wf_shade_blocks(c, F.n), c->cap);
+                    if (eb == cudaSuccess) eb = launch_wf_trace(S, P0, F, c->shape_wf, budget, c->wf_tail, c->cap);
+                    if (eb == cudaSuccess) eb = launch_wf_advance_graph(F, loop, c->cap);
+                    cudaGraph_t done = nullptr;
+                    e = cudaStreamEndCapture(c->cap, &done);
+                    if (eb != cudaSuccess) e = eb;
+                }
             }
+            if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(c->stream, &loop_node, 1, cudaStreamSetCaptureDependencies);
         }
-        if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(c->stream, &loop_node, 1, cudaStreamSetCaptureDependencies);
+        if (e == cudaSuccess) e = launch_reduce_batch(B, c->stream);
     }
-    if (e == cudaSuccess) e = launch_reduce_batch(B, c->stream);
     cudaError_t e2 = cudaStreamEndCapture(c->stream, &graph);
     if (e == cudaSuccess) e = e2;
     if (e == cudaSuccess) e = cudaGraphInstantiate(&c->batch_graph, graph, 0);
@@ -1155,67 +1162,101 @@ lw_status lw_batch_prepare(lw_ctx *c, const lw_camera_job *jobs, uint32_t n) {
     // Layout: items, slots, accumulators, images, item sums.
     uint64_t total_samples = 0;
     for (uint32_t i = 0; i < n; i++) total_samples += (uint64_t)jobs[i].params.frame[0] * jobs[i].params.frame[1] * jobs[i].spp;
-    // Samples per item: as few as keep the item sums (16 B each, one launch) within 40 GiB and a
-    // third of the device memory free now; one sample per item drains the pool fastest (the
-    // 64-camera workload: +7 % over 9 per item).
+    // Samples per item and passes. The item sums (16 B each) of a pass must fit 40 GiB and a third
+    // of the device memory free now. The wavefront engine with automatic items takes one sample per
+    // item (a slot that ends a sample takes the next item at once, so the pool drains fastest) and
+    // as many passes as the cap needs, each covering an equal slice of every camera's samples; with
+    // items of `sub` samples (the tuning's, or the megakernel's) the batch is one pass of items as
+    // small as fit.
     size_t free_b = 0, total_b = 0;
     uint64_t sums_cap = 40ull << 30;
     if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b / 3 < sums_cap) sums_cap = free_b / 3;
+    if (const char *mb = std::getenv("LUMENWRIGHT_BATCH_SUMS_MB")) sums_cap = std::min<uint64_t>(sums_cap, std::strtoull(mb, nullptr, 10) << 20);
     const uint64_t max_items = sums_cap / sizeof(float4) > 0 ? sums_cap / sizeof(float4) : 1;
     uint64_t sub = (total_samples + max_items - 1) / max_items;
     sub = sub < 1 ? 1 : (sub > 64 ? 64 : sub);
+    uint32_t passes = 1;
+    if (c->tuning.engine == LW_ENGINE_WAVEFRONT && c->tuning.sub == 0) {
+        passes = (uint32_t)std::min<uint64_t>((total_samples + max_items - 1) / max_items, 64);
+        if (passes < 1) passes = 1;
+        sub = 1;
+    }
     if (c->tuning.sub) sub = c->tuning.sub;
-    std::vector<DevJob> dj(n);
-    std::vector<uint32_t> ib(n), sb(n);
-    uint64_t items = 0, slots = 0, pixels = 0, partials = 0;
+    // Per pass and camera: the camera's share of the pass's items, item sums and samples.
+    std::vector<DevJob> dj((size_t)n * passes);
+    std::vector<uint32_t> ib((size_t)n * passes), sb(n);
+    std::vector<uint64_t> pass_items(passes, 0), pass_samples(passes, 0);
+    uint64_t slots = 0, pixels = 0, max_partials = 0;
     c->batch_out_off.assign(n, 0);
     for (uint32_t i = 0; i < n; i++) {
         const lw_params &p = jobs[i].params;
-        DevJob &J = dj[i];
-        J.P = dev_params(&p);
-        J.sky = sky_dev[i];
-        J.w = p.frame[0];
-        J.h = p.frame[1];
-        J.tiles_x = (J.w + 7) / 8;
-        J.n_slots = J.tiles_x * ((J.h + 3) / 4) * 32u;
-        J.sample_start = jobs[i].sample_start;
-        J.spp = jobs[i].spp;
-        J.sub = (uint32_t)(sub < J.spp ? sub : J.spp);
-        J.n_sub = (J.spp + J.sub - 1) / J.sub;
-        J.item_begin = (uint32_t)items;
-        J.slot_begin = (uint32_t)slots;
-        J.partial_off = partials;
-        J.acc = nullptr;
-        J.out = nullptr;
-        ib[i] = J.item_begin;
-        sb[i] = J.slot_begin;
-        items += (uint64_t)J.n_slots * J.n_sub;
-        slots += J.n_slots;
-        partials += (uint64_t)J.n_slots * J.n_sub;
         c->batch_out_off[i] = (size_t)pixels;
-        pixels += (uint64_t)J.w * J.h;
+        pixels += (uint64_t)p.frame[0] * p.frame[1];
     }
-    if (items >= 0xFFFFFFFFull || slots >= 0xFFFFFFFFull)
-        return fail(c, LW_ERR_INVALID_ARGUMENT, "the batch has %llu work items; at most 2^32 - 1 fit one launch",
-                    (unsigned long long)items);
+    for (uint32_t k = 0; k < passes; k++) {
+        uint64_t items = 0, partials = 0;
+        slots = 0;
+        for (uint32_t i = 0; i < n; i++) {
+            const lw_params &p = jobs[i].params;
+            DevJob &J = dj[(size_t)k * n + i];
+            J.P = dev_params(&p);
+            J.sky = sky_dev[i];
+            J.w = p.frame[0];
+            J.h = p.frame[1];
+            J.tiles_x = (J.w + 7) / 8;
+            J.n_slots = J.tiles_x * ((J.h + 3) / 4) * 32u;
+            // this pass's slice of the camera's samples
+            const uint64_t s0 = (uint64_t)jobs[i].spp * k / passes, s1 = (uint64_t)jobs[i].spp * (k + 1) / passes;
+            J.sample_start = jobs[i].sample_start + (uint32_t)s0;
+            J.spp = (uint32_t)(s1 - s0);
+            J.sub = J.spp == 0 ? 1u : (uint32_t)(sub < J.spp ? sub : J.spp);
+            J.n_sub = (J.spp + J.sub - 1) / J.sub;
+            J.item_begin = (uint32_t)items;
+            J.slot_begin = (uint32_t)slots;
+            J.partial_off = partials;
+            J.acc = c->batch_acc.p;  // set below, once the accumulators are allocated
+            J.out = nullptr;
+            ib[(size_t)k * n + i] = J.item_begin;
+            sb[i] = J.slot_begin;
+            items += (uint64_t)J.n_slots * J.n_sub;
+            slots += J.n_slots;
+            partials += (uint64_t)J.n_slots * J.n_sub;
+            pass_samples[k] += (uint64_t)J.w * J.h * J.spp;
+        }
+        if (items >= 0xFFFFFFFFull || slots >= 0xFFFFFFFFull)
+            return fail(c, LW_ERR_INVALID_ARGUMENT, "a pass of the batch has %llu work items; at most 2^32 - 1 fit one launch",
+                        (unsigned long long)items);
+        pass_items[k] = items;
+        max_partials = std::max(max_partials, partials);
+    }
     CK(c, ensure(c->batch_acc, pixels), "allocating the accumulators");
     CK(c, ensure(c->batch_out, 3 * pixels), "allocating the images");
-    CK(c, ensure(c->batch_partials, partials), "allocating the item sums");
-    for (uint32_t i = 0; i < n; i++) {
-        dj[i].acc = c->batch_acc.p + c->batch_out_off[i];
-        dj[i].out = c->batch_out.p + 3 * c->batch_out_off[i];
+    CK(c, ensure(c->batch_partials, max_partials), "allocating the item sums");
+    for (size_t q = 0; q < dj.size(); q++) {
+        const size_t i = q % n;
+        dj[q].acc = c->batch_acc.p + c->batch_out_off[i];
+        dj[q].out = c->batch_out.p + 3 * c->batch_out_off[i];
     }
-    CK(c, ensure(c->batch_jobs, n), "allocating the job table");
-    CK(c, ensure(c->batch_item_begin, n), "allocating the job table");
+    CK(c, ensure(c->batch_jobs, dj.size()), "allocating the job table");
+    CK(c, ensure(c->batch_item_begin, ib.size()), "allocating the job table");
     CK(c, ensure(c->batch_slot_begin, n), "allocating the job table");
-    CK(c, cudaMemcpyAsync(c->batch_jobs.p, dj.data(), sizeof(DevJob) * n, cudaMemcpyHostToDevice, c->stream), "uploading jobs");
-    CK(c, cudaMemcpyAsync(c->batch_item_begin.p, ib.data(), 4 * n, cudaMemcpyHostToDevice, c->stream), "uploading jobs");
+    CK(c, cudaMemcpyAsync(c->batch_jobs.p, dj.data(), sizeof(DevJob) * dj.size(), cudaMemcpyHostToDevice, c->stream),
+       "uploading jobs");
+    CK(c, cudaMemcpyAsync(c->batch_item_begin.p, ib.data(), 4 * ib.size(), cudaMemcpyHostToDevice, c->stream),
+       "uploading jobs");
     CK(c, cudaMemcpyAsync(c->batch_slot_begin.p, sb.data(), 4 * n, cudaMemcpyHostToDevice, c->stream), "uploading jobs");
     CK(c, cudaStreamSynchronize(c->stream), "uploading jobs");
-    BatchDesc B{c->batch_jobs.p, c->batch_item_begin.p, c->batch_slot_begin.p, n, (uint32_t)items, (uint32_t)slots,
-                c->tuning.budget, c->counter.p, c->batch_partials.p, c->cancel_word.p};
+    std::vector<BatchDesc> Bs(passes);
+    for (uint32_t k = 0; k < passes; k++)
+        Bs[k] = BatchDesc{c->batch_jobs.p + (size_t)k * n, c->batch_item_begin.p + (size_t)k * n, c->batch_slot_begin.p, n,
+                          (uint32_t)pass_items[k], (uint32_t)slots, c->tuning.budget, c->counter.p, c->batch_partials.p,
+                          c->cancel_word.p};
+    const BatchDesc &B = Bs[0];
+    c->batch_passes = passes;
     if (c->tuning.engine == LW_ENGINE_WAVEFRONT) {
-        lw_status ws = batch_graph_wavefront(c, B, dj[0].P, pixels, wf_slots(c, total_samples, items));
+        uint64_t most = *std::max_element(pass_samples.begin(), pass_samples.end());
+        uint64_t most_items = *std::max_element(pass_items.begin(), pass_items.end());
+        lw_status ws = batch_graph_wavefront(c, Bs, dj[0].P, pixels, wf_slots(c, most, most_items));
         if (ws != LW_OK) return ws;
         c->batch_host.assign(jobs, jobs + n);
         c->batch_samples = total_samples;

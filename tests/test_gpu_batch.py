@@ -69,6 +69,24 @@ def test_batch_cameras_match_the_oracle(ctx):
     assert checked == {"maps", "cache"}
 
 
+def test_a_batch_in_passes_gives_the_separate_renders_bit_for_bit(ctx, monkeypatch):
+    # With the item sums capped small the wavefront batch runs in several passes of one-sample
+    # items (each an equal slice of every camera's samples): each camera's image is lw_render_hq's
+    # (one-sample items, the same order of additions) bit for bit.
+    monkeypatch.setenv("LUMENWRIGHT_BATCH_SUMS_MB", "1")
+    hq, jobs = BT.c3_jobs(ctx, small_cameras())
+    ctx.upload_hq_scene(hq)
+    ctx.set_tuning(threads=128, budget=0, sub=0, engine=0, paths=0)
+    total = sum(int(p["frame"][0]) * int(p["frame"][1]) * spp for p, _, spp in jobs)
+    assert total * 16 > 2 * (1 << 20)  # at least three passes (one camera has fewer spp than passes)
+    outs = ctx.batch_prepare(jobs)
+    ctx.batch_run()
+    ctx.batch_read()
+    for (p, sky, spp), got in zip(jobs, outs):
+        want = ctx.render_hq(p, sky, spp)
+        assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), int(p["frame"][0])
+
+
 def test_autotuner_picks_a_tuning(ctx, tmp_path):
     hq, jobs = BT.c3_jobs(ctx, small_cameras())
     ctx.upload_hq_scene(hq)
