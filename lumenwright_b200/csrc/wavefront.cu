@@ -270,12 +270,19 @@ LW_DI void shade_slot(bool valid, uint32_t i, const DevScene &S0, const DevParam
 // the rays the tracing of iteration t - 1 carried over; the shading of iteration t reads set
 // (t - 1) % 3 and clears set (t + 1) % 3 for the next iteration. The iteration is the device word
 // ctr[12], advanced by k_wf_advance after each trace.
-// Blocks of 128 threads' worth per SM the shading kernel must fit: 6, so 80 registers a thread.
+// Blocks of 128 threads' worth per SM the shading kernel must fit: 6, so 80 registers a thread. The
+// batched one (the camera's Params and sky read through its job, on top) spills 160 bytes a thread
+// at 80, and none at 100 (LW_WF_SHADE_MINB_BATCH 4, two blocks a SM), but the occupancy counts for
+// more: the full-spp 64-camera batch runs at 513.8 Msamples/s at 80 and 492.9 at 100.
 #ifndef LW_WF_SHADE_MINB
 #define LW_WF_SHADE_MINB 6
 #endif
+#ifndef LW_WF_SHADE_MINB_BATCH
+#define LW_WF_SHADE_MINB_BATCH 6
+#endif
 template <bool BATCH>
-__global__ void __launch_bounds__(kShadeThreads, LW_WF_SHADE_MINB * 128 / kShadeThreads) k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
+__global__ void __launch_bounds__(kShadeThreads, (BATCH ? LW_WF_SHADE_MINB_BATCH : LW_WF_SHADE_MINB) * 128 / kShadeThreads)
+k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
                                                   const BatchDesc B, const WfState F) {
     const uint32_t t = *(volatile uint32_t *)&F.ctr[12];
     const uint32_t cur = t % 3u, prev = (t + 2u) % 3u, next = (t + 1u) % 3u;
