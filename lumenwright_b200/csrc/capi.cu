@@ -124,7 +124,9 @@ struct lw_ctx {
     // kernel_ms of the launches already timed when the last one is still running (stats.kernel_ms
     // is then -1 until lw_get_stats adds the last launch's event time)
     double kernel_ms_base = 0.0;
-    LaunchShape shape_wf{};
+    LaunchShape shape_wf{};        // the tracing kernel reading the scene from global memory
+    LaunchShape shape_wf_staged{}; // ... and staging it in shared memory (stage_bytes of it)
+    size_t stage_bytes = 0;
     struct WfBufs {
         DBuf<float4> state, hit0, ts;
         DBuf<float> hit1;
@@ -287,6 +289,8 @@ DevScene dev_scene(const lw_ctx *c) {
     S.sky = c->sky.p;
     S.gamma = c->gamma.p;
     S.sky_brick_y = c->sky_brick_y;
+    S.n_top = c->nb;
+    S.n_occ = c->n_bricks;
     return S;
 }
 
@@ -487,7 +491,8 @@ lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const 
         CK(c, cudaEventRecord(e[0], c->stream), "recording an event");
         CK(c, launch_wf_shade(S, P, W, F, wf_shade_blocks(c, n), c->stream), "launching the shading kernel");
         CK(c, cudaEventRecord(e[1], c->stream), "recording an event");
-        CK(c, launch_wf_trace(S, P, F, c->shape_wf, budget, c->wf_tail, c->stream), "launching the tracing kernel");
+        CK(c, launch_wf_trace(S, P, F, c->stage_bytes ? c->shape_wf_staged : c->shape_wf, budget, c->wf_tail, c->stage_bytes,
+                              c->stream), "launching the tracing kernel");
         CK(c, cudaEventRecord(e[2], c->stream), "recording an event");
         CK(c, launch_wf_advance(F, c->stream), "launching the iteration step");
         c->stats.shade_launches++;
@@ -612,7 +617,9 @@ lw_status batch_graph_wavefront(lw_ctx *c, const std::vector<BatchDesc> &Bs, con
                 e = cudaStreamBeginCaptureToGraph(c->cap, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
                 if (e == cudaSuccess) {
                     cudaError_t eb = launch_wf_shade_batch(S, P0, B, F, wf_shade_blocks(c, F.n), c->cap);
-                    if (eb == cudaSuccess) eb = launch_wf_trace(S, P0, F, c->shape_wf, budget, c->wf_tail, c->cap);
+                    if (eb == cudaSuccess)
+                        eb = launch_wf_trace(S, P0, F, c->stage_bytes ? c->shape_wf_staged : c->shape_wf, budget, c->wf_tail,
+                                             c->stage_bytes, c->cap);
                     if (eb == cudaSuccess) eb = launch_wf_advance_graph(F, loop, c->cap);
                     cudaGraph_t done = nullptr;
                     e = cudaStreamEndCapture(c->cap, &done);
@@ -914,6 +921,9 @@ lw_status install_scene(lw_ctx *c, const lw_scene_desc *d, uint32_t n_bricks, ui
     std::memcpy(c->atlas_size, d->atlas_size, sizeof c->atlas_size);
     c->nb = (uint32_t)nb;
     c->n_bricks = n_bricks;
+    // The tracing kernel stages the top level and the occupancy masks per block when they are small.
+    c->stage_bytes = (nb + n_bricks) * sizeof(uint2) <= (uint64_t)LW_TRACE_STAGE_MAX ? (nb + n_bricks) * sizeof(uint2) : 0;
+    if (c->stage_bytes) c->shape_wf_staged = wf_trace_shape(c->device, c->stage_bytes);
     c->n_ov_bricks = n_ov;
     c->grid_len = d->grid_len;
     c->models_len = d->models_len;

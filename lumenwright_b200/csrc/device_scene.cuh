@@ -71,7 +71,16 @@ struct DevScene {
     // The lowest brick row above which every brick is empty (no block, no overlay): a ray in an
     // empty brick at or above it that does not go down meets nothing more.
     uint32_t sky_brick_y;
+    uint32_t n_top, n_occ;  // entries of `top` and `occ` (what a block stages in shared memory)
 };
+
+// A top-level entry or occupancy mask: from global memory through the read-only path, or (STAGED)
+// from the block's copy in shared memory, which `top` and `occ` then point into.
+template <bool STAGED>
+LW_DI uint2 scene_word(const uint2 *p) {
+    if (STAGED) return *p;
+    return __ldg(p);
+}
 
 template <typename T>
 LW_DI T ldg(const T *p) { return __ldg(p); }
@@ -264,7 +273,7 @@ LW_DI RayDda ray_dda(const DevParams &P, V3 d) {
 //    empty brick above the last occupied brick row that does not go down ends there, no hit.
 //  * Every visit (brick skip, empty voxel, voxel with quads) counts towards MAX_STEPS as one
 //    iteration of the reference's loop does.
-template <bool RUNS = true>
+template <bool RUNS = true, bool STAGED = false>
 LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, const RayDda &R, BrickCache &bc,
                 uint32_t &model) {
     const uint32_t dx = P.grid_dims.x, dz = P.grid_dims.z;
@@ -275,10 +284,10 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
     uint32_t b = (by * dz + bz) * dx + bx;
     if (b != bc.b) {
         bc.b = b;
-        uint2 e = ldg(S.top + b);
+        uint2 e = scene_word<STAGED>(S.top + b);
         bc.entry = e.x;
         bc.ov = e.y;
-        if (bc.entry != EMPTY && !(bc.entry & UNIFORM)) bc.occ = ldg(S.occ + bc.entry);
+        if (bc.entry != EMPTY && !(bc.entry & UNIFORM)) bc.occ = scene_word<STAGED>(S.occ + bc.entry);
     }
     const V3 inv = ts.inv;
     if (bc.entry == EMPTY && bc.ov == EMPTY) {
@@ -341,12 +350,12 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
             const int da = (int)(axis == 0 ? dx : (axis == 1 ? P.grid_dims.y : dz));
             if (na < 0 || na >= da) return -1;  // the exit cell leaves the grid
             const uint32_t nb = ((uint32_t)nb1 * dz + (uint32_t)nb2) * dx + (uint32_t)nb0;
-            const uint2 e = ldg(S.top + nb);
+            const uint2 e = scene_word<STAGED>(S.top + nb);
             if (e.x != EMPTY || e.y != EMPTY) {
                 bc.b = nb;
                 bc.entry = e.x;
                 bc.ov = e.y;
-                if (bc.entry != EMPTY && !(bc.entry & UNIFORM)) bc.occ = ldg(S.occ + bc.entry);
+                if (bc.entry != EMPTY && !(bc.entry & UNIFORM)) bc.occ = scene_word<STAGED>(S.occ + bc.entry);
                 break;
             }
             // The next brick is empty too: the reference's next visit, counted, skips it.
@@ -535,6 +544,7 @@ LW_DI bool warp_test_cells(const DevScene &S, const DevParams &P, const TraceSta
 // cells the lanes reached, so a warp runs one phase of quad tests per round, spread over its 32
 // lanes. Returns as trace_run does (1 hit, -1 no hit, 0 the round ended first); after 0 the next
 // round continues from `ts`. The visits and quad tests are trace_run's, in the same order.
+template <bool STAGED = false>
 LW_DI int trace_round_warp(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, float tmin,
                            uint32_t budget, bool have, Hit &out, float4 *sq) {
     const RayDda R = ray_dda(P, d);
@@ -544,7 +554,7 @@ LW_DI int trace_round_warp(const DevScene &S, const DevParams &P, TraceState &ts
     if (have) {
         uint32_t more = budget - 1u;  // visits left in this round after the next one
         for (;;) {
-            r = visit(S, P, ts, o, d, R, bc, model);
+            r = visit<true, STAGED>(S, P, ts, o, d, R, bc, model);
             if (r != 0 || more == 0u) break;
             more--;
         }

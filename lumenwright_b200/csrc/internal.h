@@ -106,13 +106,20 @@ constexpr uint32_t kWfBudget = 5u;
 #endif
 // Threads per block of the shading kernel (256: shading -2.6 % against 128 at c2; 64 is slower).
 constexpr uint32_t kShadeThreads = LW_SHADE_THREADS;
-LaunchShape wf_trace_shape(int device);
+// The tracing kernel can stage the scene's top level and occupancy masks in shared memory, per
+// block, when they take at most LW_TRACE_STAGE_MAX bytes. Off (0) by default: the tables stay in
+// L1 anyway, and staged the c2 frame's tracing took 147.2 ms a 256-spp frame against 124.8 (29 KB
+// a block leaves 7 blocks a SM instead of 8), the c4 frame's 19.3 against 19.0 (same occupancy).
+#ifndef LW_TRACE_STAGE_MAX
+#define LW_TRACE_STAGE_MAX 0
+#endif
+LaunchShape wf_trace_shape(int device, size_t stage_bytes = 0);
 cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, uint32_t blocks,
                             cudaStream_t st);
 cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const BatchDesc &B, const WfState &F,
                                   uint32_t blocks, cudaStream_t st);
 cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState &F, LaunchShape trace_shape,
-                            uint32_t budget, uint32_t tail, cudaStream_t st);
+                            uint32_t budget, uint32_t tail, size_t stage_bytes, cudaStream_t st);
 cudaError_t launch_wf_advance(const WfState &F, cudaStream_t st);
 cudaError_t launch_wf_advance_graph(const WfState &F, cudaGraphConditionalHandle loop, cudaStream_t st);
 

@@ -326,8 +326,22 @@ __global__ void k_wf_advance_graph(const WfState F, cudaGraphConditionalHandle l
 // next queued ray as soon as its ray ends. Once the queue
 // has run dry, a ray still on its way after `tail` more rounds saves its traversal state and goes
 // to the next iteration's queue, so an iteration does not wait for its single longest ray.
-__global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(const DevScene S, const DevParams P, const WfState F,
+// STAGED: the block first copies the scene's top level and occupancy masks (S0.n_top + S0.n_occ
+// entries of 8 bytes, the dynamic shared memory of the launch) into shared memory and reads them
+// there.
+template <bool STAGED>
+__global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(const DevScene S0, const DevParams P, const WfState F,
                                                                       uint32_t budget, uint32_t tail) {
+    extern __shared__ uint2 s_scene[];
+    DevScene S = S0;
+    if (STAGED) {
+        const uint32_t n = S0.n_top + S0.n_occ;
+        for (uint32_t i = threadIdx.x; i < n; i += kTraceThreads)
+            s_scene[i] = i < S0.n_top ? __ldg(S0.top + i) : __ldg(S0.occ + (i - S0.n_top));
+        __syncthreads();
+        S.top = s_scene;
+        S.occ = s_scene + S0.n_top;
+    }
     const unsigned FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t t = *(volatile uint32_t *)&F.ctr[12];
@@ -403,7 +417,7 @@ __global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(co
         if (__all_sync(FULL, done && !have)) break;
         if (__any_sync(FULL, done)) rounds++;  // the queue is dry: count the tail rounds
         Hit h = no_hit();
-        const int r = trace_round_warp(S, P, ts, o, d, tmin, budget, have, h, s_quads[threadIdx.x >> 5]);
+        const int r = trace_round_warp<STAGED>(S, P, ts, o, d, tmin, budget, have, h, s_quads[threadIdx.x >> 5]);
         if (have) {
             if (r != 0) {
                 if (r != 1) h = no_hit();
@@ -423,10 +437,11 @@ __global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(co
     }
 }
 
-LaunchShape wf_trace_shape(int device) {
+LaunchShape wf_trace_shape(int device, size_t stage_bytes) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_wf_trace, kTraceThreads, 0);
+    const void *k = stage_bytes ? (const void *)k_wf_trace<true> : (const void *)k_wf_trace<false>;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTraceThreads, stage_bytes);
     if (per_sm < 1) per_sm = 1;
     return LaunchShape{sms * per_sm, kTraceThreads};
 }
@@ -446,9 +461,12 @@ cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const 
 }
 
 cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState &F, LaunchShape trace_shape,
-                            uint32_t budget, uint32_t tail, cudaStream_t st) {
+                            uint32_t budget, uint32_t tail, size_t stage_bytes, cudaStream_t st) {
     if (budget == 0u) budget = kWfBudget;  // a round makes at least one visit
-    k_wf_trace<<<trace_shape.blocks, trace_shape.threads, 0, st>>>(S, P, F, budget, tail);
+    if (stage_bytes)
+        k_wf_trace<true><<<trace_shape.blocks, trace_shape.threads, stage_bytes, st>>>(S, P, F, budget, tail);
+    else
+        k_wf_trace<false><<<trace_shape.blocks, trace_shape.threads, 0, st>>>(S, P, F, budget, tail);
     return cudaGetLastError();
 }
 
