@@ -20,7 +20,8 @@ At N = 1 the line also carries the north star's other forms, each on its own con
 timed the same way (unless --no-extras): ``reference_cuda_port`` (the reference's CUDA backend
 ported as written, on the same frame), ``batched_c3`` (64 cameras in one CUDA graph against 64
 separate renders), ``adjoint_c4`` (forward + backward), ``precision_c5`` (3840x2160 at --c5-spp
-with its FP64-oracle error), the drop-in image's FP64-oracle error (``accuracy``) and the tracing
+with chunk-origin rebasing and its FP64-oracle error, the grid's frame beside it), the drop-in
+image's FP64-oracle error (``accuracy``) and the tracing
 kernel against the L2 read bandwidth measured in the run (``roofline_l2``).
 """
 
@@ -153,16 +154,17 @@ def camera64(frame):
                       float(p["cam_pos"][3]), float(p["cam_fwd"][3]))
 
 
-def accuracy(frame, img, crop=64):
+def accuracy(frame, img, crop=64, ref=None):
     """The image's error against the FP64 oracle (FP64 throughout, camera rays from the f64 eye, the
     same random streams) on the crop x crop pixels at the frame's centre, relative to the crop's
-    mean radiance."""
+    mean radiance. `ref`: the oracle's crop, when already rendered."""
     from oracle import oracle as O
     p = frame.params
     w, h = int(p["frame"][0]), int(p["frame"][1])
     x0, y0 = w // 2 - crop // 2, h // 2 - crop // 2
     t0 = time.perf_counter()
-    ref = O.OracleScene.from_frame(frame).render_mean64(x0, y0, crop, crop, frame.spp, cam=camera64(frame))
+    if ref is None:
+        ref = O.OracleScene.from_frame(frame).render_mean64(x0, y0, crop, crop, frame.spp, cam=camera64(frame))
     dt = time.perf_counter() - t0
     err = img[y0:y0 + crop, x0:x0 + crop].astype(np.float64) - ref
     mean = float(ref.mean())
@@ -263,31 +265,55 @@ def extra_adjoint(device, steps=3):
 
 def extra_precision(device, spp):
     """The precision configuration's frame (32x32 chunks translated to x = 1,000,000, 3840x2160, 8
-    bounces) at `spp` (of its 4096), FP32 traversal, Kahan FP32 sums; its error against the FP64
-    oracle on the 64x64 centre crop."""
+    bounces) at `spp` (of its 4096): FP32 traversal with chunk-origin rebasing (every path origin
+    held relative to its nearest chunk corner), Kahan FP32 sums; its error against the FP64 oracle
+    on the 64x64 centre crop. The same frame in the grid's frame (positions relative to the grid
+    origin, as the reference holds them) beside it, and, per sample on a 32x32 centre crop at 16
+    spp, the paths that split from the FP64 twin in each frame."""
     from lumenwright_b200 import request as R
     from lumenwright_b200.native import Context
+    from oracle import oracle as O
     ctx = Context(device)
-    frame = R.make_frame(R.CONFIGS["c5"], sky_backend=ctx, spp=spp)
-    p = frame.params
+    grid = R.make_frame(R.CONFIGS["c5"], sky_backend=ctx, spp=spp)
+    chunk = R.with_chunk_frames(grid)
+    p = grid.params
     w, h = int(p["frame"][0]), int(p["frame"][1])
-    ctx.upload_hq_scene(frame.scene)
-    ctx.upload_sky(frame.sky)
-    ctx.clear_accumulator(w, h)
-    ctx.render_device(p, 0, 2)  # warm-up
-    ctx.stats()
-    ctx.clear_accumulator(w, h)
-    with ClockSampler(device) as clocks:
-        ctx.mark(0)
-        ctx.render_device(p, 0, spp)
-        ctx.mark(1)
-        ms = ctx.elapsed(0, 1)
-    st = ctx.stats()
-    img = ctx.read_accumulator(w, h)
+    ctx.upload_hq_scene(grid.scene)
+    ctx.upload_sky(grid.sky)
+    view = O.OracleScene.from_frame(grid)
+    crop = 64
+    x0, y0 = w // 2 - crop // 2, h // 2 - crop // 2
+    ref = view.render_mean64(x0, y0, crop, crop, spp, cam=camera64(grid))
+    out = {}
+    for name, frame in (("chunk", chunk), ("grid", grid)):
+        ctx.clear_accumulator(w, h)
+        ctx.render_device(frame.params, 0, 2)  # warm-up
+        ctx.stats()
+        ctx.clear_accumulator(w, h)
+        with ClockSampler(device) as clocks:
+            ctx.mark(0)
+            ctx.render_device(frame.params, 0, spp)
+            ctx.mark(1)
+            ms = ctx.elapsed(0, 1)
+        st = ctx.stats()
+        img = ctx.read_accumulator(w, h)
+        out[name] = {"value": w * h * spp / ms / 1e3, "unit": "Msamples/s", "ms": ms, "launches": st["launches"],
+                     "trace_ms": st["trace_ms"], "shade_ms": st["shade_ms"], "accuracy": accuracy(frame, img, crop, ref),
+                     "clocks": clocks.summary()}
+    n, count = 32, 16
+    sx, sy = w // 2 - n // 2, h // 2 - n // 2
+    ref_s = view.render_samples64(sx, sy, n, n, 0, count, cam=camera64(grid))
+    splits = {"crop": [sx, sy, n, n], "samples": n * n * count}
+    for name, frame in (("chunk", chunk), ("grid", grid)):
+        got = ctx.render_samples(frame.params, sx, sy, n, n, 0, count).astype(np.float64)
+        err = np.abs(got - ref_s)
+        split = np.any(err > 1e-3 * np.maximum(np.abs(ref_s), np.abs(got)) + 1e-5, axis=-1)
+        splits[name] = int(split.sum())
     ctx.close()
-    return {"value": w * h * spp / ms / 1e3, "unit": "Msamples/s", "ms": ms, "width": w, "height": h, "spp": spp,
-            "of_spp": R.CONFIGS["c5"].spp, "launches": st["launches"], "trace_ms": st["trace_ms"],
-            "shade_ms": st["shade_ms"], "accuracy": accuracy(frame, img), "clocks": clocks.summary()}
+    line = dict(out["chunk"])
+    line.update({"frames": "chunk-origin rebasing", "width": w, "height": h, "spp": spp, "of_spp": R.CONFIGS["c5"].spp,
+                 "grid_frame": out["grid"], "paths_split_from_fp64": splits})
+    return line
 
 
 def run_reference(args, rank, world):
@@ -472,7 +498,7 @@ def main():
     ap.add_argument("--c3-scale", type=float, default=0.25, help="spp scale of the 64 cameras (c3)")
     ap.add_argument("--no-extras", action="store_true",
                     help="leave out the other forms' lines (reference port, batched, adjoint, precision)")
-    ap.add_argument("--c5-spp", type=int, default=2048, help="spp of the precision frame in the extras")
+    ap.add_argument("--c5-spp", type=int, default=1024, help="spp of the precision frame in the extras (each frame)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -44,7 +44,14 @@ typedef struct {
     uint32_t faces[4]; /* x = face count */
 } lw_emitter;
 
-/* `Params` (scene.rs:160-228), 27 x 16 = 432 bytes, layout-identical. */
+/* `Params` (scene.rs:160-228), 27 x 16 = 432 bytes, layout-identical. Two of its unused words
+ * carry this library's chunk-origin rebasing (the precision form): see_through[2] = 1 holds every
+ * position of a path relative to the chunk corner nearest its current origin instead of the grid
+ * origin, starting from the camera's chunk corner packed in see_through[3] (chunk indices in two's
+ * complement, x in bits 0-10, y in 11-20, z in 21-31), cam_pos.xyz then being the eye relative to
+ * that corner. lw_rebase_camera sets the three from the eye in f64. see_through[2] = 0 (the
+ * reference's value) renders in the grid's frame, as the reference does. The batched and
+ * differentiable forms, and lw_trace_rays, take the grid's frame only. */
 typedef struct {
     float cam_pos[4], cam_fwd[4], cam_right[4], cam_up[4];
     float sun_dir[4], sun_color[4], sky_sun[4], sky_zenith[4];
@@ -435,6 +442,16 @@ lw_status lw_adjoint_backward(lw_ctx *ctx, const lw_adj_frame *frame, uint32_t s
  * differences (plus - minus) and of the pairs' midpoints. */
 lw_status lw_adjoint_fd(lw_ctx *ctx, const lw_adj_frame *plus, const lw_adj_frame *minus, const lw_adj_frame *nominal,
                         uint32_t spp, double *diff_rgb, double *mean_rgb);
+/* Chunk-origin rebasing of a frame's camera, on the host, in f64: the eye (relative to the grid
+ * origin, as request.rs:640-644 rebases it from the world) is split into the chunk corner nearest
+ * it, 16 * rint(eye / 16) per axis, and the remainder, at most 8 blocks on each axis, which is
+ * rounded once to f32 into params->cam_pos.xyz; see_through[2] and [3] are set as `lw_params`
+ * describes. The kernels then hold each path origin relative to its own nearest chunk corner,
+ * moving between corners by exact integer offsets. LW_ERR_INVALID_ARGUMENT for a non-finite eye
+ * or one whose chunk is outside the packed range (x and z within +-1024 chunks, y +-512). No GPU
+ * is used. */
+lw_status lw_rebase_camera(lw_params *params, const double eye[3]);
+
 /* The byte-to-linear table the kernels decode texels with: gamma_to_linear(k / 255) for k in
  * 0..255 (crates/lumenwright-kernel/src/math.rs:183-216), so a caller can form nominal albedos. */
 lw_status lw_gamma_table(float out[256]);

@@ -130,8 +130,9 @@ struct lw_ctx {
     struct WfBufs {
         DBuf<float4> state, hit0, ts;
         DBuf<float> hit1;
-        DBuf<uint32_t> queue, ctr;
+        DBuf<uint32_t> queue, ctr, frame;
         void free_() {
+            frame.free_();
             state.free_();
             hit0.free_();
             ts.free_();
@@ -310,6 +311,9 @@ lw_status check_params(lw_ctx *c, const lw_params *p, bool need_frame, uint64_t 
         return fail(c, LW_ERR_INVALID_ARGUMENT, "params.off2 does not match the scene (ov_quads offset, atlas size)");
     if (need_frame && (p->frame[0] == 0 || p->frame[1] == 0))
         return fail(c, LW_ERR_INVALID_ARGUMENT, "frame size %ux%u", p->frame[0], p->frame[1]);
+    if (p->see_through[2] > 1u)
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "params.see_through[2] = %u: the origin frames are 0 (the grid's) or 1 (chunk "
+                    "corners)", p->see_through[2]);
     if ((uint64_t)p->see_through[0] + p->see_through[1] > c->quads_len)
         return fail(c, LW_ERR_BUFFER_LENGTH, "see-through quads [%u, +%u) outside %llu quads", p->see_through[0],
                     p->see_through[1], (unsigned long long)c->quads_len);
@@ -397,9 +401,10 @@ lw_status wf_setup(lw_ctx *c, lw_ctx::WfBufs &b, uint32_t n, WfState &F, cudaStr
     CK(c, ensure(b.ts, (size_t)3 * n), "allocating the carried traversals");
     CK(c, ensure(b.hit1, n), "allocating the hits");
     CK(c, ensure(b.queue, (size_t)3 * n), "allocating the ray queues");
+    CK(c, ensure(b.frame, n), "allocating the path frames");
     CK(c, ensure(b.ctr, 16), "allocating the queue counters");
     if (!c->wf_host) CK(c, cudaMallocHost((void **)&c->wf_host, 4), "allocating a pinned word");
-    F = WfState{b.state.p, n, b.queue.p, b.hit0.p, b.hit1.p, b.ctr.p, b.ts.p};
+    F = WfState{b.state.p, n, b.queue.p, b.hit0.p, b.hit1.p, b.ctr.p, b.ts.p, b.frame.p};
     // the slots' core words (flags 0: no item yet), the counters and the iteration, the hits
     CK(c, cudaMemsetAsync(b.state.p + (size_t)4 * n, 0, (size_t)n * sizeof(float4), st), "clearing the slots");
     CK(c, cudaMemsetAsync(b.ctr.p, 0, 16 * sizeof(uint32_t), st), "clearing the queue counters");
@@ -491,7 +496,8 @@ lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const 
         CK(c, cudaEventRecord(e[0], c->stream), "recording an event");
         CK(c, launch_wf_shade(S, P, W, F, wf_shade_blocks(c, n), c->stream), "launching the shading kernel");
         CK(c, cudaEventRecord(e[1], c->stream), "recording an event");
-        CK(c, launch_wf_trace(S, P, F, c->stage_bytes ? c->shape_wf_staged : c->shape_wf, budget, c->wf_tail, c->stage_bytes,
+        const bool staged = c->stage_bytes && P.see_through.z == 0u;  // the rebased tracing kernel is unstaged
+        CK(c, launch_wf_trace(S, P, F, staged ? c->shape_wf_staged : c->shape_wf, budget, c->wf_tail, staged ? c->stage_bytes : 0,
                               c->stream), "launching the tracing kernel");
         CK(c, cudaEventRecord(e[2], c->stream), "recording an event");
         CK(c, launch_wf_advance(F, c->stream), "launching the iteration step");
@@ -1168,6 +1174,8 @@ lw_status lw_batch_prepare(lw_ctx *c, const lw_camera_job *jobs, uint32_t n) {
         lw_status s = check_params(c, &jobs[i].params, true, jobs[i].sky_len);
         if (s != LW_OK) return s;
         if (jobs[i].spp == 0) return fail(c, LW_ERR_INVALID_ARGUMENT, "camera %u has spp 0", i);
+        if (jobs[i].params.see_through[2])
+            return fail(c, LW_ERR_INVALID_ARGUMENT, "camera %u: the batched form renders in the grid's frame only", i);
     }
     // Layout: items, slots, accumulators, images, item sums.
     uint64_t total_samples = 0;
@@ -1409,6 +1417,24 @@ lw_status lw_draw_sky_map(lw_ctx *c, const lw_quick_sky *q, const uint32_t *star
     return LW_OK;
 }
 
+lw_status lw_rebase_camera(lw_params *p, const double eye[3]) {
+    if (!p || !eye) return LW_ERR_INVALID_ARGUMENT;
+    const int lo[3] = {-1024, -512, -1024}, hi[3] = {1023, 511, 1023};
+    int k[3];
+    float local[3];
+    for (int a = 0; a < 3; a++) {
+        if (!std::isfinite(eye[a])) return LW_ERR_INVALID_ARGUMENT;
+        const double ch = std::nearbyint(eye[a] / 16.0);  // exact scaling, rounding to the nearest (ties to even)
+        if (ch < lo[a] || ch > hi[a]) return LW_ERR_INVALID_ARGUMENT;
+        k[a] = (int)ch;
+        local[a] = (float)(eye[a] - 16.0 * ch);  // exact in f64, rounded once to f32
+    }
+    for (int a = 0; a < 3; a++) p->cam_pos[a] = local[a];
+    p->see_through[2] = 1u;
+    p->see_through[3] = ((uint32_t)k[0] & 0x7FFu) | (((uint32_t)k[1] & 0x3FFu) << 11) | (((uint32_t)k[2] & 0x7FFu) << 21);
+    return LW_OK;
+}
+
 lw_status lw_gamma_table(float out[256]) {
     if (!out) return LW_ERR_INVALID_ARGUMENT;
     for (int k = 0; k < 256; k++) out[k] = ref_gamma_to_linear((float)k / 255.0f);
@@ -1426,6 +1452,8 @@ lw_status adj_upload(lw_ctx *c, const lw_adj_frame *f, int k, AdjFrame &out, uin
         return fail(c, LW_ERR_INVALID_ARGUMENT, "adjoint frame %d: null argument", k);
     lw_status s = check_params(c, f->params, true, f->sky_len);
     if (s != LW_OK) return s;
+    if (f->params->see_through[2])
+        return fail(c, LW_ERR_INVALID_ARGUMENT, "adjoint frame %d: the differentiable form renders in the grid's frame only", k);
     if (f->params->misc_f[2] >= 1.0f && f->params->sky_map[0] < 1.0f) {
         double n = std::floor((double)f->params->misc_f[2]);
         if ((n + 1.0) * (n + 1.0) * 3.0 > (double)f->sky_len) return fail(c, LW_ERR_BUFFER_LENGTH, "sky cache too short");

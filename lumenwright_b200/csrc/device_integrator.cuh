@@ -135,13 +135,30 @@ LW_DI uint32_t pick(uint32_t n, float u) {
     return i < n ? i : n - 1u;
 }
 
-LW_DI void emitter_cell(const DevScene &S, V3 p, uint32_t &start, uint32_t &count) {
+// The cell of integer block coordinate b in cells of `cell` (an integer) blocks, floor(b / cell):
+// exact in f32 for |b| < 2^24, which every block coordinate of a packable frame is: the quotient's
+// rounding error, at most |b| / cell * 2^-24, is below 1 / cell, the least distance from a quotient
+// that is not an integer to the integers.
+LW_DI int cell_of_block(int b, float cell) { return to_i32(floorf(__fdiv_rn((float)b, cell))); }
+
+// emitter_cell (integrator.rs:358-373). REB: p is in frame A, and the cell is found from p's
+// block in the grid, floor(p) + A: for an integer cell size, floor((b + f) / size) =
+// floor(b / size) for every fraction f in [0, 1), so this is the cell of the exact position.
+template <bool REB = false>
+LW_DI void emitter_cell(const DevScene &S, V3 p, uint32_t &start, uint32_t &count, const Frame &A = Frame{}) {
     const uint32_t *g = S.emitter_grid;
     float cell = (float)ldg(g);
     int sx = (int)ldg(g + 1), sy = (int)ldg(g + 2), sz = (int)ldg(g + 3);
-    int cx = to_i32(floorf(__fdiv_rn(p.x, cell))) - (int)ldg(g + 4);
-    int cy = to_i32(floorf(__fdiv_rn(p.y, cell))) - (int)ldg(g + 5);
-    int cz = to_i32(floorf(__fdiv_rn(p.z, cell))) - (int)ldg(g + 6);
+    int cx, cy, cz;
+    if (REB) {
+        cx = cell_of_block(to_i32(floorf(p.x)) + A.x(), cell) - (int)ldg(g + 4);
+        cy = cell_of_block(to_i32(floorf(p.y)) + A.y(), cell) - (int)ldg(g + 5);
+        cz = cell_of_block(to_i32(floorf(p.z)) + A.z(), cell) - (int)ldg(g + 6);
+    } else {
+        cx = to_i32(floorf(__fdiv_rn(p.x, cell))) - (int)ldg(g + 4);
+        cy = to_i32(floorf(__fdiv_rn(p.y, cell))) - (int)ldg(g + 5);
+        cz = to_i32(floorf(__fdiv_rn(p.z, cell))) - (int)ldg(g + 6);
+    }
     if (cx < 0 || cy < 0 || cz < 0 || cx >= sx || cy >= sy || cz >= sz) {
         start = 0u;
         count = 0u;
@@ -174,19 +191,24 @@ LW_COLD bool water_interface(const DevParams &P, V3 pos, V3 d, V3 n, bool front,
     return front;
 }
 
-LW_DI bool water_plane(const DevParams &P, V3 o, V3 d, float &tp) {
+// The water plane's height in frame A.
+LW_DI float water_height(const DevParams &P, const Frame &A) { return P.water_plane.x - (float)A.y(); }
+
+// water_plane (integrator.rs:511-526); o in frame A, where the grid's columns span [-A, size - A).
+LW_DI bool water_plane(const DevParams &P, V3 o, V3 d, float &tp, const Frame &A = Frame{}) {
     if (P.water_plane.y == 0.0f || d.y == 0.0f) return false;
-    float t = __fdiv_rn(P.water_plane.x - o.y, d.y);
+    float t = __fdiv_rn(water_height(P, A) - o.y, d.y);
     if (!(t > 0.0f && t < kINF)) return false;
     V3 at = o + d * t;
-    float sx = (float)(P.grid_dims.x * 16u), sz = (float)(P.grid_dims.z * 16u);
-    if (at.x >= 0.0f && at.z >= 0.0f && at.x < sx && at.z < sz) return false;
+    float x0 = (float)(-A.x()), z0 = (float)(-A.z());
+    float sx = (float)((int)(P.grid_dims.x * 16u) - A.x()), sz = (float)((int)(P.grid_dims.z * 16u) - A.z());
+    if (at.x >= x0 && at.z >= z0 && at.x < sx && at.z < sz) return false;
     tp = t;
     return true;
 }
 
-LW_DI bool under_water_plane(const DevParams &P, V3 o, V3 d) {
-    return P.water_plane.y != 0.0f && o.y < P.water_plane.x && d.y <= 0.0f;
+LW_DI bool under_water_plane(const DevParams &P, V3 o, V3 d, const Frame &A = Frame{}) {
+    return P.water_plane.y != 0.0f && o.y < water_height(P, A) && d.y <= 0.0f;
 }
 
 // ---- the per-lane path ----------------------------------------------------------------------
@@ -215,6 +237,8 @@ struct Path {
     uint32_t emode, fmode;
     V3 eoff;
     float dist;
+    // with chunk-origin rebasing, the frame (frame_word) that o and origin are held in
+    uint32_t frame;
 };
 
 }  // namespace lw

@@ -21,7 +21,12 @@ enum Act : uint32_t {
     A_FINISH_SURFACE,   // Russian roulette and the next direction
 };
 
+// Whether the frame's Params ask for chunk-origin rebasing: the camera's position is then given
+// relative to the chunk corner of word see_through.w.
+LW_HDI bool rebased(const DevParams &P) { return P.see_through.z != 0u; }
+
 // The camera ray of sample `sample` at pixel (px, py) (integrator.rs:545-569).
+template <bool REB = false>
 LW_DI void begin_sample(Path &p, const DevParams &P, uint32_t px, uint32_t py, uint32_t sample) {
     uint32_t width = P.frame.x, height = P.frame.y;
     p.rng = rng_new(py * width + px, sample, P.misc_u.x);
@@ -32,6 +37,7 @@ LW_DI void begin_sample(Path &p, const DevParams &P, uint32_t px, uint32_t py, u
     float sy = (1.0f - __fdiv_rn(2.0f * ((float)py + jy), (float)height)) * tan_half;
     p.d = normalize(f4v(P.cam_fwd) + f4v(P.cam_right) * sx + f4v(P.cam_up) * sy);
     p.o = f4v(P.cam_pos);
+    if (REB) p.frame = P.see_through.w;
     p.radiance = v3(0.0f, 0.0f, 0.0f);
     p.beta = v3(1.0f, 1.0f, 1.0f);
     p.bounces = 0;
@@ -46,13 +52,18 @@ LW_DI void begin_sample(Path &p, const DevParams &P, uint32_t px, uint32_t py, u
 LW_DI uint32_t strategy_of(const DevParams &P) { return P.misc_u.w > 0u ? P.emitter.x : EMITTER_SAMPLING_NONE; }
 
 // The result of a path ray (the body of render_sample's event loop, integrator.rs:571-706).
+// REB (chunk-origin rebasing): the path's positions are in the frame of p.frame; each new origin
+// (the offset origin of a surface, a water crossing, a translucent pass) moves the path to the
+// frame of the chunk corner nearest it (rebase), after the last use of the old frame.
+template <bool REB = false>
 LW_DI Act on_extend(Path &p, const DevScene &S, const DevParams &P, Hit h) {
     const float eps = P.misc_f.y;
+    const Frame A = REB ? frame_of(p.frame) : Frame{};
     p.events++;
     bool found = h.quad != NO_QUAD;
     bool forced = false;
     if (p.bounces == 0 && P.see_through.y > 0u && found && !is_see_through(P, h.quad)) {
-        Hit st = see_through_hit(S, P, p.o, p.d, h.t);
+        Hit st = see_through_hit<REB>(S, P, p.o, p.d, h.t, A);
         if (st.quad != NO_QUAD) {
             uint32_t sflags = __float_as_uint(ldg(&S.quads[st.quad].p0_flags).w);
             if ((sflags & FLAG_ALPHA_MASK) == ALPHA_TRANSLUCENT) {
@@ -78,14 +89,14 @@ LW_DI Act on_extend(Path &p, const DevScene &S, const DevParams &P, Hit h) {
     // through the remaining steps.
     Act act = A_EMIT_START;
     bool done = false;
-    if (water_plane(P, p.o, p.d, tp) && (!found || tp < h.t)) {
+    if (water_plane(P, p.o, p.d, tp, A) && (!found || tp < h.t)) {
         if (p.in_water) p.beta = vmul(p.beta, transmittance(sigma, tp));
         wfront = p.d.y < 0.0f;
         wn = v3(0.0f, wfront ? 1.0f : -1.0f, 0.0f);
         wpos = p.o + p.d * tp;
         water = true;
     } else if (!found) {
-        if (!p.in_water && !under_water_plane(P, p.o, p.d)) {
+        if (!p.in_water && !under_water_plane(P, p.o, p.d, A)) {
             p.radiance = p.radiance + vmul(p.beta, sky_of(S, P, p.d, p.bounces == 0));
             if (p.specular && p.bounces == 0) p.radiance = p.radiance + vmul(p.beta, sun_texture(S, P, p.d));
         }
@@ -120,6 +131,7 @@ LW_DI Act on_extend(Path &p, const DevScene &S, const DevParams &P, Hit h) {
         p.in_water = water_interface(P, wpos, p.d, wn, wfront, p.in_water, eps, p.rng, nd, no);
         p.d = nd;
         p.o = no;
+        if (REB) rebase(p.o, p.frame);
         p.specular = true;
         p.tmin = 0.0f;
         act = A_CONTINUE;
@@ -128,6 +140,7 @@ LW_DI Act on_extend(Path &p, const DevScene &S, const DevParams &P, Hit h) {
     if (!done && !forced && (flags & FLAG_ALPHA_MASK) == ALPHA_TRANSLUCENT && rng_next(p.rng) >= alpha) {
         p.beta = vmul(p.beta, lerp(v3(1.0f, 1.0f, 1.0f), albedo, alpha));
         p.o = pos + p.d * eps;
+        if (REB) rebase(p.o, p.frame);
         p.tmin = 0.0f;
         act = A_CONTINUE;
         done = true;
@@ -148,11 +161,12 @@ LW_DI Act on_extend(Path &p, const DevScene &S, const DevParams &P, Hit h) {
         // beta.mul(albedo), the factor of the sun and emitter terms and the path's next beta.
         p.beta = vmul(p.beta, albedo);
         if (!emits && strategy != EMITTER_SAMPLING_NONE) {
-            emitter_cell(S, pos, p.list, p.count);  // no draw: evaluated here, used after the sun
-            p.emode = 1u;                           // emitters to sample
+            emitter_cell<REB>(S, pos, p.list, p.count, A);  // no draw: evaluated here, used after the sun
+            p.emode = 1u;                                   // emitters to sample
         } else {
             p.emode = 0u;
         }
+        if (REB) rebase(p.origin, p.frame);  // the rays from this surface start in the new frame
 
         V3 sun = f4v(P.sun_dir);
         float sin_r = __fsqrt_rn(fmax_r(1.0f - P.sun_dir.w * P.sun_dir.w, 0.0f));
@@ -226,6 +240,7 @@ LW_DI Act on_emit(Path &p, const DevScene &S, const DevParams &P, const Hit &h, 
 // run each step's code together as they fall through it; only the loop over emitters and faces
 // goes back. A lane that is done (a ray to trace, or the path's end) falls through the remaining
 // steps rather than leaving early: one exit keeps the steps' code and registers shared.
+template <bool REB = false>
 LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 val) {
     const float eps = P.misc_f.y;
     bool done = act == A_TRACE || act == A_END;
@@ -268,6 +283,7 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
             float4 e0 = ldg(S.emitters + 2u * i);
             float4 e1 = ldg(S.emitters + 2u * i + 1u);
             p.eoff = f4v(e0);
+            if (REB) p.eoff = p.eoff - frame_origin(frame_of(p.frame));  // the block's corner in the frame: exact
             p.first = __float_as_uint(e0.w);
             p.faces = __float_as_uint(e1.x);
             if (p.faces == 0u) {
@@ -375,16 +391,18 @@ LW_DI Act advance(Path &p, const DevScene &S, const DevParams &P, Act act, V3 va
 }
 
 // The result of the lane's last ray, by its kind (on_extend, on_shadow, on_emit).
+template <bool REB = false>
 LW_DI Act on_result(Path &p, const DevScene &S, const DevParams &P, const Hit &h, V3 &val) {
-    if (p.kind == K_EXTEND) return on_extend(p, S, P, h);
+    if (p.kind == K_EXTEND) return on_extend<REB>(p, S, P, h);
     if (p.kind == K_SHADOW) return on_shadow(p, S, P, h);
     return on_emit(p, S, P, h, val);
 }
 
+template <bool REB = false>
 LW_DI Act shade(Path &p, const DevScene &S, const DevParams &P, const Hit &h) {
     V3 val = v3(0.0f, 0.0f, 0.0f);
-    Act a = on_result(p, S, P, h, val);
-    return advance(p, S, P, a, val);
+    Act a = on_result<REB>(p, S, P, h, val);
+    return advance<REB>(p, S, P, a, val);
 }
 
 LW_DI void kahan_add(float &s, float &c, float x) {

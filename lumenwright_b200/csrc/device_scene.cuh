@@ -92,6 +92,46 @@ struct Hit {
 };
 LW_DI Hit no_hit() { return Hit{kINF, NO_QUAD, 0u, 0.0f, 0.0f}; }
 
+// ---- chunk-origin frames ------------------------------------------------------------------------
+// With chunk-origin rebasing (Params.see_through.z = 1) a path's positions are held relative to a
+// chunk corner A of the grid (a multiple of 16 blocks on each axis), the corner nearest the path's
+// current origin, so every origin is within 8 blocks of its frame's origin: an f32 step of 2^-20
+// block at most, where a grid-relative coordinate of a 32-chunk grid has steps of 2^-15. The word
+// packs A's chunk indices in two's complement: x in bits 0-10, y in 11-20, z in 21-31. The grid's
+// cell c is the frame's integer c - A, so the traversal forms its boundaries in the frame from
+// integers, exactly, and reads the grid at the grid's own indices. In the grid's own frame
+// (rebasing off) A is 0 and every expression below reduces to the reference's.
+// The frame is kept as its packed word (one register in the kernels' loops) and unpacked where it
+// is used; the grid's frame is word 0, for which every use below folds to the reference's
+// expression.
+struct Frame {
+    uint32_t w;  // the packed chunk indices (frame_word)
+    // the frame's origin in the grid, in blocks (16 x the chunk index, sign-extended)
+    LW_DI int x() const { return (int)(w << 21) >> 17; }
+    LW_DI int y() const { return ((int)(w << 11) >> 18) & ~15; }
+    LW_DI int z() const { return ((int)w >> 17) & ~15; }
+};
+LW_DI Frame frame_of(uint32_t w) { return Frame{w}; }
+LW_DI uint32_t frame_word(int cx, int cy, int cz) {
+    return ((uint32_t)cx & 0x7FFu) | (((uint32_t)cy & 0x3FFu) << 11) | (((uint32_t)cz & 0x7FFu) << 21);
+}
+LW_DI V3 frame_origin(const Frame &A) { return v3((float)A.x(), (float)A.y(), (float)A.z()); }
+
+// Moves position x, held in the frame of word w, to the frame of the chunk corner nearest it:
+// k = rint(x / 16) chunks per axis (the frame kept within the packable chunk range), x - 16 k. Both
+// steps are exact: x / 16 is a scaling by a power of two, 16 k and x are multiples of x's ulp, and
+// |x - 16 k| <= |x| whenever k != 0, so the difference is representable.
+LW_DI int chunk_step(float x) { return to_i32(fminf(fmaxf(rintf(x * 0.0625f), -4096.0f), 4096.0f)); }
+LW_DI void rebase(V3 &x, uint32_t &w) {
+    const Frame f = frame_of(w);
+    const int cx = f.x() >> 4, cy = f.y() >> 4, cz = f.z() >> 4;
+    const int nx = clamp_i(cx + chunk_step(x.x), -1024, 1023);
+    const int ny = clamp_i(cy + chunk_step(x.y), -512, 511);
+    const int nz = clamp_i(cz + chunk_step(x.z), -1024, 1023);
+    x = v3(x.x - (float)((nx - cx) * 16), x.y - (float)((ny - cy) * 16), x.z - (float)((nz - cz) * 16));
+    w = frame_word(nx, ny, nz);
+}
+
 // SceneView::texel (scene.rs:288-294).
 LW_DI uint32_t texel(const DevScene &S, const DevParams &P, float u, float v) {
     int w = (int)P.off2.y, h = (int)P.off2.z;
@@ -110,8 +150,11 @@ LW_DI V3 linear_rgb(const float *gamma, uint32_t c) {
 // is not cut out; the hit in `h`. The normal eu x ev and n . n come precomputed; a front-only quad
 // met from behind is rejected before the division instead of after it: `normal() . d` is exactly
 // `-(n . d)`, and intersect_quad has no side effects, so the outcome is the reference's.
+// SHIFT: the quad's p0 is taken relative to `pb` (p0 - pb), for a quad given in grid coordinates
+// and a ray in another frame.
+template <bool SHIFT = false>
 LW_DI bool quad_candidate(const DevScene &S, const DevParams &P, uint32_t qi, V3 o, V3 d, float tmin, float t_limit,
-                          Hit &h) {
+                          Hit &h, V3 pb = V3{0.0f, 0.0f, 0.0f}) {
     const DevQuad *q = S.quads + qi;
     float4 a = ldg(&q->n_nn);
     V3 n = f4v(a);
@@ -121,6 +164,7 @@ LW_DI bool quad_candidate(const DevScene &S, const DevParams &P, uint32_t qi, V3
     uint32_t flags = __float_as_uint(b.w);
     if ((flags & FLAG_FRONT_ONLY) && -denom >= 0.0f) return false;
     V3 p0 = f4v(b);
+    if (SHIFT) p0 = p0 - pb;
     float t = __fdiv_rn(dot(n, p0 - o), denom);
     if (!(t > tmin && t < t_limit)) return false;
     V3 eu = f4v(ldg(&q->eu_tint));
@@ -151,9 +195,11 @@ LW_DI float reach_of(const Hit &best, uint32_t qi) {
 }
 
 // test_quad (trace.rs:81-109).
-LW_DI void test_quad(const DevScene &S, const DevParams &P, uint32_t qi, V3 o, V3 d, float tmin, Hit &best) {
+template <bool SHIFT = false>
+LW_DI void test_quad(const DevScene &S, const DevParams &P, uint32_t qi, V3 o, V3 d, float tmin, Hit &best,
+                     V3 pb = V3{0.0f, 0.0f, 0.0f}) {
     const float reach = reach_of(best, qi);
-    quad_candidate(S, P, qi, o, d, tmin, reach, best);  // writes `best` only when the quad is taken
+    quad_candidate<SHIFT>(S, P, qi, o, d, tmin, reach, best, pb);  // writes `best` only when the quad is taken
 }
 
 // SceneView::voxel (scene.rs:271-284) on the re-laid grid.
@@ -175,9 +221,10 @@ LW_DI float safe_inv(float x) {  // trace.rs:293-299
     return __fdiv_rn(1.0f, x);
 }
 LW_DI int sgn(float x) { return x > 0.0f ? 1 : (x < 0.0f ? -1 : 0); }
-LW_DI float next_boundary(float o, float inv, int cell, int step) {  // trace.rs:313-319
+// `a`: the frame's origin on this axis (the boundary of grid cell c is at c - a in the frame).
+LW_DI float next_boundary(float o, float inv, int cell, int step, int a = 0) {  // trace.rs:313-319
     if (step == 0) return kINF;
-    float bound = (float)(step > 0 ? cell + 1 : cell);
+    float bound = (float)((step > 0 ? cell + 1 : cell) - a);
     return (bound - o) * inv;
 }
 
@@ -189,7 +236,8 @@ struct Dda {
     float n0, n1, n2;  // distances to its next boundary along each axis
     float t;           // distance at which the ray entered the cell
 };
-LW_DI bool dda_advance(Dda &s, V3 o, V3 inv, int s0, int s1, int s2, int gs0, int gs1, int gs2, float t_end) {
+LW_DI bool dda_advance(Dda &s, V3 o, V3 inv, int s0, int s1, int s2, int gs0, int gs1, int gs2, float t_end,
+                       const Frame &A = Frame{}) {
     int axis = s.n0 < s.n1 ? (s.n0 < s.n2 ? 0 : 2) : (s.n1 < s.n2 ? 1 : 2);
     bool ax0 = axis == 0, ax1 = axis == 1;
     s.t = ax0 ? s.n0 : (ax1 ? s.n1 : s.n2);
@@ -198,7 +246,8 @@ LW_DI bool dda_advance(Dda &s, V3 o, V3 inv, int s0, int s1, int s2, int gs0, in
     int c = (ax0 ? s.c0 : (ax1 ? s.c1 : s.c2)) + st;
     int g = ax0 ? gs0 : (ax1 ? gs1 : gs2);
     if (c < 0 || c >= g) return false;
-    float nb = next_boundary(ax0 ? o.x : (ax1 ? o.y : o.z), ax0 ? inv.x : (ax1 ? inv.y : inv.z), c, st);
+    float nb = next_boundary(ax0 ? o.x : (ax1 ? o.y : o.z), ax0 ? inv.x : (ax1 ? inv.y : inv.z), c, st,
+                             ax0 ? A.x() : (ax1 ? A.y() : A.z()));
     s.c0 = ax0 ? c : s.c0;
     s.c1 = ax1 ? c : s.c1;
     s.c2 = (!ax0 && !ax1) ? c : s.c2;
@@ -220,12 +269,14 @@ struct TraceState {
 
 // The set-up of trace (trace.rs:137-174): the slab test against the grid and the first cell.
 // False when the range misses the grid (trace returns None at once).
-LW_DI bool trace_begin(TraceState &ts, const DevParams &P, V3 o, V3 d, float tmax) {
+// In frame A the grid spans [-A, size - A).
+LW_DI bool trace_begin(TraceState &ts, const DevParams &P, V3 o, V3 d, float tmax, const Frame &A = Frame{}) {
     const uint32_t dx = P.grid_dims.x, dy = P.grid_dims.y, dz = P.grid_dims.z;
-    V3 size = v3((float)(dx * 16u), (float)(dy * 16u), (float)(dz * 16u));
+    V3 lo = v3((float)(-A.x()), (float)(-A.y()), (float)(-A.z()));
+    V3 hi = v3((float)((int)(dx * 16u) - A.x()), (float)((int)(dy * 16u) - A.y()), (float)((int)(dz * 16u) - A.z()));
     V3 inv = v3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
-    V3 ta = vmul(v3(0.0f, 0.0f, 0.0f) - o, inv);
-    V3 tb = vmul(size - o, inv);
+    V3 ta = vmul(lo - o, inv);
+    V3 tb = vmul(hi - o, inv);
     float t_enter = fmax_r(fmax_r(fmin_r(ta.x, tb.x), fmin_r(ta.y, tb.y)), fmin_r(ta.z, tb.z));
     float t_exit = fmin_r(fmin_r(fmax_r(ta.x, tb.x), fmax_r(ta.y, tb.y)), fmax_r(ta.z, tb.z));
     float t0 = fmax_r(t_enter, 0.0f);
@@ -233,12 +284,12 @@ LW_DI bool trace_begin(TraceState &ts, const DevParams &P, V3 o, V3 d, float tma
     if (t0 > t_end) return false;
     V3 start = o + d * (t0 + 1e-4f);
     const int s0 = sgn(d.x), s1 = sgn(d.y), s2 = sgn(d.z);
-    ts.s.c0 = clamp_i(to_i32(floorf(start.x)), 0, (int)dx * 16 - 1);
-    ts.s.c1 = clamp_i(to_i32(floorf(start.y)), 0, (int)dy * 16 - 1);
-    ts.s.c2 = clamp_i(to_i32(floorf(start.z)), 0, (int)dz * 16 - 1);
-    ts.s.n0 = next_boundary(o.x, inv.x, ts.s.c0, s0);
-    ts.s.n1 = next_boundary(o.y, inv.y, ts.s.c1, s1);
-    ts.s.n2 = next_boundary(o.z, inv.z, ts.s.c2, s2);
+    ts.s.c0 = clamp_i(to_i32(floorf(start.x)) + A.x(), 0, (int)dx * 16 - 1);
+    ts.s.c1 = clamp_i(to_i32(floorf(start.y)) + A.y(), 0, (int)dy * 16 - 1);
+    ts.s.c2 = clamp_i(to_i32(floorf(start.z)) + A.z(), 0, (int)dz * 16 - 1);
+    ts.s.n0 = next_boundary(o.x, inv.x, ts.s.c0, s0, A.x());
+    ts.s.n1 = next_boundary(o.y, inv.y, ts.s.c1, s1, A.y());
+    ts.s.n2 = next_boundary(o.z, inv.z, ts.s.c2, s2, A.z());
     ts.s.t = t0;
     ts.inv = inv;
     ts.t_end = t_end;
@@ -275,7 +326,7 @@ LW_DI RayDda ray_dda(const DevParams &P, V3 d) {
 //    iteration of the reference's loop does.
 template <bool RUNS = true, bool STAGED = false>
 LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, const RayDda &R, BrickCache &bc,
-                uint32_t &model) {
+                uint32_t &model, const Frame &A = Frame{}) {
     const uint32_t dx = P.grid_dims.x, dz = P.grid_dims.z;
     Dda &s = ts.s;
     if (ts.it >= MAX_STEPS) return -1;
@@ -301,28 +352,28 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
             float t_out = kINF;
             int axis = 0;
             if (R.s0 != 0) {
-                float tt = ((float)(R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
+                float tt = ((float)((R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - A.x()) - o.x) * inv.x;
                 if (tt < t_out) { t_out = tt; axis = 0; }
             }
             if (R.s1 != 0) {
-                float tt = ((float)(R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
+                float tt = ((float)((R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - A.y()) - o.y) * inv.y;
                 if (tt < t_out) { t_out = tt; axis = 1; }
             }
             if (R.s2 != 0) {
-                float tt = ((float)(R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
+                float tt = ((float)((R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - A.z()) - o.z) * inv.z;
                 if (tt < t_out) { t_out = tt; axis = 2; }
             }
             if (t_out > ts.t_end) return -1;
             V3 pos = o + d * t_out;
-            s.c0 = axis == 0 ? (R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
-            s.c1 = axis == 1 ? (R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
-            s.c2 = axis == 2 ? (R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
+            s.c0 = axis == 0 ? (R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)) + A.x(), bc0 * 16, bc0 * 16 + 15);
+            s.c1 = axis == 1 ? (R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)) + A.y(), bc1 * 16, bc1 * 16 + 15);
+            s.c2 = axis == 2 ? (R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)) + A.z(), bc2 * 16, bc2 * 16 + 15);
             int ca = axis == 0 ? s.c0 : (axis == 1 ? s.c1 : s.c2);
             int ga = axis == 0 ? R.gs0 : (axis == 1 ? R.gs1 : R.gs2);
             if (ca < 0 || ca >= ga) return -1;
-            s.n0 = next_boundary(o.x, inv.x, s.c0, R.s0);
-            s.n1 = next_boundary(o.y, inv.y, s.c1, R.s1);
-            s.n2 = next_boundary(o.z, inv.z, s.c2, R.s2);
+            s.n0 = next_boundary(o.x, inv.x, s.c0, R.s0, A.x());
+            s.n1 = next_boundary(o.y, inv.y, s.c1, R.s1, A.y());
+            s.n2 = next_boundary(o.z, inv.z, s.c2, R.s2, A.z());
             s.t = t_out;
             return 0;
         }
@@ -332,9 +383,9 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
         // stepped brick by brick here, each one counted as the reference's loop counts it, and
         // the cell, next boundaries and distance are formed once, as the last skip forms them.
         int bc0 = (int)bx, bc1 = (int)by, bc2 = (int)bz;
-        float e0 = R.s0 != 0 ? ((float)(R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x : kINF;
-        float e1 = R.s1 != 0 ? ((float)(R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y : kINF;
-        float e2 = R.s2 != 0 ? ((float)(R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z : kINF;
+        float e0 = R.s0 != 0 ? ((float)((R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - A.x()) - o.x) * inv.x : kINF;
+        float e1 = R.s1 != 0 ? ((float)((R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - A.y()) - o.y) * inv.y : kINF;
+        float e2 = R.s2 != 0 ? ((float)((R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - A.z()) - o.z) * inv.z : kINF;
         float t_out;
         int axis;
         for (;;) {
@@ -365,17 +416,17 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
             bc0 = nb0;
             bc1 = nb1;
             bc2 = nb2;
-            if (axis == 0) e0 = ((float)(R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - o.x) * inv.x;
-            else if (axis == 1) e1 = ((float)(R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - o.y) * inv.y;
-            else e2 = ((float)(R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - o.z) * inv.z;
+            if (axis == 0) e0 = ((float)((R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16) - A.x()) - o.x) * inv.x;
+            else if (axis == 1) e1 = ((float)((R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16) - A.y()) - o.y) * inv.y;
+            else e2 = ((float)((R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16) - A.z()) - o.z) * inv.z;
         }
         V3 pos = o + d * t_out;
-        s.c0 = axis == 0 ? (R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)), bc0 * 16, bc0 * 16 + 15);
-        s.c1 = axis == 1 ? (R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)), bc1 * 16, bc1 * 16 + 15);
-        s.c2 = axis == 2 ? (R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)), bc2 * 16, bc2 * 16 + 15);
-        s.n0 = next_boundary(o.x, inv.x, s.c0, R.s0);
-        s.n1 = next_boundary(o.y, inv.y, s.c1, R.s1);
-        s.n2 = next_boundary(o.z, inv.z, s.c2, R.s2);
+        s.c0 = axis == 0 ? (R.s0 > 0 ? (bc0 + 1) * 16 : bc0 * 16 - 1) : clamp_i(to_i32(floorf(pos.x)) + A.x(), bc0 * 16, bc0 * 16 + 15);
+        s.c1 = axis == 1 ? (R.s1 > 0 ? (bc1 + 1) * 16 : bc1 * 16 - 1) : clamp_i(to_i32(floorf(pos.y)) + A.y(), bc1 * 16, bc1 * 16 + 15);
+        s.c2 = axis == 2 ? (R.s2 > 0 ? (bc2 + 1) * 16 : bc2 * 16 - 1) : clamp_i(to_i32(floorf(pos.z)) + A.z(), bc2 * 16, bc2 * 16 + 15);
+        s.n0 = next_boundary(o.x, inv.x, s.c0, R.s0, A.x());
+        s.n1 = next_boundary(o.y, inv.y, s.c1, R.s1, A.y());
+        s.n2 = next_boundary(o.z, inv.z, s.c2, R.s2, A.z());
         s.t = t_out;
         return 0;
     }
@@ -392,33 +443,48 @@ LW_DI int visit(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 
         }
     }
     if (model != 0u || bc.ov != EMPTY) return 1;
-    return dda_advance(s, o, inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end) ? 0 : -1;
+    return dda_advance(s, o, inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end, A) ? 0 : -1;
+}
+
+// The overlay quads of the cell: in the grid's frame with the ray's own origin (trace.rs:243-263);
+// in a chunk frame (REB) relative to the cell, like a model's quads: the origin o - (c - A) and the
+// quads' p0 - c.
+template <bool REB>
+LW_DI void test_overlay(const DevScene &S, const DevParams &P, const Dda &s, uint32_t ov, V3 o, V3 olo, V3 d, float t_lo,
+                        Hit &best) {
+    uint32_t local = (uint32_t)((((s.c1 & 15) * 16 + (s.c2 & 15)) * 16) + (s.c0 & 15));
+    size_t base = (size_t)P.off.w + (size_t)ov * OV_CELL_WORDS + local * 2u;
+    uint32_t off = ldg(S.grid + base);
+    uint32_t count = ldg(S.grid + base + 1);
+    const V3 cell = v3((float)s.c0, (float)s.c1, (float)s.c2);
+    for (uint32_t i = 0; i < count; i++) {
+        uint32_t qi = ldg(S.grid + (size_t)P.off2.x + off + i);
+        if (REB) test_quad<true>(S, P, qi, olo, d, t_lo, best, cell);
+        else test_quad(S, P, qi, o, d, t_lo, best);
+    }
+}
+
+// The origin relative to the cell the DDA is in: o - (c - A).
+LW_DI V3 cell_origin(V3 o, const Dda &s, const Frame &A) {
+    return o - v3((float)(s.c0 - A.x()), (float)(s.c1 - A.y()), (float)(s.c2 - A.z()));
 }
 
 // The quads of the cell the DDA is in (trace.rs:228-264): true with the closest hit in `out`.
+template <bool REB = false>
 LW_DI bool test_cell(const DevScene &S, const DevParams &P, const TraceState &ts, V3 o, V3 d, float tmin, uint32_t model,
-                     uint32_t ov, Hit &out) {
+                     uint32_t ov, Hit &out, const Frame &A = Frame{}) {
     const Dda &s = ts.s;
     float t_cell_exit = fmin_r(s.n0, fmin_r(s.n1, s.n2));
     float t_lo = fmax_r(s.t - 1e-4f, tmin);
     float t_hi = t_cell_exit + 1e-4f;
     Hit cand = no_hit();
     cand.t = fmin_r(t_hi, ts.t_end + 1e-3f);
+    const V3 lo = cell_origin(o, s, A);
     if (model != 0u) {
         uint4 m = ldg(S.models + model);
-        V3 lo = o - v3((float)s.c0, (float)s.c1, (float)s.c2);
         for (uint32_t i = 0; i < m.y; i++) test_quad(S, P, m.x + i, lo, d, t_lo, cand);
     }
-    if (ov != EMPTY) {
-        uint32_t local = (uint32_t)((((s.c1 & 15) * 16 + (s.c2 & 15)) * 16) + (s.c0 & 15));
-        size_t base = (size_t)P.off.w + (size_t)ov * OV_CELL_WORDS + local * 2u;
-        uint32_t off = ldg(S.grid + base);
-        uint32_t count = ldg(S.grid + base + 1);
-        for (uint32_t i = 0; i < count; i++) {
-            uint32_t qi = ldg(S.grid + (size_t)P.off2.x + off + i);
-            test_quad(S, P, qi, o, d, t_lo, cand);
-        }
-    }
+    if (ov != EMPTY) test_overlay<REB>(S, P, s, ov, o, lo, d, t_lo, cand);
     if (cand.quad == NO_QUAD) return false;
     out = cand;
     return true;
@@ -432,9 +498,9 @@ LW_DI bool test_cell(const DevScene &S, const DevParams &P, const TraceState &ts
 // how the lanes of a warp are kept together: the loop is split in two (a "while-while" traversal),
 // an inner loop that steps through empty bricks and empty voxels until the ray reaches a cell with
 // quads, then the quads of that cell, so the lanes of a warp reach the quad tests together.
-template <bool RUNS = true>
+template <bool RUNS = true, bool REB = false>
 LW_DI int trace_run(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, float tmin, uint32_t budget,
-                    Hit &out) {
+                    Hit &out, const Frame &A = Frame{}) {
     const RayDda R = ray_dda(P, d);
     BrickCache bc = no_brick();
     uint32_t n = 0;
@@ -443,12 +509,12 @@ LW_DI int trace_run(const DevScene &S, const DevParams &P, TraceState &ts, V3 o,
         for (;;) {
             if (budget != 0u && n >= budget) return 0;
             n++;
-            int r = visit<RUNS>(S, P, ts, o, d, R, bc, model);
+            int r = visit<RUNS>(S, P, ts, o, d, R, bc, model, A);
             if (r < 0) return -1;
             if (r > 0) break;
         }
-        if (test_cell(S, P, ts, o, d, tmin, model, bc.ov, out)) return 1;
-        if (!dda_advance(ts.s, o, ts.inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end)) return -1;
+        if (test_cell<REB>(S, P, ts, o, d, tmin, model, bc.ov, out, A)) return 1;
+        if (!dda_advance(ts.s, o, ts.inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end, A)) return -1;
     }
 }
 
@@ -459,8 +525,9 @@ LW_DI int trace_run(const DevScene &S, const DevParams &P, TraceState &ts, V3 o,
 // for this warp). Each owner then takes its own quads' candidates in quad order under trace's
 // acceptance rule (reach_of), exactly as the sequential loop of test_cell would, and tests its
 // cell's overlay quads, if any, after them. Returns true with the closest hit in `out`.
+template <bool REB = false>
 LW_DI bool warp_test_cells(const DevScene &S, const DevParams &P, const TraceState &ts, V3 o, V3 d, float tmin,
-                           bool pending, uint32_t model, uint32_t ov, Hit &out, float4 *sq) {
+                           bool pending, uint32_t model, uint32_t ov, Hit &out, float4 *sq, const Frame &A = Frame{}) {
     const unsigned FULL = 0xFFFFFFFFu;
     const uint32_t lane = threadIdx.x & 31u;
     const Dda &s = ts.s;
@@ -497,8 +564,8 @@ LW_DI bool warp_test_cells(const DevScene &S, const DevParams &P, const TraceSta
         // the owner's origin relative to its cell, formed here from its origin and cell (fewer
         // registers live across the loop than keeping it in the owner)
         const V3 olo = v3(__shfl_sync(FULL, o.x, L), __shfl_sync(FULL, o.y, L), __shfl_sync(FULL, o.z, L)) -
-                       v3((float)__shfl_sync(FULL, s.c0, L), (float)__shfl_sync(FULL, s.c1, L),
-                          (float)__shfl_sync(FULL, s.c2, L));
+                       v3((float)__shfl_sync(FULL, s.c0 - A.x(), L), (float)__shfl_sync(FULL, s.c1 - A.y(), L),
+                          (float)__shfl_sync(FULL, s.c2 - A.z(), L));
         const V3 od = v3(__shfl_sync(FULL, d.x, L), __shfl_sync(FULL, d.y, L), __shfl_sync(FULL, d.z, L));
         const float otlo = __shfl_sync(FULL, t_lo, L);
         const uint32_t oq = __shfl_sync(FULL, qbase, L) + (k - __shfl_sync(FULL, pre, L));
@@ -523,16 +590,7 @@ LW_DI bool warp_test_cells(const DevScene &S, const DevParams &P, const TraceSta
         }
         __syncwarp();
     }
-    if (pending && ov != EMPTY) {
-        uint32_t local = (uint32_t)((((s.c1 & 15) * 16 + (s.c2 & 15)) * 16) + (s.c0 & 15));
-        size_t b = (size_t)P.off.w + (size_t)ov * OV_CELL_WORDS + local * 2u;
-        uint32_t off = ldg(S.grid + b);
-        uint32_t count = ldg(S.grid + b + 1);
-        for (uint32_t i = 0; i < count; i++) {
-            uint32_t qi = ldg(S.grid + (size_t)P.off2.x + off + i);
-            test_quad(S, P, qi, o, d, t_lo, best);
-        }
-    }
+    if (pending && ov != EMPTY) test_overlay<REB>(S, P, s, ov, o, REB ? cell_origin(o, s, A) : o, d, t_lo, best);
     if (!pending || best.quad == NO_QUAD) return false;
     out = best;
     return true;
@@ -544,9 +602,9 @@ LW_DI bool warp_test_cells(const DevScene &S, const DevParams &P, const TraceSta
 // cells the lanes reached, so a warp runs one phase of quad tests per round, spread over its 32
 // lanes. Returns as trace_run does (1 hit, -1 no hit, 0 the round ended first); after 0 the next
 // round continues from `ts`. The visits and quad tests are trace_run's, in the same order.
-template <bool STAGED = false>
+template <bool STAGED = false, bool REB = false>
 LW_DI int trace_round_warp(const DevScene &S, const DevParams &P, TraceState &ts, V3 o, V3 d, float tmin,
-                           uint32_t budget, bool have, Hit &out, float4 *sq) {
+                           uint32_t budget, bool have, Hit &out, float4 *sq, const Frame &A = Frame{}) {
     const RayDda R = ray_dda(P, d);
     BrickCache bc = no_brick();
     uint32_t model = 0;
@@ -554,15 +612,15 @@ LW_DI int trace_round_warp(const DevScene &S, const DevParams &P, TraceState &ts
     if (have) {
         uint32_t more = budget - 1u;  // visits left in this round after the next one
         for (;;) {
-            r = visit<true, STAGED>(S, P, ts, o, d, R, bc, model);
+            r = visit<true, STAGED>(S, P, ts, o, d, R, bc, model, A);
             if (r != 0 || more == 0u) break;
             more--;
         }
     }
     const bool pending = have && r > 0;
     if (__any_sync(0xFFFFFFFFu, pending)) {
-        const bool hit = warp_test_cells(S, P, ts, o, d, tmin, pending, model, bc.ov, out, sq);
-        if (pending) r = hit ? 1 : (dda_advance(ts.s, o, ts.inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end) ? 0 : -1);
+        const bool hit = warp_test_cells<REB>(S, P, ts, o, d, tmin, pending, model, bc.ov, out, sq, A);
+        if (pending) r = hit ? 1 : (dda_advance(ts.s, o, ts.inv, R.s0, R.s1, R.s2, R.gs0, R.gs1, R.gs2, ts.t_end, A) ? 0 : -1);
     }
     return have ? r : 0;
 }
@@ -570,12 +628,13 @@ LW_DI int trace_round_warp(const DevScene &S, const DevParams &P, TraceState &ts
 // trace (trace.rs:137-290): the closest hit along o + t d, t in (tmin, tmax), in one go.
 // RUNS: whether a visit steps a whole run of empty bricks (the adjoint's kernels, whose registers
 // are bounded tighter, run 10 % faster with one brick per visit).
-template <bool RUNS = true>
-LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, float tmax) {
+// REB: o is in frame A (chunk-origin rebasing).
+template <bool RUNS = true, bool REB = false>
+LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, float tmax, const Frame &A = Frame{}) {
     TraceState ts;
-    if (!trace_begin(ts, P, o, d, tmax)) return no_hit();
+    if (!trace_begin(ts, P, o, d, tmax, A)) return no_hit();
     Hit h;
-    if (trace_run<RUNS>(S, P, ts, o, d, tmin, 0u, h) == 1) return h;
+    if (trace_run<RUNS, REB>(S, P, ts, o, d, tmin, 0u, h, A) == 1) return h;
     return no_hit();
 }
 
@@ -583,9 +642,14 @@ LW_DI Hit trace(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, f
 LW_DI bool is_see_through(const DevParams &P, uint32_t qi) {
     return qi >= P.see_through.x && qi - P.see_through.x < P.see_through.y;
 }
-LW_COLD Hit see_through_hit(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin) {
+// REB: o in frame A, the quads' p0 taken relative to A.
+template <bool REB = false>
+LW_COLD Hit see_through_hit(const DevScene &S, const DevParams &P, V3 o, V3 d, float tmin, const Frame &A = Frame{}) {
     Hit best = no_hit();
-    for (uint32_t i = 0; i < P.see_through.y; i++) test_quad(S, P, P.see_through.x + i, o, d, tmin, best);
+    for (uint32_t i = 0; i < P.see_through.y; i++) {
+        if (REB) test_quad<true>(S, P, P.see_through.x + i, o, d, tmin, best, frame_origin(A));
+        else test_quad(S, P, P.see_through.x + i, o, d, tmin, best);
+    }
     return best;
 }
 

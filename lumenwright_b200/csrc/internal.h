@@ -97,6 +97,7 @@ struct WfState {
     uint32_t *ctr;    // per queue set s: [4s] its length, [4s + 1] the trace fetch counter; [12]: the
                       // iteration; [14..15]: rays traced (64-bit, 8-byte aligned)
     float4 *ts;       // 3 float4 per slot (word k at ts[k * n + i]): a carried-over traversal
+    uint32_t *frame;  // per slot: the frame word of its path (chunk-origin rebasing only)
 };
 // Visits through empty space per round of the wavefront's tracing kernel when the tuning leaves it
 // at 0 (5: +1 % over 4 at c2 and c4; 6 gives the same).

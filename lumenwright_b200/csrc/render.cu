@@ -27,8 +27,9 @@ __device__ unsigned long long g_stats[16];
 // lane's ray by at most `W.budget` voxel visits instead (the regrouping period): a lane whose ray
 // ends shades it and sets up its next ray, a lane whose ray is still on its way keeps it for the
 // next iteration, so no lane waits longer than one budget for the longest traversal of its warp;
-// the price is the traversal state kept live across iterations (more registers).
-template <int MODE, int THREADS, bool RESUME>
+// the price is the traversal state kept live across iterations (more registers). REB: chunk-origin
+// rebasing (the path's positions in the frame of p.frame).
+template <int MODE, int THREADS, bool RESUME, bool REB = false>
 __global__ void __launch_bounds__(THREADS, THREADS == 128 ? LW_MIN_BLOCKS : (THREADS == 64 ? 2 * LW_MIN_BLOCKS : 2))
 k_render(const DevScene S, const DevParams P, const WorkDesc W) {
     const uint32_t lane = threadIdx.x & 31u;
@@ -68,7 +69,7 @@ k_render(const DevScene S, const DevParams P, const WorkDesc W) {
                         sample = W.sample_start + j * W.sub;
                         s_end = min(sample + W.sub, W.sample_start + W.spp);
                         s0 = s1 = s2 = c0 = c1 = c2 = 0.0f;
-                        begin_sample(p, P, px, py, sample);
+                        begin_sample<REB>(p, P, px, py, sample);
                         active = true;
                         tracing = false;
                     }
@@ -91,12 +92,13 @@ k_render(const DevScene S, const DevParams P, const WorkDesc W) {
         int r = -1;
         if (!RESUME) {
             // The whole traversal at once: nothing of it lives on past this iteration.
-            h = trace(S, P, p.o, p.d, p.tmin, p.tmax);
+            h = trace<true, REB>(S, P, p.o, p.d, p.tmin, p.tmax, REB ? frame_of(p.frame) : Frame{});
             r = h.quad != NO_QUAD ? 1 : -1;
         } else {
-        if (!tracing) tracing = trace_begin(ts, P, p.o, p.d, p.tmax);
+        const Frame A = REB ? frame_of(p.frame) : Frame{};
+        if (!tracing) tracing = trace_begin(ts, P, p.o, p.d, p.tmax, A);
         if (tracing) {
-            r = trace_run(S, P, ts, p.o, p.d, p.tmin, W.budget, h);
+            r = trace_run<true, REB>(S, P, ts, p.o, p.d, p.tmin, W.budget, h, A);
 #if LW_STATS
             {
                 unsigned am = __activemask();
@@ -126,7 +128,7 @@ k_render(const DevScene S, const DevParams P, const WorkDesc W) {
             }
         }
 #endif
-        Act a = shade(p, S, P, h);
+        Act a = shade<REB>(p, S, P, h);
         if (a == A_END) {
             if (MODE == MODE_SAMPLES) {
                 size_t at = ((size_t)((py - W.y0) * W.w + (px - W.x0)) * W.spp + (sample - W.sample_start)) * 3u;
@@ -140,7 +142,7 @@ k_render(const DevScene S, const DevParams P, const WorkDesc W) {
             }
             sample++;
             if (sample < s_end) {
-                begin_sample(p, P, px, py, sample);
+                begin_sample<REB>(p, P, px, py, sample);
             } else {
                 if (MODE == MODE_ACCUM) W.partials[(size_t)j * W.n_slots + slot] = make_float4(s0 - c0, s1 - c1, s2 - c2, 0.0f);
                 active = false;
@@ -228,8 +230,10 @@ static const void *kernel_for_r(int threads) {
     if (threads == 256) return (const void *)k_render<MODE, 256, RESUME>;
     return (const void *)k_render<MODE, 128, RESUME>;
 }
+// With chunk-origin rebasing one form: 128 threads, whole traversals.
 template <int MODE>
-static const void *kernel_for(int threads, bool resume = false) {
+static const void *kernel_for(int threads, bool resume = false, bool reb = false) {
+    if (reb) return (const void *)k_render<MODE, 128, false, true>;
     return resume ? kernel_for_r<MODE, true>(threads) : kernel_for_r<MODE, false>(threads);
 }
 
@@ -247,9 +251,15 @@ cudaError_t launch_render(int mode, const DevScene &S, const DevParams &P, const
                           cudaStream_t st) {
     void *args[] = {(void *)&S, (void *)&P, (void *)&W};
     const bool resume = W.budget != 0u;
-    const void *k = mode == MODE_SAMPLES ? kernel_for<MODE_SAMPLES>(shape.threads, resume)
-                                         : kernel_for<MODE_ACCUM>(shape.threads, resume);
-    return cudaLaunchKernel(k, dim3(shape.blocks), dim3(shape.threads), args, 0, st);
+    const bool reb = rebased(P);
+    LaunchShape sh = shape;
+    if (reb && sh.threads != 128) {  // the same threads in blocks of 128 (the kernel is persistent)
+        sh.blocks = sh.blocks * sh.threads / 128 > 0 ? sh.blocks * sh.threads / 128 : 1;
+        sh.threads = 128;
+    }
+    const void *k = mode == MODE_SAMPLES ? kernel_for<MODE_SAMPLES>(sh.threads, resume, reb)
+                                         : kernel_for<MODE_ACCUM>(sh.threads, resume, reb);
+    return cudaLaunchKernel(k, dim3(sh.blocks), dim3(sh.threads), args, 0, st);
 }
 
 cudaError_t launch_reduce(const WorkDesc &W, Accum *acc, uint32_t frame_w, cudaStream_t st) {

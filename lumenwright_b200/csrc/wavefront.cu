@@ -167,8 +167,9 @@ LW_DI ItemRef decode_item(const WorkDesc &W, const BatchDesc &B, uint32_t item) 
 
 // One shading step of slot i (none when valid is false); its next ray goes to queue set `cur`.
 // Slots with nothing to shade (dead, or their ray still being traced) leave after the state
-// machine rather than before it, so the kernel has one exit.
-template <bool BATCH>
+// machine rather than before it, so the kernel has one exit. REB: chunk-origin rebasing, the
+// path's frame word in F.frame.
+template <bool BATCH, bool REB = false>
 LW_DI void shade_slot(bool valid, uint32_t i, const DevScene &S0, const DevParams &P0, const WorkDesc &W,
                       const BatchDesc &B, const WfState &F, uint32_t cur) {
     float4 core = valid ? ld(F, W_CORE, i) : u4(0u, 0u, 0u, F_DEAD);
@@ -193,13 +194,14 @@ LW_DI void shade_slot(bool valid, uint32_t i, const DevScene &S0, const DevParam
             float4 wo = ld(F, W_O, i), wd = ld(F, W_D, i), wr = ld(F, W_RAD, i), wb = ld(F, W_BETA, i);
             float h1 = F.hit1[i];
             unpack_core(p, wo, wd, wr, wb, core);
+            if (REB) p.frame = F.frame[i];
             if (p.kind != K_EXTEND) load_nee(F, i, p);
             Hit h{h0.x, fu(h0.y), fu(h0.z), h0.w, h1};
-            a = on_result(p, S, P, h, val);
+            a = on_result<REB>(p, S, P, h, val);
             part = true;
         }
     }
-    if (part) a = advance(p, S, P, a, val);
+    if (part) a = advance<REB>(p, S, P, a, val);
     if (!live) return;
     if (a == A_END) {
         // The sample is over: the item's sums, then its next sample or the next item.
@@ -251,7 +253,7 @@ LW_DI void shade_slot(bool valid, uint32_t i, const DevScene &S0, const DevParam
                 a = A_TRACE;
             }
         }
-        if (a == A_TRACE) begin_sample(p, BATCH ? B.jobs[job].P : P0, px, py, sample);  // one call site
+        if (a == A_TRACE) begin_sample<REB>(p, BATCH ? B.jobs[job].P : P0, px, py, sample);  // one call site
         st(F, W_ITEM, i, u4(px, py, sample, s_end));
         st(F, W_ITEM2, i, u4(j, pslot, job, 0u));
         st(F, W_SUM, i, make_float4(s0, s1, s2, c0));
@@ -260,6 +262,7 @@ LW_DI void shade_slot(bool valid, uint32_t i, const DevScene &S0, const DevParam
     if (a == A_TRACE) {
         F.queue[(size_t)cur * F.n + ticket(&F.ctr[4 * cur])] = i;
         store_core(F, i, p, flags);
+        if (REB) F.frame[i] = p.frame;
         if (p.kind != K_EXTEND) store_nee(F, i, p);
     } else {
         st(F, W_CORE, i, u4(0u, 0u, 0u, flags));
@@ -280,10 +283,9 @@ LW_DI void shade_slot(bool valid, uint32_t i, const DevScene &S0, const DevParam
 #ifndef LW_WF_SHADE_MINB_BATCH
 #define LW_WF_SHADE_MINB_BATCH 6
 #endif
-template <bool BATCH>
+template <bool BATCH, bool REB = false>
 __global__ void __launch_bounds__(kShadeThreads, (BATCH ? LW_WF_SHADE_MINB_BATCH : LW_WF_SHADE_MINB) * 128 / kShadeThreads)
-k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
-                                                  const BatchDesc B, const WfState F) {
+k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W, const BatchDesc B, const WfState F) {
     const uint32_t t = *(volatile uint32_t *)&F.ctr[12];
     const uint32_t cur = t % 3u, prev = (t + 2u) % 3u, next = (t + 1u) % 3u;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
@@ -298,7 +300,7 @@ k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W,
     const uint32_t n = dense ? F.n : queued;
     const uint32_t *list = F.queue + (size_t)prev * F.n;
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;  // the grid covers every slot
-    shade_slot<BATCH>(k < n, k < n ? (dense ? k : list[k]) : 0u, S0, P0, W, B, F, cur);
+    shade_slot<BATCH, REB>(k < n, k < n ? (dense ? k : list[k]) : 0u, S0, P0, W, B, F, cur);
 }
 
 // The end of an iteration: the next iteration's number; in a graph, whether to run another one (the
@@ -328,8 +330,8 @@ __global__ void k_wf_advance_graph(const WfState F, cudaGraphConditionalHandle l
 // to the next iteration's queue, so an iteration does not wait for its single longest ray.
 // STAGED: the block first copies the scene's top level and occupancy masks (S0.n_top + S0.n_occ
 // entries of 8 bytes, the dynamic shared memory of the launch) into shared memory and reads them
-// there.
-template <bool STAGED>
+// there. REB: chunk-origin rebasing, each ray in the frame of its slot's frame word.
+template <bool STAGED, bool REB = false>
 __global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(const DevScene S0, const DevParams P, const WfState F,
                                                                       uint32_t budget, uint32_t tail) {
     extern __shared__ uint2 s_scene[];
@@ -351,6 +353,7 @@ __global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(co
     const uint32_t *list = F.queue + (size_t)cur * F.n;
     TraceState ts;
     V3 o = v3(0.0f, 0.0f, 0.0f), d = o;
+    Frame A = Frame{};
     float tmin = 0.0f;
     uint32_t slot = 0, rounds = 0;
     bool have = false, done = false;
@@ -391,6 +394,7 @@ __global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(co
                     o = f4v(a);
                     tmin = a.w;
                     d = f4v(b);
+                    if (REB) A = frame_of(F.frame[slot]);
                     if (fu(F.hit0[slot].y) == RESUME_MARK) {
                         // a ray carried over from the previous iteration
                         float4 t0 = F.ts[slot], t1 = F.ts[F.n + slot], t2 = F.ts[2 * (size_t)F.n + slot];
@@ -405,7 +409,7 @@ __global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(co
                         ts.t_end = t2.z;
                         ts.it = fu(t2.w);
                         have = true;
-                    } else if (trace_begin(ts, P, o, d, b.w)) {
+                    } else if (trace_begin(ts, P, o, d, b.w, A)) {
                         have = true;
                     } else {
                         F.hit0[slot] = make_float4(kINF, __uint_as_float(NO_QUAD), 0.0f, 0.0f);
@@ -417,7 +421,7 @@ __global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(co
         if (__all_sync(FULL, done && !have)) break;
         if (__any_sync(FULL, done)) rounds++;  // the queue is dry: count the tail rounds
         Hit h = no_hit();
-        const int r = trace_round_warp<STAGED>(S, P, ts, o, d, tmin, budget, have, h, s_quads[threadIdx.x >> 5]);
+        const int r = trace_round_warp<STAGED, REB>(S, P, ts, o, d, tmin, budget, have, h, s_quads[threadIdx.x >> 5], A);
         if (have) {
             if (r != 0) {
                 if (r != 1) h = no_hit();
@@ -449,7 +453,8 @@ LaunchShape wf_trace_shape(int device, size_t stage_bytes) {
 cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, uint32_t blocks,
                             cudaStream_t st) {
     BatchDesc none{};
-    k_wf_shade<false><<<blocks, kShadeThreads, 0, st>>>(S, P, W, none, F);
+    if (rebased(P)) k_wf_shade<false, true><<<blocks, kShadeThreads, 0, st>>>(S, P, W, none, F);
+    else k_wf_shade<false><<<blocks, kShadeThreads, 0, st>>>(S, P, W, none, F);
     return cudaGetLastError();
 }
 
@@ -463,7 +468,9 @@ cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const 
 cudaError_t launch_wf_trace(const DevScene &S, const DevParams &P, const WfState &F, LaunchShape trace_shape,
                             uint32_t budget, uint32_t tail, size_t stage_bytes, cudaStream_t st) {
     if (budget == 0u) budget = kWfBudget;  // a round makes at least one visit
-    if (stage_bytes)
+    if (rebased(P))  // one form: unstaged
+        k_wf_trace<false, true><<<trace_shape.blocks, trace_shape.threads, 0, st>>>(S, P, F, budget, tail);
+    else if (stage_bytes)
         k_wf_trace<true><<<trace_shape.blocks, trace_shape.threads, stage_bytes, st>>>(S, P, F, budget, tail);
     else
         k_wf_trace<false><<<trace_shape.blocks, trace_shape.threads, 0, st>>>(S, P, F, budget, tail);

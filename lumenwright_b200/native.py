@@ -32,7 +32,7 @@ EXPORTS = (
     "lw_batch_run", "lw_batch_read", "lw_render_batch", "lw_adjoint_forward", "lw_adjoint_backward", "lw_adjoint_fd",
     "lw_gamma_table", "lw_tonemap_rgba", "lw_read_accumulator_rgba", "lw_scene_build_keys", "lw_scene_build_grid",
     "lw_scene_read", "lw_water_exp", "lw_draw_sky_map", "lw_set_timeout", "lw_render_device_shard",
-    "lw_accumulator_device",
+    "lw_accumulator_device", "lw_rebase_camera",
 )
 
 # lw_tonemap operators (post.rs `Tonemap`)
@@ -179,6 +179,7 @@ def load(path: str = LIB_PATH):
     L.lw_adjoint_backward.argtypes = [P, C.POINTER(AdjFrame), C.c_uint32, P, C.POINTER(Gradient)]
     L.lw_adjoint_fd.argtypes = [P, C.POINTER(AdjFrame), C.POINTER(AdjFrame), C.POINTER(AdjFrame), C.c_uint32, P, P]
     L.lw_gamma_table.argtypes = [P]
+    L.lw_rebase_camera.argtypes = [P, C.POINTER(C.c_double)]
     L.lw_tonemap_rgba.argtypes = [P, P, C.c_uint64, C.POINTER(ToneMap), P]
     L.lw_scene_build_keys.argtypes = [P, C.POINTER(WorldDesc), P, C.c_uint32, C.POINTER(C.c_uint32)]
     L.lw_scene_build_grid.argtypes = [P, C.POINTER(WorldDesc), C.POINTER(InstancesDesc), C.POINTER(BuildInfo)]
@@ -202,6 +203,19 @@ def gamma_table() -> np.ndarray:
     if st:
         raise LwError(st, "lw_gamma_table")
     return out
+
+
+def rebase_camera(params: np.ndarray, eye64) -> np.ndarray:
+    """Chunk-origin rebasing of a frame's camera (`lw_rebase_camera`, on the host in f64): a copy
+    of ``params`` whose ``cam_pos.xyz`` is the eye relative to the chunk corner nearest it and whose
+    ``see_through[2:4]`` switch the kernels to chunk frames from that corner. ``eye64`` is the eye
+    relative to the grid origin, in f64 (request.rs:640-644 rebases it from the world)."""
+    p = np.array(params, copy=True)
+    e = (C.c_double * 3)(*[float(v) for v in eye64])
+    st = load().lw_rebase_camera(p.ctypes.data, e)
+    if st:
+        raise LwError(st, f"lw_rebase_camera: eye {tuple(eye64)}")
+    return p
 
 
 class Context:

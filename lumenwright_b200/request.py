@@ -190,3 +190,15 @@ def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None)
     cfg.notes.update(dict(weight=float(weight), emitter_intensity=float(intensity), stats=vars(hq.stats),
                           emitters=world.emitters_placed, solid=world.solid_blocks))
     return HqFrame(scene=hq, params=p, spp=spp, sky=sky, eye64=eye64)
+
+
+def with_chunk_frames(frame: HqFrame) -> HqFrame:
+    """The same frame rendered with chunk-origin rebasing (the precision form's option): the eye,
+    relative to the grid origin in f64, split by `lw_rebase_camera` into the chunk corner nearest
+    it and an f32 remainder of at most 8 blocks per axis; the kernels then hold every path origin
+    relative to its own nearest chunk corner. The scene, sky and random streams are unchanged."""
+    from .native import rebase_camera
+    if frame.eye64 is None:
+        raise ValueError("chunk frames need the frame's f64 eye")
+    return HqFrame(scene=frame.scene, params=rebase_camera(frame.params, frame.eye64), spp=frame.spp, sky=frame.sky,
+                   eye64=frame.eye64)

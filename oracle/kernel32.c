@@ -107,7 +107,8 @@ static lwo_hit to_pub(Hit h) {
     return r;
 }
 static Cam params_cam(const lwo_params *p) {
-    Cam c = {v3f4(p->cam_pos), v3f4(p->cam_fwd), v3f4(p->cam_right), v3f4(p->cam_up), p->cam_pos[3], p->cam_fwd[3]};
+    Cam c = {v3f4(p->cam_pos), v3f4(p->cam_fwd), v3f4(p->cam_right), v3f4(p->cam_up), p->cam_pos[3], p->cam_fwd[3],
+             p->see_through[2], p->see_through[3]};
     return c;
 }
 
@@ -136,6 +137,13 @@ void lwo32_render_sample(const lwo_scene *s, uint32_t px, uint32_t py, uint32_t 
 void lwo32_sample_emitters(const lwo_scene *s, const float pos[3], const float origin[3], const float n[3],
                            uint32_t *rng_state, float out[3]) {
     v3o(sample_emitters(s, v3a(pos), v3a(origin), v3a(n), rng_state), out);
+}
+void lwo32_rebase(float x[3], uint32_t *word) {
+    frame_unpack(*word, lwo_fa);
+    v3o(rebase(v3a(x)), x);
+    *word = ((uint32_t)(lwo_fa[0] >> 4) & 0x7FFu) | (((uint32_t)(lwo_fa[1] >> 4) & 0x3FFu) << 11) |
+            (((uint32_t)(lwo_fa[2] >> 4) & 0x7FFu) << 21);
+    lwo_fa[0] = lwo_fa[1] = lwo_fa[2] = 0;
 }
 void lwo32_emitter_cell(const lwo_scene *s, const float p[3], uint32_t *start, uint32_t *count) {
     emitter_cell(s, v3a(p), start, count);

@@ -32,11 +32,13 @@ static inline void d_sin_cos_turns(double u, double *s, double *c) {
 static Cam cam64(const lwo_scene *s, const lwo_camera64 *c) {
     if (!c) {
         const lwo_params *p = s->params;
-        Cam r = {v3f4(p->cam_pos), v3f4(p->cam_fwd), v3f4(p->cam_right), v3f4(p->cam_up), p->cam_pos[3], p->cam_fwd[3]};
+        Cam r = {v3f4(p->cam_pos), v3f4(p->cam_fwd), v3f4(p->cam_right), v3f4(p->cam_up), p->cam_pos[3], p->cam_fwd[3],
+                 p->see_through[2], p->see_through[3]};
         return r;
     }
+    /* the f64 camera's eye is relative to the grid origin: the grid's frame */
     Cam r = {v3(c->eye[0], c->eye[1], c->eye[2]), v3(c->fwd[0], c->fwd[1], c->fwd[2]),
-             v3(c->right[0], c->right[1], c->right[2]), v3(c->up[0], c->up[1], c->up[2]), c->tan_half, c->aspect};
+             v3(c->right[0], c->right[1], c->right[2]), v3(c->up[0], c->up[1], c->up[2]), c->tan_half, c->aspect, 0u, 0u};
     return r;
 }
 
@@ -47,6 +49,22 @@ void lwo64_render_sample(const lwo_scene *s, const lwo_camera64 *cam, uint32_t p
     out[0] = r.x;
     out[1] = r.y;
     out[2] = r.z;
+}
+
+void lwo64_render_samples(const lwo_scene *s, const lwo_camera64 *cam, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                          uint32_t sample_start, uint32_t count, double *out, int threads) {
+    Cam c = cam64(s, cam);
+    if (threads <= 0) threads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+    for (uint32_t py = 0; py < h; py++)
+        for (uint32_t px = 0; px < w; px++)
+            for (uint32_t k = 0; k < count; k++) {
+                V3 r = render_sample(s, &c, x0 + px, y0 + py, sample_start + k);
+                double *o = out + ((uint64_t)(py * w + px) * count + k) * 3u;
+                o[0] = r.x;
+                o[1] = r.y;
+                o[2] = r.z;
+            }
 }
 
 void lwo64_render_mean(const lwo_scene *s, const lwo_camera64 *cam, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,

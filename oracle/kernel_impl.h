@@ -228,14 +228,50 @@ static inline Hit no_hit(void) {
     return h;
 }
 
-/* intersect_quad (trace.rs:37-58). Returns 1 and (t, s, tt) on a hit. */
+/* ---- chunk-origin frames (the library's precision option; the reference has none) -------- */
+/* With Params.see_through[2] = 1 the library holds a path's positions relative to a chunk corner
+ * A of the grid (a multiple of 16 blocks per axis), the corner nearest the path's current origin,
+ * starting from the camera's corner packed in see_through[3] (chunk indices, two's complement: x in
+ * bits 0-10, y in 11-20, z in 21-31); the grid's cell c is the frame's integer c - A. Restated from
+ * the library's kernels (csrc/device_scene.cuh `Frame`, `rebase`). The sample being rendered sets
+ * the frame here, per thread; every other entry point runs in the grid's frame (A = 0). */
+static __thread int lwo_reb;
+static __thread int32_t lwo_fa[3];
+static inline void frame_unpack(uint32_t w, int32_t a[3]) {
+    a[0] = ((int32_t)(w << 21) >> 21) * 16;
+    a[1] = ((int32_t)(w << 11) >> 22) * 16;
+    a[2] = ((int32_t)w >> 21) * 16;
+}
+static inline V3 frame_origin(const int32_t a[3]) { return v3((REAL)a[0], (REAL)a[1], (REAL)a[2]); }
+/* rint(x / 16), kept within +-4096 (NaN to -4096). */
+static inline int32_t chunk_step(REAL x) {
+    double r = rint((double)(x * K(0.0625)));
+    if (!(r >= -4096.0)) r = -4096.0;
+    if (r > 4096.0) r = 4096.0;
+    return (int32_t)r;
+}
+/* x (in the current frame) moved to the frame of the chunk corner nearest it, which becomes the
+ * current frame: k = rint(x / 16) chunks per axis (the frame within the packable chunk range),
+ * x - 16 k, exactly (16 k and x are multiples of x's ulp, and |x - 16 k| <= |x| when k != 0). */
+static inline V3 rebase(V3 x) {
+    const int32_t c[3] = {lwo_fa[0] >> 4, lwo_fa[1] >> 4, lwo_fa[2] >> 4};
+    const int32_t n[3] = {clamp_i32(c[0] + chunk_step(x.x), -1024, 1023), clamp_i32(c[1] + chunk_step(x.y), -512, 511),
+                          clamp_i32(c[2] + chunk_step(x.z), -1024, 1023)};
+    V3 r = v3(x.x - (REAL)((n[0] - c[0]) * 16), x.y - (REAL)((n[1] - c[1]) * 16), x.z - (REAL)((n[2] - c[2]) * 16));
+    for (int a = 0; a < 3; a++) lwo_fa[a] = n[a] * 16;
+    return r;
+}
+
+/* intersect_quad (trace.rs:37-58). Returns 1 and (t, s, tt) on a hit. With `pb` the quad's p0 is
+ * taken relative to *pb (a quad given in grid coordinates, a ray in a chunk frame). */
 static inline int intersect_quad(const lwo_quad *q, V3 o, V3 d, REAL tmin, REAL tmax, REAL *pt,
-                                 REAL *ps, REAL *ptt) {
+                                 REAL *ps, REAL *ptt, const V3 *pb) {
     V3 eu = q_eu(q), ev = q_ev(q);
     V3 n = vcross(eu, ev);
     REAL denom = vdot(n, d);
     if (rabs(denom) < K(1e-12)) return 0;
     V3 p0 = q_origin(q);
+    if (pb) p0 = vsub(p0, *pb);
     REAL t = vdot(n, vsub(p0, o)) / denom;
     if (!(t > tmin && t < tmax)) return 0;
     V3 p = vsub(vadd(o, vmuls(d, t)), p0);
@@ -274,12 +310,12 @@ static inline uint64_t quad_texel_index(const lwo_scene *s, const lwo_quad *q, R
 #define COPLANAR K(1e-5) /* trace.rs:73 */
 
 /* test_quad (trace.rs:81-109). */
-static inline void test_quad(const lwo_scene *s, uint32_t qi, V3 o, V3 d, REAL tmin, Hit *best) {
+static inline void test_quad(const lwo_scene *s, uint32_t qi, V3 o, V3 d, REAL tmin, Hit *best, const V3 *pb) {
     const lwo_quad *q = QUAD(s, qi);
     CNT(quad_tests);
     REAL reach = (best->quad != NO_QUAD && qi > best->quad) ? best->t + COPLANAR : best->t;
     REAL t, ss, tt;
-    if (intersect_quad(q, o, d, tmin, reach, &t, &ss, &tt)) {
+    if (intersect_quad(q, o, d, tmin, reach, &t, &ss, &tt, pb)) {
         if ((q_flags(q) & FLAG_FRONT_ONLY) && vdot(q_normal(q), d) >= K(0.0)) return;
         uint32_t tx = quad_texel(s, q, ss, tt);
         uint32_t alpha = tx >> 24;
@@ -299,11 +335,12 @@ static inline int is_see_through(const lwo_scene *s, uint32_t qi) {
     return qi >= st[0] && qi - st[0] < st[1];
 }
 
-/* see_through_hit (trace.rs:120-131). */
+/* see_through_hit (trace.rs:120-131); in a chunk frame the quads' p0 relative to its origin. */
 static Hit see_through_hit(const lwo_scene *s, V3 o, V3 d, REAL tmin) {
     const uint32_t *st = s->params->see_through;
     Hit best = no_hit();
-    for (uint32_t i = 0; i < st[1]; i++) test_quad(s, st[0] + i, o, d, tmin, &best);
+    V3 fo = frame_origin(lwo_fa);
+    for (uint32_t i = 0; i < st[1]; i++) test_quad(s, st[0] + i, o, d, tmin, &best, lwo_reb ? &fo : NULL);
     return best;
 }
 
@@ -312,22 +349,26 @@ static inline REAL safe_inv(REAL x) { /* trace.rs:293-299 */
     return K(1.0) / x;
 }
 static inline int32_t sgn(REAL x) { return x > K(0.0) ? 1 : (x < K(0.0) ? -1 : 0); }
-static inline REAL next_boundary(REAL o, REAL inv, int32_t cell, int32_t step) { /* :313-319 */
+/* `a`: the frame's origin on this axis (grid cell c's boundary is at c - a in the frame). */
+static inline REAL next_boundary(REAL o, REAL inv, int32_t cell, int32_t step, int32_t a) { /* :313-319 */
     if (step == 0) return (REAL)INFINITY;
-    REAL bound = (REAL)(step > 0 ? cell + 1 : cell);
+    REAL bound = (REAL)((step > 0 ? cell + 1 : cell) - a);
     return (bound - o) * inv;
 }
 
-/* trace (trace.rs:137-290). */
+/* trace (trace.rs:137-290), with o in the current frame: the grid spans [-A, size - A) there. */
 static Hit trace(const lwo_scene *s, V3 o, V3 d, REAL tmin, REAL tmax) {
     const lwo_params *p = s->params;
     const uint32_t *dims = p->grid_dims;
-    V3 size = grid_size(s);
+    const int32_t A[3] = {lwo_reb ? lwo_fa[0] : 0, lwo_reb ? lwo_fa[1] : 0, lwo_reb ? lwo_fa[2] : 0};
+    V3 lo = v3((REAL)(-A[0]), (REAL)(-A[1]), (REAL)(-A[2]));
+    V3 hi = v3((REAL)((int32_t)(dims[0] * 16u) - A[0]), (REAL)((int32_t)(dims[1] * 16u) - A[1]),
+               (REAL)((int32_t)(dims[2] * 16u) - A[2]));
     CNT(traces);
 
     V3 inv = v3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
-    V3 ta = vmul(vsub(V3_ZERO, o), inv);
-    V3 tb = vmul(vsub(size, o), inv);
+    V3 ta = vmul(vsub(lo, o), inv);
+    V3 tb = vmul(vsub(hi, o), inv);
     REAL t_enter = rmax(rmax(rmin(ta.x, tb.x), rmin(ta.y, tb.y)), rmin(ta.z, tb.z));
     REAL t_exit = rmin(rmin(rmax(ta.x, tb.x), rmax(ta.y, tb.y)), rmax(ta.z, tb.z));
     REAL t = rmax(t_enter, K(0.0));
@@ -336,12 +377,12 @@ static Hit trace(const lwo_scene *s, V3 o, V3 d, REAL tmin, REAL tmax) {
 
     V3 start = vadd(o, vmuls(d, t + K(1e-4)));
     int32_t gs[3] = {(int32_t)dims[0] * 16, (int32_t)dims[1] * 16, (int32_t)dims[2] * 16};
-    int32_t cell[3] = {clamp_i32(to_i32(R_FLOOR(start.x)), 0, gs[0] - 1),
-                       clamp_i32(to_i32(R_FLOOR(start.y)), 0, gs[1] - 1),
-                       clamp_i32(to_i32(R_FLOOR(start.z)), 0, gs[2] - 1)};
+    int32_t cell[3] = {clamp_i32(to_i32(R_FLOOR(start.x)) + A[0], 0, gs[0] - 1),
+                       clamp_i32(to_i32(R_FLOOR(start.y)) + A[1], 0, gs[1] - 1),
+                       clamp_i32(to_i32(R_FLOOR(start.z)) + A[2], 0, gs[2] - 1)};
     int32_t step[3] = {sgn(d.x), sgn(d.y), sgn(d.z)};
     REAL next[3];
-    for (int a = 0; a < 3; a++) next[a] = next_boundary(vget(o, a), vget(inv, a), cell[a], step[a]);
+    for (int a = 0; a < 3; a++) next[a] = next_boundary(vget(o, a), vget(inv, a), cell[a], step[a], A[a]);
 
     uint32_t top_off = p->off[0];
     uint32_t ov_top_off = p->off[2];
@@ -362,7 +403,7 @@ static Hit trace(const lwo_scene *s, V3 o, V3 d, REAL tmin, REAL tmax) {
             for (int a = 0; a < 3; a++) {
                 if (step[a] != 0) {
                     int32_t bound = step[a] > 0 ? (bc[a] + 1) * 16 : bc[a] * 16;
-                    REAL tt = ((REAL)bound - vget(o, a)) * vget(inv, a);
+                    REAL tt = ((REAL)(bound - A[a]) - vget(o, a)) * vget(inv, a);
                     if (tt < t_out) { t_out = tt; axis = a; }
                 }
             }
@@ -372,10 +413,10 @@ static Hit trace(const lwo_scene *s, V3 o, V3 d, REAL tmin, REAL tmax) {
                 if (a == axis)
                     cell[a] = step[a] > 0 ? (bc[a] + 1) * 16 : bc[a] * 16 - 1;
                 else
-                    cell[a] = clamp_i32(to_i32(R_FLOOR(vget(pos, a))), bc[a] * 16, bc[a] * 16 + 15);
+                    cell[a] = clamp_i32(to_i32(R_FLOOR(vget(pos, a))) + A[a], bc[a] * 16, bc[a] * 16 + 15);
             }
             if (cell[axis] < 0 || cell[axis] >= gs[axis]) break;
-            for (int a = 0; a < 3; a++) next[a] = next_boundary(vget(o, a), vget(inv, a), cell[a], step[a]);
+            for (int a = 0; a < 3; a++) next[a] = next_boundary(vget(o, a), vget(inv, a), cell[a], step[a], A[a]);
             t = t_out;
             continue;
         }
@@ -397,11 +438,12 @@ static Hit trace(const lwo_scene *s, V3 o, V3 d, REAL tmin, REAL tmax) {
         }
         Hit cand = no_hit();
         cand.t = rmin(t_hi, best_t);
+        /* the origin relative to the cell: o - (c - A) */
+        V3 olo = vsub(o, v3((REAL)(cell[0] - A[0]), (REAL)(cell[1] - A[1]), (REAL)(cell[2] - A[2])));
         if (model != 0) {
             lwo_model m = MODEL(s, model);
             CNT(model_fetches);
-            V3 lo = vsub(o, v3((REAL)cell[0], (REAL)cell[1], (REAL)cell[2]));
-            for (uint32_t i = 0; i < m.quad_count; i++) test_quad(s, m.quad_offset + i, lo, d, t_lo, &cand);
+            for (uint32_t i = 0; i < m.quad_count; i++) test_quad(s, m.quad_offset + i, olo, d, t_lo, &cand, NULL);
         }
         if (ov != EMPTY) {
             uint32_t local = (uint32_t)((((cell[1] & 15) * 16 + (cell[2] & 15)) * 16) + (cell[0] & 15));
@@ -409,9 +451,12 @@ static Hit trace(const lwo_scene *s, V3 o, V3 d, REAL tmin, REAL tmax) {
             uint32_t off = GRID(s, base);
             uint32_t count = GRID(s, base + 1);
             CNT(overlay_reads);
+            /* in a chunk frame relative to the cell, like a model's quads: the quads' p0 - c */
+            V3 cv = v3((REAL)cell[0], (REAL)cell[1], (REAL)cell[2]);
             for (uint32_t i = 0; i < count; i++) {
                 uint32_t qi = GRID(s, (uint64_t)(p->off2[0] + off + i));
-                test_quad(s, qi, o, d, t_lo, &cand);
+                if (lwo_reb) test_quad(s, qi, olo, d, t_lo, &cand, &cv);
+                else test_quad(s, qi, o, d, t_lo, &cand, NULL);
             }
         }
         if (cand.quad != NO_QUAD) return cand;
@@ -421,7 +466,7 @@ static Hit trace(const lwo_scene *s, V3 o, V3 d, REAL tmin, REAL tmax) {
         if (t > t_end) break;
         cell[axis] += step[axis];
         if (cell[axis] < 0 || cell[axis] >= gs[axis]) break;
-        next[axis] = next_boundary(vget(o, axis), vget(inv, axis), cell[axis], step[axis]);
+        next[axis] = next_boundary(vget(o, axis), vget(inv, axis), cell[axis], step[axis], A[axis]);
     }
     return no_hit();
 }
@@ -713,13 +758,25 @@ static inline uint32_t pick(uint32_t n, REAL u) {
     return i < n ? i : n - 1;
 }
 
-/* emitter_cell (integrator.rs:358-373). */
+/* floor(b / cell) for an integer block coordinate b and integer cell: exact for |b| < 2^24 (the
+ * quotient's rounding error stays below 1 / cell, its least distance to an integer it is not). */
+static inline int32_t cell_of_block(int32_t b, REAL cell) { return to_i32(R_FLOOR((REAL)b / cell)); }
+
+/* emitter_cell (integrator.rs:358-373). In a chunk frame the cell of p's block in the grid,
+ * floor(p) + A, in integers (floor((b + f) / size) = floor(b / size) for f in [0, 1)). */
 static void emitter_cell(const lwo_scene *s, V3 p, uint32_t *start, uint32_t *count) {
     REAL cell = (REAL)EGRID(s, 0);
     int32_t size[3] = {(int32_t)EGRID(s, 1), (int32_t)EGRID(s, 2), (int32_t)EGRID(s, 3)};
-    int32_t c[3] = {to_i32(R_FLOOR(p.x / cell)) - (int32_t)EGRID(s, 4),
-                    to_i32(R_FLOOR(p.y / cell)) - (int32_t)EGRID(s, 5),
-                    to_i32(R_FLOOR(p.z / cell)) - (int32_t)EGRID(s, 6)};
+    int32_t c[3];
+    if (lwo_reb) {
+        c[0] = cell_of_block(to_i32(R_FLOOR(p.x)) + lwo_fa[0], cell) - (int32_t)EGRID(s, 4);
+        c[1] = cell_of_block(to_i32(R_FLOOR(p.y)) + lwo_fa[1], cell) - (int32_t)EGRID(s, 5);
+        c[2] = cell_of_block(to_i32(R_FLOOR(p.z)) + lwo_fa[2], cell) - (int32_t)EGRID(s, 6);
+    } else {
+        c[0] = to_i32(R_FLOOR(p.x / cell)) - (int32_t)EGRID(s, 4);
+        c[1] = to_i32(R_FLOOR(p.y / cell)) - (int32_t)EGRID(s, 5);
+        c[2] = to_i32(R_FLOOR(p.z / cell)) - (int32_t)EGRID(s, 6);
+    }
     CNT(emitter_cell_reads);
     if (c[0] < 0 || c[1] < 0 || c[2] < 0 || c[0] >= size[0] || c[1] >= size[1] || c[2] >= size[2]) {
         *start = 0;
@@ -739,7 +796,9 @@ static V3 sample_emitter_face(const lwo_scene *s, V3 origin, V3 n, const lwo_emi
     const lwo_quad *q = QUAD(s, (uint64_t)(bits_of(e->pos[3]) + face));
     REAL ss = rng_next(rng);
     REAL t = rng_next(rng);
-    V3 at = vadd(vadd(vadd(v3f4(e->pos), q_origin(q)), vmuls(q_eu(q), ss)), vmuls(q_ev(q), t));
+    V3 epos = v3f4(e->pos);
+    if (lwo_reb) epos = vsub(epos, frame_origin(lwo_fa));  /* the block's corner in the frame: exact */
+    V3 at = vadd(vadd(vadd(epos, q_origin(q)), vmuls(q_eu(q), ss)), vmuls(q_ev(q), t));
     V3 to = vsub(at, origin);
     if (vdot(to, n) <= K(0.0)) return V3_ZERO;
     REAL dist = vlength(to);
@@ -773,10 +832,8 @@ static V3 sample_emitter(const lwo_scene *s, V3 origin, V3 n, const lwo_emitter 
     return sum;
 }
 
-/* sample_emitters (integrator.rs:441-469). */
-static V3 sample_emitters(const lwo_scene *s, V3 pos, V3 origin, V3 n, uint32_t *rng) {
-    uint32_t start, count;
-    emitter_cell(s, pos, &start, &count);
+/* sample_emitters (integrator.rs:441-469) on the emitters of a cell emitter_cell found. */
+static V3 sample_cell_emitters(const lwo_scene *s, uint32_t start, uint32_t count, V3 origin, V3 n, uint32_t *rng) {
     if (count == 0) return V3_ZERO;
     uint64_t list = (uint64_t)EMITTER_GRID_HEADER +
                     (uint64_t)EGRID(s, 1) * (uint64_t)EGRID(s, 2) * (uint64_t)EGRID(s, 3) * 2u + start;
@@ -802,6 +859,13 @@ static V3 sample_emitters(const lwo_scene *s, V3 pos, V3 origin, V3 n, uint32_t 
     return V3_ZERO;
 }
 
+/* sample_emitters (integrator.rs:441-469). */
+static V3 sample_emitters(const lwo_scene *s, V3 pos, V3 origin, V3 n, uint32_t *rng) {
+    uint32_t start, count;
+    emitter_cell(s, pos, &start, &count);
+    return sample_cell_emitters(s, start, count, origin, n, rng);
+}
+
 /* water_interface (integrator.rs:477-505). Writes the new direction and origin. */
 static int water_interface(const lwo_params *p, V3 pos, V3 d, V3 n, int front, int in_water, REAL eps,
                            uint32_t *rng, V3 *nd, V3 *no) {
@@ -824,15 +888,23 @@ static int water_interface(const lwo_params *p, V3 pos, V3 d, V3 n, int front, i
     return front;
 }
 
-/* water_plane (integrator.rs:511-526). Returns 1 and the distance when met. */
+/* The water plane's height in the current frame. */
+static inline REAL water_height(const lwo_params *p) {
+    return lwo_reb ? (REAL)p->water_plane[0] - (REAL)lwo_fa[1] : (REAL)p->water_plane[0];
+}
+
+/* water_plane (integrator.rs:511-526). Returns 1 and the distance when met. In the current frame
+ * the grid's columns span [-A, size - A). */
 static int water_plane(const lwo_scene *s, V3 o, V3 d, REAL *tp) {
     const lwo_params *p = s->params;
     if ((REAL)p->water_plane[1] == K(0.0) || d.y == K(0.0)) return 0;
-    REAL t = ((REAL)p->water_plane[0] - o.y) / d.y;
+    REAL t = (water_height(p) - o.y) / d.y;
     if (!(t > K(0.0) && t < (REAL)INFINITY)) return 0;
     V3 at = vadd(o, vmuls(d, t));
-    V3 size = grid_size(s);
-    if (at.x >= K(0.0) && at.z >= K(0.0) && at.x < size.x && at.z < size.z) return 0;
+    const int32_t ax = lwo_reb ? lwo_fa[0] : 0, az = lwo_reb ? lwo_fa[2] : 0;
+    REAL x0 = (REAL)(-ax), z0 = (REAL)(-az);
+    REAL sx = (REAL)((int32_t)(p->grid_dims[0] * 16u) - ax), sz = (REAL)((int32_t)(p->grid_dims[2] * 16u) - az);
+    if (at.x >= x0 && at.z >= z0 && at.x < sx && at.z < sz) return 0;
     *tp = t;
     return 1;
 }
@@ -840,15 +912,27 @@ static int water_plane(const lwo_scene *s, V3 o, V3 d, REAL *tp) {
 /* under_water_plane (integrator.rs:531-534). */
 static inline int under_water_plane(const lwo_scene *s, V3 o, V3 d) {
     const lwo_params *p = s->params;
-    return (REAL)p->water_plane[1] != K(0.0) && o.y < (REAL)p->water_plane[0] && d.y <= K(0.0);
+    return (REAL)p->water_plane[1] != K(0.0) && o.y < water_height(p) && d.y <= K(0.0);
 }
 
 /* The camera a sample starts from: Params in the FP32 build, the f64 camera in the FP64
- * twin when one is given. */
-typedef struct { V3 pos, fwd, right, up; REAL tan_half, aspect; } Cam;
+ * twin when one is given. `framed`: pos is relative to the chunk corner of `frame` (Params'
+ * see_through[2] and [3]); otherwise to the grid origin. */
+typedef struct { V3 pos, fwd, right, up; REAL tan_half, aspect; uint32_t framed, frame; } Cam;
 
-/* render_sample (integrator.rs:539-709). */
+static V3 render_path(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_t py, uint32_t sample);
+
+/* render_sample (integrator.rs:539-709), in the camera's frame. */
 static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_t py, uint32_t sample) {
+    lwo_reb = cam->framed != 0;
+    if (lwo_reb) frame_unpack(cam->frame, lwo_fa);
+    V3 r = render_path(s, cam, px, py, sample);
+    lwo_reb = 0;
+    lwo_fa[0] = lwo_fa[1] = lwo_fa[2] = 0;
+    return r;
+}
+
+static V3 render_path(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_t py, uint32_t sample) {
     const lwo_params *p = s->params;
     uint32_t width = p->frame[0], height = p->frame[1], max_bounces = p->frame[3];
     REAL eps = (REAL)p->misc_f[1];
@@ -901,6 +985,7 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
             in_water = water_interface(p, vadd(o, vmuls(d, tp)), d, n, front, in_water, eps, &rng, &nd, &no);
             d = nd;
             o = no;
+            if (lwo_reb) o = rebase(o);
             specular = 1;
             tmin = K(0.0);
             continue;
@@ -935,6 +1020,7 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
             in_water = water_interface(p, pos, d, n, front, in_water, eps, &rng, &nd, &no);
             d = nd;
             o = no;
+            if (lwo_reb) o = rebase(o);
             specular = 1;
             tmin = K(0.0);
             continue;
@@ -943,6 +1029,7 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
             beta = vmul(beta, vlerp(V3_ONE, albedo, alpha));
             if (TH) beta0 = vmul(beta0, vlerp(V3_ONE, albedo0, alpha));
             o = vadd(pos, vmuls(d, eps));
+            if (lwo_reb) o = rebase(o);
             tmin = K(0.0);
             continue;
         }
@@ -958,6 +1045,11 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
         bounces += 1;
 
         V3 origin = vadd(pos, vmuls(n, eps));
+        /* the emitters' cell, found in the hit's frame before the origin moves to its own */
+        const int sample_e = !emits && strategy != EMITTER_SAMPLING_NONE;
+        uint32_t e_start = 0, e_count = 0;
+        if (sample_e) emitter_cell(s, pos, &e_start, &e_count);
+        if (lwo_reb) origin = rebase(origin);
         V3 sun = TH ? v3((REAL)TH->sun[0], (REAL)TH->sun[1], (REAL)TH->sun[2]) : v3f4(p->sun_dir);
         REAL sd3 = TH ? (REAL)TH->sun[3] : (REAL)p->sun_dir[3];
         REAL sin_r = R_SQRT(rmax(K(1.0) - sd3 * sd3, K(0.0)));
@@ -979,8 +1071,8 @@ static V3 render_sample(const lwo_scene *s, const Cam *cam, uint32_t px, uint32_
                 radiance = vadd(radiance, vmuls(vmul(vmul(vmul(beta, albedo), v3f4(p->sun_color)), tr), cos_l));
             }
         }
-        if (!emits && strategy != EMITTER_SAMPLING_NONE)
-            radiance = vadd(radiance, vmul(vmul(beta, albedo), sample_emitters(s, pos, origin, n, &rng)));
+        if (sample_e)
+            radiance = vadd(radiance, vmul(vmul(beta, albedo), sample_cell_emitters(s, e_start, e_count, origin, n, &rng)));
 
         beta = vmul(beta, albedo);
         if (TH) beta0 = vmul(beta0, albedo0);

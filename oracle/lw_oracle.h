@@ -136,6 +136,9 @@ void lwo32_render_sample(const lwo_scene *s, uint32_t px, uint32_t py, uint32_t 
 void lwo32_sample_emitters(const lwo_scene *s, const float pos[3], const float origin[3],
                            const float n[3], uint32_t *rng_state, float out[3]);
 void lwo32_emitter_cell(const lwo_scene *s, const float p[3], uint32_t *start, uint32_t *count);
+/* One step of chunk-origin rebasing (the library's precision option): x, held in the frame of
+ * chunk corner *word, moved to the frame of the corner nearest it; *word becomes that corner. */
+void lwo32_rebase(float x[3], uint32_t *word);
 void lwo32_preetham_radiance(const lwo_scene *s, const float d[3], float out[3]);
 void lwo32_build_sky_cache(const lwo_scene *s, uint32_t n, float *out);
 void lwo32_sky_radiance(const lwo_scene *s, const float d[3], float out[3]);
@@ -186,6 +189,9 @@ double lwo_game_before_gamma(double x);
 /* ---- FP64 build ---------------------------------------------------------------------- */
 void lwo64_render_sample(const lwo_scene *s, const lwo_camera64 *cam, uint32_t px, uint32_t py,
                          uint32_t sample, double out[3]);
+/* Per-sample radiance of the FP64 twin, (h, w, count, 3) doubles. */
+void lwo64_render_samples(const lwo_scene *s, const lwo_camera64 *cam, uint32_t x0, uint32_t y0, uint32_t w, uint32_t h,
+                          uint32_t sample_start, uint32_t count, double *out, int threads);
 void lwo64_render_mean(const lwo_scene *s, const lwo_camera64 *cam, uint32_t x0, uint32_t y0,
                        uint32_t w, uint32_t h, uint32_t spp, double *out, int threads);
 /* lwo64_render_mean under a theta. */

@@ -132,6 +132,7 @@ def _declare(L):
     L.lwo_bounds_errors.restype = C.c_uint64
     L.lwo64_render_sample.argtypes = [sp, P(Camera64), C.c_uint32, C.c_uint32, C.c_uint32, D3]
     L.lwo64_render_mean.argtypes = [sp, P(Camera64)] + [C.c_uint32] * 5 + [C.c_void_p, C.c_int]
+    L.lwo64_render_samples.argtypes = [sp, P(Camera64)] + [C.c_uint32] * 6 + [C.c_void_p, C.c_int]
     L.lwo_tonemap.argtypes = [C.c_void_p, C.c_uint64, C.c_float, C.c_uint32, C.c_uint32, C.c_uint32, C.c_float,
                               C.c_void_p]
     L.lwo_game_tone_curve.argtypes = [C.c_void_p]
@@ -271,6 +272,13 @@ class OracleScene:
                                 out.ctypes.data, threads)
         return out
 
+    def render_samples64(self, x0, y0, w, h, sample_start, count, cam=None, threads=0):
+        """The FP64 oracle's per-sample radiance, shape (h, w, count, 3), f64."""
+        out = np.zeros((h, w, count, 3), dtype=np.float64)
+        lib().lwo64_render_samples(self.ref, C.byref(cam) if cam is not None else None, x0, y0, w, h, sample_start,
+                                   count, out.ctypes.data, threads)
+        return out
+
     def render_mean_theta(self, theta, x0, y0, w, h, spp, cam=None, threads=0):
         """The FP64 mean radiance under a `Theta`, shape (h, w, 3)."""
         out = np.zeros((h, w, 3), dtype=np.float64)
@@ -352,6 +360,18 @@ def water_exp(x):
     out = np.zeros_like(x)
     L.lwo32_water_exp(x.size, x.ctypes.data, out.ctypes.data)
     return out
+
+
+def rebase(x, word):
+    """One step of chunk-origin rebasing (kernel_impl.h `rebase`): (x moved to the frame of the chunk
+    corner nearest it, that corner's frame word), for x (3 f32) held in the frame of ``word``."""
+    L = lib()
+    L.lwo32_rebase.argtypes = [C.c_void_p, C.POINTER(C.c_uint32)]
+    L.lwo32_rebase.restype = None
+    v = np.ascontiguousarray(x, np.float32).copy()
+    w = C.c_uint32(int(word))
+    L.lwo32_rebase(v.ctypes.data, C.byref(w))
+    return v, int(w.value)
 
 
 def draw_sky_map(quick_sky, stars, w, h, atlas, atlas_w, threads=0):
