@@ -905,7 +905,7 @@ lw_status install_scene(lw_ctx *c, const lw_scene_desc *d, uint32_t n_bricks, ui
     CK(c, ensure(c->occ, n_bricks), "allocating the occupancy masks");
     CK(c, cudaMemsetAsync(c->error.p, 0, 4, c->stream), "clearing the error word");
     SceneUploadDesc u{c->grid.p, (uint32_t)nb, n_bricks, o[0], o[1], o[2], (uint32_t)d->models_len, n_ov,
-                      c->top.p, c->bricks.p, c->occ.p, c->error.p};
+                      (const uint4 *)c->models.p, c->top.p, c->bricks.p, c->occ.p, c->error.p};
     CK(c, launch_relayout(u, c->stream), "re-laying the grid");
     uint32_t err = 0;
     CK(c, cudaMemcpyAsync(&err, c->error.p, 4, cudaMemcpyDeviceToHost, c->stream), "reading the error word");
@@ -1128,6 +1128,7 @@ lw_status lw_voxel_lookup(lw_ctx *c, uint32_t n, const int32_t *xyz, uint32_t *o
                 return fail(c, LW_ERR_INVALID_ARGUMENT, "voxel %u outside the grid", i);
     lw_params p{};
     std::memcpy(p.grid_dims, c->dims, sizeof c->dims);
+    std::memcpy(p.off, c->offsets, sizeof p.off);  // the reference grid's top and brick offsets
     CK(c, ensure(c->xyz, (size_t)3 * n), "allocating coordinates");
     CK(c, ensure(c->vox, n), "allocating ids");
     CK(c, cudaMemcpyAsync(c->xyz.p, xyz, 12 * (size_t)n, cudaMemcpyHostToDevice, c->stream), "uploading coordinates");

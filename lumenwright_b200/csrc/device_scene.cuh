@@ -3,13 +3,15 @@
 // Layout in HBM (built by lw_scene_upload from the reference's `HqScene` buffers):
 //   top     uint2[nb]            (top entry, overlay entry) per brick: one 8-byte load per brick
 //                                where the reference reads two words (trace.rs:181-182)
-//   bricks  uint16[n * 4096]     the voxel ids of each non-uniform brick, 4x4x4-sub-block-major:
+//   bricks  uint16[n * 4096]     the voxel ids of each non-uniform brick (a model without quads
+//                                re-laid as air, 0: csrc/scene.cu), 4x4x4-sub-block-major:
 //                                sub-block ((y>>2)*4 + (z>>2))*4 + (x>>2), then ((y&3)*4+(z&3))*4+(x&3)
 //                                inside it, so one sub-block is one 128-byte line
 //   occ     uint2[n]             a 64-bit mask per non-uniform brick: bit s set when sub-block s
-//                                holds a voxel whose model is not 0 (air)
+//                                holds a voxel whose model has quads
 //   quads   DevQuad[q]           96-byte records with the normal eu x ev and |n|^2 precomputed
-//   grid    uint32[]             the reference's grid, read for the overlay cells and ov_quads
+//   grid    uint32[]             the reference's grid, read for the overlay cells and ov_quads and
+//                                by the voxel lookup
 //   models, atlas, emitters, emitter_grid, sky: the reference's buffers unchanged
 //   gamma   float[256]           gamma_to_linear(k / 255) for every byte k (math.rs:214-216)
 #pragma once
@@ -208,12 +210,16 @@ LW_DI uint32_t brick_voxel(const DevScene &S, uint32_t entry, int lx, int ly, in
     uint32_t v = (uint32_t)(((ly & 3) * 4 + (lz & 3)) * 4 + (lx & 3));
     return ldg(S.bricks + ((size_t)entry * 4096u + sb * 64u + v));
 }
+// The reference's voxel id, from the reference's grid (the traversal's bricks re-lay models
+// without quads as air).
 LW_DI uint32_t voxel(const DevScene &S, const DevParams &P, int x, int y, int z) {
     uint32_t b = ((uint32_t)(y >> 4) * P.grid_dims.z + (uint32_t)(z >> 4)) * P.grid_dims.x + (uint32_t)(x >> 4);
-    uint32_t e = ldg(S.top + b).x;
+    uint32_t e = ldg(S.grid + (size_t)P.off.x + b);
     if (e == EMPTY) return 0;
     if (e & UNIFORM) return e & ~UNIFORM;
-    return brick_voxel(S, e, x & 15, y & 15, z & 15);
+    uint32_t local = (uint32_t)((((y & 15) * 16 + (z & 15)) * 16) + (x & 15));
+    uint32_t w = ldg(S.grid + (size_t)P.off.y + (size_t)e * 2048u + (local >> 1));
+    return (w >> ((local & 1u) * 16u)) & 0xFFFFu;
 }
 
 LW_DI float safe_inv(float x) {  // trace.rs:293-299

@@ -186,6 +186,7 @@ struct SceneUploadDesc {
     const uint32_t *grid;  // device copy of the reference grid
     uint32_t nb, n_bricks, off_top, off_bricks, off_ov_top;
     uint32_t n_models, n_ov_bricks;
+    const uint4 *models;   // device copy of the models (quad offset, quad count, flags, -)
     uint2 *top;
     uint16_t *bricks;
     uint2 *occ;

@@ -1,5 +1,13 @@
 // Scene re-layout kernels run by lw_scene_upload: the fused (top, overlay) entries, the
 // sub-block-major bricks with their occupancy masks, and the 96-byte quad records.
+//
+// In the traversal's copy a voxel whose model has no quads (a fluid block inside its fluid, every
+// face culled) is re-laid as air, 0, and counts as empty in the occupancy masks. The traversal
+// visits such a cell exactly as an air cell (one iteration of trace.rs's loop, the same DDA step,
+// no quad to test), so the results are the reference's; the cell no longer stops its lane for a
+// round of quad tests with nothing to test. A uniform brick of such a model keeps its entry as a
+// uniform brick of air, which is still stepped voxel by voxel, not skipped as an empty brick. The
+// reference's ids stay in the uploaded grid, which the voxel lookup reads.
 #include "internal.h"
 
 namespace lw {
@@ -13,8 +21,13 @@ __global__ void k_top(SceneUploadDesc d) {
     uint32_t ov = d.grid[d.off_ov_top + b];
     bool bad = false;
     if (e != EMPTY) {
-        if (e & UNIFORM) bad |= (e & ~UNIFORM) >= d.n_models;
-        else bad |= e >= d.n_bricks;
+        if (e & UNIFORM) {
+            const uint32_t m = e & ~UNIFORM;
+            bad |= m >= d.n_models;
+            if (!bad && d.models[m].y == 0u) e = UNIFORM;  // a uniform brick of air
+        } else {
+            bad |= e >= d.n_bricks;
+        }
     }
     if (ov != EMPTY) bad |= ov >= d.n_ov_bricks;
     if (bad) {
@@ -46,9 +59,10 @@ __global__ void __launch_bounds__(256) k_bricks(SceneUploadDesc d) {
             uint32_t x = local & 15u, z = (local >> 4) & 15u, y = local >> 8;
             uint32_t sb = ((y >> 2) * 4u + (z >> 2)) * 4u + (x >> 2);
             uint32_t v = ((y & 3u) * 4u + (z & 3u)) * 4u + (x & 3u);
+            bad |= id >= d.n_models;
+            if (id != 0u && id < d.n_models && d.models[id].y == 0u) id = 0u;  // no quads: air
             dst[sb * 64u + v] = (uint16_t)id;
             if (id != 0u) mine |= 1ull << sb;
-            bad |= id >= d.n_models;
         }
     }
     atomicOr(&mask, mine);

@@ -98,7 +98,7 @@ def test_later_coplanar_quad(ctx):  # tests.rs:688-721
     assert [h.quad for h in got] == [6, 7] * 16
 
 
-def test_voxel_lookup_is_bit_exact(ctx):  # scene.rs:271-284 on the re-laid bricks
+def test_voxel_lookup_is_bit_exact(ctx):  # scene.rs:271-284 on the uploaded reference grid
     for ks in (basic_scene(True), lamp_scene(L.EMITTER_SAMPLING_ONE, True), wall_scene()):
         upload(ctx, ks)
         dims = [int(v) for v in ks.params["grid_dims"][:3]]
