@@ -646,7 +646,11 @@ def main():
                          "rays_per_launch": rays / max(1, trace_launches),
                          "algorithmic_bytes_per_launch": trace_bytes / max(1, trace_launches),
                          "avg_launch_ms": trace_ms / max(1, trace_launches),
-                         "trace_bytes_per_sample": alg["trace_bytes_per_sample"]},
+                         "trace_bytes_per_sample": alg["trace_bytes_per_sample"],
+                         # the same accesses rounded up to the 32-byte sectors L2 and DRAM move
+                         "trace_sector_bytes_per_sample": alg.get("trace_sector_bytes_per_sample"),
+                         "achieved_sector_rounded": (alg["trace_sector_bytes_per_sample"] * my_samples / (trace_ms / 1e3) / 1e9
+                                                     if trace_ms > 0 and "trace_sector_bytes_per_sample" in alg else None)},
             "roofline_issue": {"bound": "issue", "kernel": "k_wf_trace", "achieved": issue, "peak": issue_peak,
                                "unit": "G warp instructions/s",
                                "frac": issue / issue_peak if issue and issue_peak else None,
