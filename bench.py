@@ -16,7 +16,7 @@ Under ``torchrun`` (N > 1) the frame's spp is N x 1024 and each rank renders eve
 1/N of the frame's 8x4-pixel tiles (weak scaling); one NCCL reduce of the accumulators per step,
 inside the timed region, gives rank 0 the frame bit for bit as one GPU renders it.
 
-At N = 1 the line also carries the north star's other forms, each on its own configuration and
+At N = 1 the line also carries the path's other forms, each on its own configuration and
 timed the same way (unless --no-extras): ``reference_cuda_port`` (the reference's CUDA backend
 ported as written, on the same frame), ``batched_c3`` (64 cameras in one CUDA graph against 64
 separate renders), ``adjoint_c4`` (forward + backward), ``precision_c5`` (3840x2160 at --c5-spp
@@ -661,7 +661,8 @@ def main():
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(frame)
         if world == 1 and not args.no_extras:
-            # The other forms of the north star, each on its own configuration, timed the same way.
+            # The other forms of the path (batched, adjoint, precision), each on its own configuration,
+            # timed the same way.
             line["accuracy"] = accuracy(frame, e2e_img)
             port_img, port = extra_reference_port(frame, local)
             port["image_rel_rmse_vs_product"] = float(np.sqrt(np.mean((port_img - e2e_img) ** 2)) / e2e_img.mean())
