@@ -125,6 +125,7 @@ struct lw_ctx {
     // is then -1 until lw_get_stats adds the last launch's event time)
     double kernel_ms_base = 0.0;
     LaunchShape shape_wf{};        // the tracing kernel reading the scene from global memory
+    LaunchShape shape_wf_reb{};    // ... with chunk-origin rebasing
     LaunchShape shape_wf_staged{}; // ... and staging it in shared memory (stage_bytes of it)
     size_t stage_bytes = 0;
     struct WfBufs {
@@ -497,7 +498,8 @@ lw_status run_wavefront(lw_ctx *c, const DevScene &S, const DevParams &P, const 
         CK(c, launch_wf_shade(S, P, W, F, wf_shade_blocks(c, n), c->stream), "launching the shading kernel");
         CK(c, cudaEventRecord(e[1], c->stream), "recording an event");
         const bool staged = c->stage_bytes && P.see_through.z == 0u;  // the rebased tracing kernel is unstaged
-        CK(c, launch_wf_trace(S, P, F, staged ? c->shape_wf_staged : c->shape_wf, budget, c->wf_tail, staged ? c->stage_bytes : 0,
+        const LaunchShape &shape = staged ? c->shape_wf_staged : (P.see_through.z ? c->shape_wf_reb : c->shape_wf);
+        CK(c, launch_wf_trace(S, P, F, shape, budget, c->wf_tail, staged ? c->stage_bytes : 0,
                               c->stream), "launching the tracing kernel");
         CK(c, cudaEventRecord(e[2], c->stream), "recording an event");
         CK(c, launch_wf_advance(F, c->stream), "launching the iteration step");
@@ -684,6 +686,7 @@ lw_status lw_ctx_create(int device, lw_ctx **out) {
     if ((e = cudaMemcpy(c->gamma.p, lut, sizeof lut, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "uploading the gamma table");
     if ((e = ensure(c->counter, 1)) != cudaSuccess || (e = ensure(c->error, 1)) != cudaSuccess) return bail(e, "allocating counters");
     c->shape_wf = wf_trace_shape(device);
+    c->shape_wf_reb = wf_trace_shape(device, 0, true);
     c->shape_accum = render_shape(MODE_ACCUM, device, (int)c->tuning.threads);
     c->shape_samples = render_shape(MODE_SAMPLES, device, (int)c->tuning.threads);
     *out = c;

@@ -114,7 +114,9 @@ constexpr uint32_t kShadeThreads = LW_SHADE_THREADS;
 #ifndef LW_TRACE_STAGE_MAX
 #define LW_TRACE_STAGE_MAX 0
 #endif
-LaunchShape wf_trace_shape(int device, size_t stage_bytes = 0);
+// The persistent tracing kernel's grid: its resident blocks per SM x the SMs (reb: the form with
+// chunk-origin rebasing).
+LaunchShape wf_trace_shape(int device, size_t stage_bytes = 0, bool reb = false);
 cudaError_t launch_wf_shade(const DevScene &S, const DevParams &P, const WorkDesc &W, const WfState &F, uint32_t blocks,
                             cudaStream_t st);
 cudaError_t launch_wf_shade_batch(const DevScene &S, const DevParams &P0, const BatchDesc &B, const WfState &F,

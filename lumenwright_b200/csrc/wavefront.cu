@@ -283,8 +283,15 @@ LW_DI void shade_slot(bool valid, uint32_t i, const DevScene &S0, const DevParam
 #ifndef LW_WF_SHADE_MINB_BATCH
 #define LW_WF_SHADE_MINB_BATCH 6
 #endif
+// The same for the forms with chunk-origin rebasing (116 B of spills at 80 registers, but at 98
+// registers and two blocks a SM the 8-spp C5 frame shaded in 51.7 ms against 44.0).
+#ifndef LW_WF_SHADE_MINB_REB
+#define LW_WF_SHADE_MINB_REB 6
+#endif
 template <bool BATCH, bool REB = false>
-__global__ void __launch_bounds__(kShadeThreads, (BATCH ? LW_WF_SHADE_MINB_BATCH : LW_WF_SHADE_MINB) * 128 / kShadeThreads)
+__global__ void __launch_bounds__(kShadeThreads,
+                                  (BATCH ? LW_WF_SHADE_MINB_BATCH : (REB ? LW_WF_SHADE_MINB_REB : LW_WF_SHADE_MINB)) * 128 /
+                                      kShadeThreads)
 k_wf_shade(const DevScene S0, const DevParams P0, const WorkDesc W, const BatchDesc B, const WfState F) {
     const uint32_t t = *(volatile uint32_t *)&F.ctr[12];
     const uint32_t cur = t % 3u, prev = (t + 2u) % 3u, next = (t + 1u) % 3u;
@@ -322,6 +329,12 @@ __global__ void k_wf_advance_graph(const WfState F, cudaGraphConditionalHandle l
 #ifndef LW_WF_TRACE_MINB
 #define LW_WF_TRACE_MINB 8
 #endif
+// The tracing kernel with chunk-origin rebasing (the frame word held across the traversal): 7 blocks
+// a SM, 72 registers, 20 B of spills; at 8 blocks (64 registers) it spills 44 B and took 99.7 ms on
+// the 8-spp C5 frame against 95.5, at 6 blocks 101.5.
+#ifndef LW_WF_TRACE_MINB_REB
+#define LW_WF_TRACE_MINB_REB 7
+#endif
 // Traces the queued rays of this iteration: each lane takes a ray and advances it in rounds
 // (trace_round: at most `budget` visits through empty space, then the quad tests of at most one
 // cell, so the lanes of a warp run one phase of quad tests per round together), and takes the
@@ -332,7 +345,7 @@ __global__ void k_wf_advance_graph(const WfState F, cudaGraphConditionalHandle l
 // entries of 8 bytes, the dynamic shared memory of the launch) into shared memory and reads them
 // there. REB: chunk-origin rebasing, each ray in the frame of its slot's frame word.
 template <bool STAGED, bool REB = false>
-__global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(const DevScene S0, const DevParams P, const WfState F,
+__global__ void __launch_bounds__(kTraceThreads, REB ? LW_WF_TRACE_MINB_REB : LW_WF_TRACE_MINB) k_wf_trace(const DevScene S0, const DevParams P, const WfState F,
                                                                       uint32_t budget, uint32_t tail) {
     extern __shared__ uint2 s_scene[];
     DevScene S = S0;
@@ -441,10 +454,11 @@ __global__ void __launch_bounds__(kTraceThreads, LW_WF_TRACE_MINB) k_wf_trace(co
     }
 }
 
-LaunchShape wf_trace_shape(int device, size_t stage_bytes) {
+LaunchShape wf_trace_shape(int device, size_t stage_bytes, bool reb) {
     int sms = 0, per_sm = 0;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    const void *k = stage_bytes ? (const void *)k_wf_trace<true> : (const void *)k_wf_trace<false>;
+    const void *k = stage_bytes ? (const void *)k_wf_trace<true>
+                                : (reb ? (const void *)k_wf_trace<false, true> : (const void *)k_wf_trace<false>);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTraceThreads, stage_bytes);
     if (per_sm < 1) per_sm = 1;
     return LaunchShape{sms * per_sm, kTraceThreads};
