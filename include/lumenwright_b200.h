@@ -135,7 +135,7 @@ typedef struct {
  * threads: threads per block of the megakernel (64, 128 or 256).
  * budget: voxel visits a ray advances before its lane may take up other work: the megakernel's
  *   regrouping period (0 = a whole traversal at once), the wavefront's visits through empty
- *   space per round, between queue fetches (0 = 5).
+ *   space per round, between queue fetches (0 = 8).
  * sub: samples per work item (0: one for the wavefront; for the megakernel and the batched form
  *   chosen from the frame so every lane gets many items).
  * paths: path slots of the wavefront (0: sized from each launch's sample count, 2^16 to 2^23). */

@@ -100,8 +100,9 @@ struct WfState {
     uint32_t *frame;  // per slot: the frame word of its path (chunk-origin rebasing only)
 };
 // Visits through empty space per round of the wavefront's tracing kernel when the tuning leaves it
-// at 0 (5: +1 % over 4 at c2 and c4; 6 gives the same).
-constexpr uint32_t kWfBudget = 5u;
+// at 0: 8, since cells without quads count as air (a 256-spp C2 frame traced in 118.0, 115.4, 114.0,
+// 113.3 and 114.0 ms at 4, 5, 6, 8 and 10; the 8-spp C5 frame in 90.0 at 5 and 87.7 at 8).
+constexpr uint32_t kWfBudget = 8u;
 #ifndef LW_SHADE_THREADS
 #define LW_SHADE_THREADS 256
 #endif
