@@ -101,7 +101,7 @@ def c3_jobs(sky_backend, cams=None, spp_scale=1.0):
 class Autotuner:
     """Picks the batched render's launch tuning for a workload by timing trial renders.
 
-    Candidates: the wavefront engine with queue depth (path slots) {automatic, 2^22, 2^23} x visits
+    Candidates: the wavefront engine with queue depth (path slots) {automatic, 2^22, 2^23, 2^24} x visits
     between queue fetches {4, 8}, and the persistent megakernel with threads per block {64, 128,
     256} x regrouping period {0 (whole traversals), 24}; each with samples per work item
     {automatic, 4}. A trial renders the workload with every camera's spp cut to
@@ -115,7 +115,7 @@ class Autotuner:
     def candidates(cls):
         out = []
         for sub in cls.SUBS:
-            for paths in (0, 1 << 22, 1 << 23):
+            for paths in (0, 1 << 22, 1 << 23, 1 << 24):
                 for budget in (4, 8):
                     out.append({"engine": 0, "threads": 128, "budget": budget, "sub": sub, "paths": paths})
             for threads in (128, 64, 256):
