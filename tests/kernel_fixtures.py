@@ -111,6 +111,35 @@ def basic_scene(entity: bool) -> KScene:
                      emitters_array([]), [0] * L.EMITTER_GRID_HEADER)
 
 
+def hollow_scene() -> KScene:
+    """3x1x1 bricks holding a model without quads (a fluid block inside its fluid): brick 0 is a
+    uniform brick of it, brick 1 is full of it but for one cube at local (8, 5, 5) and one air voxel
+    at (3, 9, 9), brick 2 is uniform cubes. The traversal re-lays the model as air."""
+    quads = cube(L.ALPHA_OPAQUE)
+    models = models_array([(0, 0), (0, 6), (6, 0)])
+    nb = 3
+    top = [L.UNIFORM | 2, 0, L.UNIFORM | 1]
+    ids = np.full(4096, 2, np.uint32)
+    ids[(5 * 16 + 5) * 16 + 8] = 1
+    ids[(9 * 16 + 9) * 16 + 3] = 0
+    brick = (ids[0::2] | (ids[1::2] << 16)).astype(np.uint32)
+    grid = list(top)
+    off_bricks = len(grid)
+    grid += list(brick)
+    off_ov_top = len(grid)
+    grid += [L.EMPTY] * nb
+    off_ov_cells = len(grid)
+    off_ov_quads = len(grid)
+    grid.append(0)
+    p = L.new_params()
+    p["grid_dims"] = [3, 1, 1, nb]
+    p["off"] = [0, off_bricks, off_ov_top, off_ov_cells]
+    p["off2"] = [off_ov_quads, 2, 1, len(quads)]
+    p["misc_f"] = [1.0, 1e-3, 0.0, 0.0]
+    return KScene(p, grid, models, L.quads_array(quads), [0xFFFF_FFFF, 0x0000_0000],
+                  emitters_array([]), [0] * L.EMITTER_GRID_HEADER)
+
+
 LAMP_EMITTANCE = 0.5  # tests.rs:301
 LAMP_INTENSITY = 13.0  # tests.rs:303
 

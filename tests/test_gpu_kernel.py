@@ -9,8 +9,8 @@ import math
 import numpy as np
 import pytest
 
-from kernel_fixtures import (INF, LAMP_EMITTANCE, LAMP_INTENSITY, SUN_ATLAS, basic_scene, lamp_scene, map_scene,
-                             norm, set_preetham_45, sun_atlas, sun_sprite_params, wall_rays, wall_scene)
+from kernel_fixtures import (INF, LAMP_EMITTANCE, LAMP_INTENSITY, SUN_ATLAS, basic_scene, hollow_scene, lamp_scene,
+                             map_scene, norm, set_preetham_45, sun_atlas, sun_sprite_params, wall_rays, wall_scene)
 from lumenwright_b200 import layout as L
 from oracle import oracle as O
 
@@ -108,6 +108,24 @@ def test_voxel_lookup_is_bit_exact(ctx):  # scene.rs:271-284 on the uploaded ref
         v = O.OracleScene(*ks.buffers())
         want = np.array([v.voxel(*map(int, p)) for p in xyz[:: max(1, len(xyz) // 20000)]], np.uint32)
         assert np.array_equal(got[:: max(1, len(xyz) // 20000)], want)
+
+
+def test_cells_of_models_without_quads_are_traversed_as_the_reference_does(ctx):
+    # The traversal's bricks hold a model without quads as air (and a uniform brick of it as a
+    # uniform brick of air); the hits are the oracle's, on the reference's grid, bit for bit, and the
+    # voxel lookup still gives the reference's ids.
+    ks = hollow_scene()
+    rng = np.random.default_rng(21)
+    rays = [((0.5, 5.5, 5.5), (1, 0, 0)), ((0.5, 9.5, 9.5), (1, 0, 0)), ((-4.0, 5.2, 5.7), (1, 0.01, 0.0))]
+    for _ in range(3000):
+        o = rng.uniform((-8.0, -8.0, -8.0), (56.0, 24.0, 24.0)).astype(np.float32)
+        tgt = rng.uniform((0.0, 0.0, 0.0), (48.0, 16.0, 16.0)).astype(np.float32)
+        rays.append((o, norm(tgt - o)))
+    got = check_rays(ctx, ks, rays)
+    assert got[0] is not None and got[0].quad == 3 and abs(got[0].t - 23.5) < 1e-3  # the cube's face at x = 24
+    assert sum(g is not None for g in got) > 1000
+    xyz = np.array([(1, 1, 1), (20, 5, 5), (24, 5, 5), (19, 9, 9), (40, 3, 3)], np.int32)
+    assert list(ctx.voxel_lookup(xyz)) == [2, 2, 1, 0, 1]
 
 
 def test_water_exp_is_the_oracles_bit_for_bit(ctx):
