@@ -22,6 +22,13 @@ static_assert(sizeof(lw_params) == sizeof(DevParams), "Params layout");
 static_assert(sizeof(lw_quad) == 80 && sizeof(lw_model) == 16 && sizeof(lw_emitter) == 32, "record layout");
 static_assert(sizeof(lw_quick_sky) == 608, "QuickSky layout");
 
+// The item sums a launch may fill (16 B each): 16 GiB, or a quarter of the device memory free when
+// the context is made if that is less. One launch then covers the 1024-spp C2 frame (15.1 GB of
+// one-sample items), which in four launches of the 4 GiB cap before took 2.1 % longer (808.0 ms
+// against 791.6: each launch ends in a drain of the path pool).
+#ifndef LW_PARTIALS_CAP_GIB
+#define LW_PARTIALS_CAP_GIB 16
+#endif
 namespace {
 
 thread_local std::string g_create_error;
@@ -115,7 +122,7 @@ struct lw_ctx {
     cudaGraphExec_t batch_graph = nullptr;
     uint64_t batch_samples = 0;
     uint32_t batch_passes = 1;  // passes of the prepared batch (the wavefront's one-sample items)
-    size_t partials_cap_bytes = size_t(4) << 30;
+    size_t partials_cap_bytes = size_t(LW_PARTIALS_CAP_GIB) << 30;
     // the wavefront engine: path slots (grown to the largest pool used), queue fetch settings
 #ifndef LW_WF_TAIL
 #define LW_WF_TAIL 12
@@ -538,7 +545,7 @@ lw_status render_batches(lw_ctx *c, const lw_params *params, uint32_t s0, uint32
         // Items of one sample: a slot that ends a sample takes the next item at once, and when the
         // items run out no slot has more than one sample left, so the pool drains in few
         // iterations (against items of up to 16 samples: c2 +8 % at 256 spp, +4.5 % at 1024 spp
-        // in launches of 291 spp that the item sums' 4 GiB allow; c4 +8 %).
+        // in the launches of 291 spp that a 4 GiB item-sum cap allowed; c4 +8 %).
         pl = plan(c, probe.n_slots, spp, 1u);
     }
     CK(c, ensure(c->partials, (size_t)probe.n_slots * ((pl.batch + pl.sub - 1) / pl.sub)), "allocating partial sums");
@@ -685,6 +692,11 @@ lw_status lw_ctx_create(int device, lw_ctx **out) {
     if ((e = ensure(c->gamma, 256)) != cudaSuccess) return bail(e, "allocating the gamma table");
     if ((e = cudaMemcpy(c->gamma.p, lut, sizeof lut, cudaMemcpyHostToDevice)) != cudaSuccess) return bail(e, "uploading the gamma table");
     if ((e = ensure(c->counter, 1)) != cudaSuccess || (e = ensure(c->error, 1)) != cudaSuccess) return bail(e, "allocating counters");
+    {
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) == cudaSuccess && free_b / 4 < c->partials_cap_bytes)
+            c->partials_cap_bytes = free_b / 4 > (size_t(1) << 28) ? free_b / 4 : size_t(1) << 28;
+    }
     c->shape_wf = wf_trace_shape(device);
     c->shape_wf_reb = wf_trace_shape(device, 0, true);
     c->shape_accum = render_shape(MODE_ACCUM, device, (int)c->tuning.threads);

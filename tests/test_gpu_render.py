@@ -80,9 +80,8 @@ def test_c2_per_sample_radiance(ctx, c2, rect):
 @pytest.mark.parametrize("start,count", [(290, 3), (1000, 4), (1020, 4)])
 @pytest.mark.parametrize("rect", [(600, 300, 48, 24), (100, 600, 48, 24)])
 def test_c2_per_sample_radiance_far_into_the_stream(ctx, c2, rect, start, count):
-    # Samples 290-292 straddle the boundary between the drop-in's first two launches of the C2
-    # frame (4 GiB of item sums hold 291 one-sample items per pixel slot); 1000-1023 are the
-    # frame's last samples at 1024 spp.
+    # Samples 290-292 (where the drop-in's launches of the C2 frame met under a 4 GiB item-sum
+    # cap) and 1000-1023, the frame's last samples at 1024 spp.
     ok, exact, got, want = per_sample(ctx, c2, *rect, count, start=start)
     report(f"C2 samples {start}..{start + count - 1}", rect, ok, exact, got, want)
     assert ok == 1.0, ok
