@@ -245,7 +245,10 @@ lw_status lw_scene_read(lw_ctx *ctx, uint32_t *grid, uint64_t grid_cap, lw_emitt
  * samples per pixel (at least 1). Writes the mean linear radiance per pixel, row-major, top row
  * first, to `out_rgb` (frame[0] * frame[1] * 3 floats). Non-finite samples are left out of the
  * sum and counted, as `pt_render` does (crates/lumenwright-ptx/src/lib.rs:76-84). The sums are
- * Kahan-compensated FP32. */
+ * Kahan-compensated FP32. The samples run in as few launches as keep a launch's item sums (16
+ * bytes a pixel sample with the wavefront's one-sample items) within 16 GiB, or a quarter of the
+ * device memory free when the context was made if that is less; `progress` is called after each
+ * launch. */
 lw_status lw_render_hq(lw_ctx *ctx, const lw_params *params, const float *sky, uint64_t sky_len, uint32_t spp,
                        lw_progress_fn progress, void *user, float *out_rgb);
 
