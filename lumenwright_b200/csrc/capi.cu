@@ -610,6 +610,8 @@ lw_status batch_graph_wavefront(lw_ctx *c, const std::vector<BatchDesc> &Bs, con
         const BatchDesc &B = Bs[k];
         e = cudaMemsetAsync(B.counter, 0, 4, c->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(F.state + (size_t)4 * F.n, 0, (size_t)F.n * sizeof(float4), c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemsetAsync(F.state + (size_t)kWfItemCameraWord * F.n, 0, (size_t)F.n * sizeof(float4), c->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(F.ctr, 0, 16 * sizeof(uint32_t), c->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(F.hit0, 0, (size_t)F.n * sizeof(float4), c->stream);
         cudaGraphNode_t loop_node = nullptr;

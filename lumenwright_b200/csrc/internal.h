@@ -99,6 +99,10 @@ struct WfState {
     float4 *ts;       // 3 float4 per slot (word k at ts[k * n + i]): a carried-over traversal
     uint32_t *frame;  // per slot: the frame word of its path (chunk-origin rebasing only)
 };
+// The path slots' word with an item's camera in the batched form (j, pixel slot, camera, -), which
+// the batched form clears with the core word before a pass: a slot that has not taken an item yet
+// then names camera 0, so the shading kernel reads the camera table within its bounds.
+constexpr int kWfItemCameraWord = 13;
 // Visits through empty space per round of the wavefront's tracing kernel when the tuning leaves it
 // at 0: 8, since cells without quads count as air (a 256-spp C2 frame traced in 118.0, 115.4, 114.0,
 // 113.3 and 114.0 ms at 4, 5, 6, 8 and 10; the 8-spp C5 frame in 90.0 at 5 and 87.7 at 8).

@@ -48,10 +48,12 @@ enum {
     W_EOFF = 10,   // eoff.xyz, k
     W_E1 = 11,     // first, faces, f, emode | fmode << 1
     W_ITEM = 12,   // px, py, sample, s_end (item words)
-    W_ITEM2 = 13,  // j, pixel slot, -, -
+    W_ITEM2 = 13,  // j, pixel slot, camera (batched form), -
     W_SUM = 14,    // s0, s1, s2, c0
     W_SUM2 = 15,   // c1, c2, -, -
 };
+
+static_assert(W_ITEM2 == kWfItemCameraWord, "the word the batched form clears");
 
 LW_DI float4 ld(const WfState &F, int k, uint32_t i) { return F.state[(size_t)k * F.n + i]; }
 LW_DI void st(const WfState &F, int k, uint32_t i, float4 v) { F.state[(size_t)k * F.n + i] = v; }
