@@ -272,6 +272,50 @@ def test_render_hq_mean_matches_cpu_backend(ctx):  # cpu/mod.rs:39-87 against cu
     assert calls and calls[-1] == (64, 64)
 
 
+def quad_view(eye, at, overlay, see_through, chunk_frames):
+    """basic_scene's cutout quad at x = 8.5 under a sky, seen from `eye`: as an overlay quad, or
+    (with its overlay cell emptied) as the frame's see-through quad behind the cube at x = 20..21,
+    in the grid's frame or in chunk frames."""
+    from lumenwright_b200 import native as N
+    ks = basic_scene(True)
+    p = ks.params
+    if not overlay:
+        ks.grid = ks.grid.copy()
+        ks.grid[int(p["off"][2])] = L.EMPTY
+    p["see_through"] = [6, 1, 0, 0] if see_through else [0, 0, 0, 0]
+    p["frame"] = [16, 16, 0, 2]
+    f = norm(np.array(at, np.float32) - np.array(eye, np.float32))
+    r = norm(np.cross(f, np.array([0, 1, 0], np.float32)).astype(np.float32))
+    u = np.cross(r, f).astype(np.float32)
+    p["cam_pos"] = [*eye, 0.12]
+    p["cam_fwd"] = [*f, 1.0]
+    p["cam_right"] = [*r, 0.0]
+    p["cam_up"] = [*u, 0.0]
+    set_preetham_45(p)
+    p["sun_dir"] = [0.3, 0.9, 0.316, 0.9995]
+    p["sun_color"] = [1.0, 0.9, 0.8, 0.03]
+    p["misc_f"][2] = 128
+    ks.sky = O.OracleScene(*ks.buffers()).build_sky_cache(128)
+    if chunk_frames:
+        ks.params = N.rebase_camera(p, eye)
+    return ks
+
+
+@pytest.mark.parametrize("view", ["overlay", "see-through"])
+@pytest.mark.parametrize("chunk_frames", [False, True])
+def test_overlay_and_see_through_quads_per_sample(ctx, view, chunk_frames):  # trace.rs:113-131 on the camera ray
+    # The overlay traversal (quads tested relative to their cell) and the see-through test (quads
+    # relative to the frame's corner) in both frames; the eyes sit in chunks 1 and 2 along x, so
+    # chunk frames hold them relative to x = 16 and x = 32.
+    eye, at = ((20.3, 7.6, 5.5), (8.5, 5.5, 5.5)) if view == "overlay" else ((24.3, 5.6, 5.4), (8.5, 5.5, 5.5))
+    ks = quad_view(eye, at, view == "overlay", view == "see-through", chunk_frames)
+    if chunk_frames:
+        assert ks.params["see_through"][2] == 1 and ks.params["see_through"][3] == (1 if view == "overlay" else 2)
+    got = samples_match(ctx, ks, 16, 16, 4)
+    bare = O.OracleScene(*quad_view(eye, at, False, False, False).buffers()).render_samples(0, 0, 16, 16, 0, 4)
+    assert (got != bare).any(-1).sum() >= 30  # the quad is in view in some samples
+
+
 def test_bad_buffers_are_refused(ctx):  # the C ABI never traps on a malformed scene
     from lumenwright_b200.native import LwError
     ks = basic_scene(False)
