@@ -9,6 +9,7 @@ from typing import Optional
 
 import numpy as np
 
+from . import anvil as AN
 from . import gamesky as G
 from . import layout as L
 from . import sky as SK
@@ -135,6 +136,21 @@ CONFIGS = {
 }
 
 
+def config_world(cfg: Config) -> S.World:
+    """The configuration's seeded world, its first column at x = ``cfg.origin_x``."""
+    world = S.generate_world(cfg.chunks, cfg.seed, emitters=cfg.emitters)
+    world.origin = (cfg.origin_x, world.origin[1], world.origin[2])
+    return world
+
+
+def write_save(cfg: Config, path: str) -> list:
+    """Writes the configuration's world as an Anvil save in `path` (``level.dat`` and
+    ``region/``, `anvil.write_world`): its chunks where the frame places them, the day time the
+    frame's, the spawn under the eye. Returns the region files written."""
+    spawn = (math.floor(cfg.eye[0]), 64, math.floor(cfg.eye[2]))
+    return AN.write_world(config_world(cfg), path, name=f"Lumenwright {cfg.name}", spawn=spawn, day_time=cfg.time)
+
+
 def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None) -> HqFrame:
     """The hq frame of a configuration, as `render()` assembles it (request.rs:640-653, 751-930).
 
@@ -152,8 +168,7 @@ def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None)
         from .native import Context
         own = sky_backend = Context(0)
     try:
-        world = S.generate_world(cfg.chunks, cfg.seed, emitters=cfg.emitters)
-        world.origin = (cfg.origin_x, world.origin[1], world.origin[2])
+        world = config_world(cfg)
         atlas = S.build_atlas(cfg.seed)
         hq = build_hq(world, atlas)
         yaw, pitch = Camera.look_at(cfg.eye, cfg.target)
