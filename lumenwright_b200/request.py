@@ -151,7 +151,7 @@ def write_save(cfg: Config, path: str) -> list:
     return AN.write_world(config_world(cfg), path, name=f"Lumenwright {cfg.name}", spawn=spawn, day_time=cfg.time)
 
 
-def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None) -> HqFrame:
+def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None, save: Optional[str] = None) -> HqFrame:
     """The hq frame of a configuration, as `render()` assembles it (request.rs:640-653, 751-930).
 
     ``sky_backend`` builds the sky inputs: an object with ``build_sky_cache(params, n)`` (`sky_cache`,
@@ -159,6 +159,10 @@ def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None)
     atlas_w)`` (`draw_map`, sky.rs:861-878: the game sky's maps, from the stated sky of the tick,
     ``gamesky.stated_sky``) and ``blend_chunky_sky(params, cache, maps, sizes, weight)``
     (sky.rs:836-850); by default the library's device kernels on device 0.
+
+    ``save`` names an Anvil save to load the world from (`anvil.read_world`, the configuration's
+    chunks, as `World::open` and `load_area` load them, world/mod.rs:297-491) instead of
+    generating it; `write_save` writes the configuration's own.
     """
     width = width or cfg.width
     height = height or cfg.height
@@ -168,7 +172,10 @@ def make_frame(cfg: Config, sky_backend=None, width=None, height=None, spp=None)
         from .native import Context
         own = sky_backend = Context(0)
     try:
-        world = config_world(cfg)
+        if save is None:
+            world = config_world(cfg)
+        else:
+            world = AN.read_world(save, (int(cfg.origin_x) // 16, 0), (cfg.chunks, cfg.chunks))
         atlas = S.build_atlas(cfg.seed)
         hq = build_hq(world, atlas)
         yaw, pitch = Camera.look_at(cfg.eye, cfg.target)

@@ -167,3 +167,17 @@ def test_config_saves_hold_the_frames_worlds(tmp_path, name):
     back = A.read_world(str(tmp_path), (cx0, 0), (cfg.chunks, cfg.chunks))
     assert back.origin == tuple(float(v) for v in want.origin) and np.array_equal(back.blocks, want.blocks)
     assert A.read_level(str(tmp_path))["DayTime"] == cfg.time
+
+
+def test_a_frame_built_from_its_save_is_the_frame(tmp_path):
+    # make_frame on the save that write_save wrote: the same scene buffers, Params and sky as the
+    # frame built from the generated world (the sky from a host stand-in, as no GPU is here).
+    from lumenwright_b200 import request as R
+    from test_frames import OracleSky
+    cfg = R.CONFIGS["c1"]
+    R.write_save(cfg, str(tmp_path))
+    a = R.make_frame(cfg, sky_backend=OracleSky(), spp=4)
+    b = R.make_frame(cfg, sky_backend=OracleSky(), spp=4, save=str(tmp_path))
+    assert a.params.tobytes() == b.params.tobytes() and np.array_equal(a.sky, b.sky) and a.eye64 == b.eye64
+    for name in ("grid", "models", "quads", "atlas", "emitters", "emitter_grid"):
+        assert getattr(a.scene, name).tobytes() == getattr(b.scene, name).tobytes(), name  # bytes: tints are NaN patterns
