@@ -417,7 +417,10 @@ def read_world(path: str, min_chunk: Tuple[int, int], chunks: Tuple[int, int]) -
             key = (cx >> 5, cz >> 5)
             if key not in cache:
                 f = os.path.join(path, "region", region_name(*key))
-                cache[key] = open(f, "rb").read() if os.path.exists(f) else None
+                cache[key] = None
+                if os.path.exists(f):
+                    with open(f, "rb") as fh:
+                        cache[key] = fh.read()
             if cache[key] is None:
                 continue
             nbt = region_chunk(cache[key], cx & 31, cz & 31)

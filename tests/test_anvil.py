@@ -131,7 +131,8 @@ def test_world_round_trip_through_a_save(tmp_path, origin_chunk):
     assert back.origin == (origin_chunk[0] * 16, -64, origin_chunk[1] * 16)
     assert w.emitters_placed > 0 and np.count_nonzero((back.blocks == S.LANTERN) | (back.blocks == S.GLOWSTONE)) == w.emitters_placed
     # a chunk of the save holds every section of the column, -4..19
-    data = open(files[0], "rb").read()
+    with open(files[0], "rb") as fh:
+        data = fh.read()
     c = A.parse_nbt(A.region_chunk(data, origin_chunk[0] & 31, origin_chunk[1] & 31))[1]
     assert [s["Y"] for s in c["sections"]] == list(range(-4, 20))
     assert c["xPos"] == origin_chunk[0] and c["zPos"] == origin_chunk[1] and c["Status"] == "minecraft:full"
